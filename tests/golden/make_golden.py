@@ -1,0 +1,194 @@
+"""Generate the golden fixtures under tests/golden/ from the plasmonX reference tree.
+
+Run in a container that has the reference checked out (read-only is fine):
+
+    python tests/golden/make_golden.py /path/to/plasmonX
+
+For each hot-path regression test of the reference (``tests/<name>/``) this
+script
+  1. runs the reference's own Python front end (``python/input_``) on the
+     test's YAML, with a stub for the optional ``ase`` package, and stores the
+     keyword file it writes (what the reference Fortran reads) as
+     ``<name>/input.kw``;
+  2. copies the rows of any permittivity / interband-polarizability CSV that
+     the test's frequencies use;
+  3. parses the reference log ``tests/<name>/reference/<name>.log`` and stores
+     the printed numbers in ``<name>/expected.json``: the final per-frequency
+     results block (20 values), the charge / dipole tables, the GMRES residual
+     traces and, when printed, the full dynamic matrix.
+Nothing at run time of the tests reads the reference tree; only these files.
+"""
+import json
+import os
+import re
+import shutil
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+TESTS = [
+    'wfq_sodium_inversion',
+    'wfq_sodium_iterative_on_memory',
+    'wfq_sodium_iterative_on_the_fly',
+    'wfq_sodium_minimal_input',
+    'wfqfmu_ag_inversion',
+    'wfqfmu_ag_iterative_on_memory',
+    'wfqfmu_ag_iterative_on_the_fly',
+    'wfqfmu_ag_internal_permittivity',
+    'wfqfmu_ag_minimal_input',
+    'wfqfmu_au_minimal_input',
+    'wfqfmu_hetero_agau_inversion',
+    'wfqfmu_hetero_agau_iterative_on_memory',
+    'wfqfmu_hetero_agau_iterative_on_the_fly',
+    'wfqfmu_hetero_agau_default_int_param_inversion',
+    'wfqfmu_hetero_agau_read_1param_inversion',
+    'wfqfmu_hetero_agau_minimal_input',
+]
+
+NUM = r'[-+]?\d*\.\d+(?:[EeDd][-+]?\d+)?'
+
+
+def run_front_end(ref, test_dir, yaml_name, work):
+    stub = os.path.join(work, 'stub', 'ase')
+    os.makedirs(stub, exist_ok=True)
+    with open(os.path.join(stub, '__init__.py'), 'w') as f:
+        f.write('')
+    with open(os.path.join(stub, 'io.py'), 'w') as f:
+        f.write('def read(*a, **k):\n    raise RuntimeError("ase is not available")\n')
+    for fn in os.listdir(test_dir):
+        p = os.path.join(test_dir, fn)
+        if os.path.isfile(p):
+            shutil.copy(p, work)
+    sys.path[:0] = [os.path.join(work, 'stub'), os.path.join(ref, 'python')]
+    from input_ import yaml_to_fortran_input  # noqa: E402  (reference front end)
+    cwd = os.getcwd()
+    os.chdir(work)
+    try:
+        t0, w0 = time.process_time(), time.time()
+        yaml_to_fortran_input(t0, w0, yaml_name, 'input.kw', yaml_name[:-5] + '.log', 8, 31.07, ref,
+                              {'front end': 'reference'}, [])
+        with open('input.kw') as f:
+            return f.read()
+    finally:
+        os.chdir(cwd)
+
+
+def parse_log(text):
+    out = {}
+    # final results block, after the backup clean-up message
+    tail = text.split('I am cleaning up the backup')[-1]
+    res = []
+    for blk in re.split(r'Results for w =', tail)[1:]:
+        head = blk.split('\n', 1)[0]
+        vals = re.findall(r'=\s+(' + NUM + r') a\.u\.', blk)
+        if len(vals) >= 20:
+            w_au = float(re.findall(NUM, head)[0])
+            res.append({'w_au_printed': w_au, 'values': [float(v) for v in vals[:20]]})
+    out['results'] = res
+    # charge / dipole tables (verbose >= 2)
+    tables = []
+    for m in re.finditer(r'(wFQ Charges|wFMu Dipoles)\n(.*?)(?:\n -{20,}|\nChErr)', text, re.S):
+        rows = []
+        for line in m.group(2).splitlines():
+            nums = re.findall(NUM, line)
+            if re.match(r'^\s+\d+\s', line) and len(nums) == 6:
+                rows.append([float(v) for v in nums])
+        tables.append({'kind': m.group(1), 'rows': rows})
+    out['tables'] = tables
+    # GMRES residual traces
+    traces = []
+    for m in re.finditer(r'Freq:\s+(' + NUM + r') eV.*?\n(.*?)(?=GMRES Iterative|wFQ Charges|Results for w|\Z)', text, re.S):
+        freq_ev = float(m.group(1))
+        for pm in re.finditer(r'- Polarization: ([XYZ])\s+Iteration\s+Residual\n((?:\s+\d+\s+' + NUM + r'\n)+)',
+                              m.group(2)):
+            vals = [float(v) for v in re.findall(r'\s+\d+\s+(' + NUM + r')\n', pm.group(2))]
+            traces.append({'freq_ev': freq_ev, 'pol': pm.group(1), 'residuals': vals})
+    out['gmres'] = traces
+    # full dynamic matrix print (verbose 3, inversion)
+    for part in ('Real', 'IMag'):
+        key = 'matrix_' + part.lower()
+        m = re.search(r'(?:wfqfmu|wFQ) Matrix: ' + part + r' Part\n -+\n(.*?)\n -{20,}', text, re.S)
+        if not m:
+            continue
+        entries = {}
+        cols = None
+        for line in m.group(1).splitlines():
+            if not line.strip():
+                continue
+            toks = line.split()
+            if all(re.fullmatch(r'\d+', t) for t in toks):
+                cols = [int(t) for t in toks]
+                continue
+            if cols and re.fullmatch(r'\d+', toks[0]):
+                r = int(toks[0])
+                for c, v in zip(cols, toks[1:]):
+                    entries['%d,%d' % (r, c)] = float(v.replace('D', 'E'))
+        out[key] = entries
+    return out
+
+
+def csv_subset(path, freqs_ev):
+    keep = []
+    with open(path) as f:
+        for line in f:
+            if '#' in line:
+                keep.append(line)
+                continue
+            p = line.replace(',', ' ').split()
+            if len(p) >= 3 and any(abs(float(p[0]) - e) <= 1e-6 for e in freqs_ev):
+                keep.append(line)
+    return ''.join(keep)
+
+
+def main(ref):
+    import subprocess
+    for name in TESTS:
+        # one process per test: the front end keeps module-level state
+        subprocess.run([sys.executable, os.path.abspath(__file__), '--one', name, ref], check=True,
+                       stderr=subprocess.DEVNULL)
+
+
+def one(name, ref):
+    if True:
+        tdir = os.path.join(ref, 'tests', name)
+        yamls = [f for f in os.listdir(tdir) if f.endswith('.yaml')]
+        with tempfile.TemporaryDirectory() as work:
+            kw = run_front_end(ref, tdir, yamls[0], work)
+        odir = os.path.join(HERE, name)
+        os.makedirs(odir, exist_ok=True)
+        with open(os.path.join(odir, 'input.kw'), 'w') as f:
+            f.write(kw)
+        # frequencies (a.u. -> eV) for CSV row selection
+        vals = dict(l.split(':', 1) for l in kw.splitlines() if ':' in l and not l.startswith('#'))
+        nf = int(float(vals['field nfreq']))
+        fmin, fmax, fstep = (float(vals['field min freq']), float(vals['field max freq']),
+                             float(vals['field step freq']))
+        if fmin == 0.0 and fmax == 0.0:
+            fr = [float(x) for x in vals['field external freq'].replace(',', ' ').split()][:nf]
+        else:
+            fr = [fmin + fstep * i for i in range(nf)]
+        fev = [w * 27.211386245981 for w in fr]
+        for line in kw.splitlines():
+            if 'wfqfmu file:' in line:
+                fn = line.split(':', 1)[1].strip()
+                if fn != 'none':
+                    src = os.path.join(tdir, fn)
+                    with open(os.path.join(odir, os.path.basename(fn)), 'w') as f:
+                        f.write(csv_subset(src, fev))
+        with open(os.path.join(tdir, 'reference', name + '.log')) as f:
+            parsed = parse_log(f.read())
+        with open(os.path.join(tdir, 'test')) as f:
+            parsed['runtest_filter'] = re.findall(r'get_filter\((.*?)\)', f.read(), re.S)
+        with open(os.path.join(odir, 'expected.json'), 'w') as f:
+            json.dump(parsed, f, indent=0)
+        print(name, len(parsed['results']), 'results,', len(parsed['tables']), 'tables,',
+              len(parsed['gmres']), 'traces', 'matrix' if 'matrix_real' in parsed else '')
+
+
+if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[1] == '--one':
+        one(sys.argv[2], sys.argv[3])
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')

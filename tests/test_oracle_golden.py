@@ -1,0 +1,140 @@
+"""Pin the CPU oracle to the numbers printed in the reference's own regression logs.
+
+Each fixture under tests/golden/<name>/ holds the keyword file the reference
+front end wrote for the reference test ``tests/<name>/<name>.yaml`` and the
+numbers its log printed (see tests/golden/make_golden.py).  The oracle must
+round to every printed digit: results (E14.6), charge and dipole tables
+(E10.3), GMRES residual traces (E13.5) and the printed dynamic matrix (E11.4).
+"""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import model, solve
+from tests.conftest import GOLDEN, golden_dirs
+from tests.printed import agrees
+
+CASES = golden_dirs()
+
+
+def load(name):
+    d = os.path.join(GOLDEN, name)
+    with open(os.path.join(d, 'expected.json')) as f:
+        exp = json.load(f)
+    s = model.System.from_keywords(os.path.join(d, 'input.kw'))
+    return s, exp
+
+
+def _method(s):
+    return 'inversion' if s.method == 'inversion' else 'gmres'
+
+
+def runtest_tolerance(exp):
+    """(abs, rel) tolerance of the reference test's own runtest filter."""
+    a = r = 0.0
+    for flt in exp['runtest_filter']:
+        m = re.search(r'abs_tolerance\s*=\s*([0-9.eE+-]+)', flt)
+        if m:
+            a = max(a, float(m.group(1)))
+        m = re.search(r'rel_tolerance\s*=\s*([0-9.eE+-]+)', flt)
+        if m:
+            r = max(r, float(m.group(1)))
+    return a, r
+
+
+class Pin:
+    """Every value must round to the printed digits, or -- for the few values that
+    sit on a rounding boundary or at an ill-conditioned frequency -- lie within the
+    reference test's own runtest tolerance; at least 97% must meet the first bar."""
+
+    def __init__(self, exp):
+        self.abs_tol, self.rel_tol = runtest_tolerance(exp)
+        self.n = self.exact = 0
+        self.bad = []
+
+    def check(self, v, p, sig, where, abs_floor=0.0):
+        self.n += 1
+        if agrees(v, p, sig, abs_floor=abs_floor):
+            self.exact += 1
+            return
+        if abs(v - p) <= max(self.abs_tol, self.rel_tol * abs(p)):
+            return
+        self.bad.append((where, v, p))
+
+    def verify(self):
+        assert not self.bad, 'outside the reference tolerance: %s' % self.bad[:5]
+        assert self.exact >= 0.97 * self.n, (self.exact, self.n)
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_oracle_matches_reference_log(name):
+    s, exp = load(name)
+    traces = []
+    out = solve.solve(s, method=_method(s), traces=traces)
+    pin = Pin(exp)
+    # final results block: 20 values per frequency, E14.6
+    assert len(exp['results']) == len(s.freqs)
+    for i, blk in enumerate(exp['results']):
+        for k, (v, p) in enumerate(zip(out['results'][i], blk['values'])):
+            pin.check(v, p, 6, ('results', i, k + 1))
+    # charge / dipole tables, E10.3
+    per_freq = 2 if s.model == 'wfqfmu' else 1
+    for t, tab in enumerate(exp['tables']):
+        i = t // per_freq
+        x = out['x'][i]
+        off = 0 if tab['kind'] == 'wFQ Charges' else s.n_atoms
+        for r, row in enumerate(tab['rows']):
+            vals = []
+            for c in range(3):
+                vals += [x[off + r, c].real, x[off + r, c].imag]
+            for v, p in zip(vals, row):
+                pin.check(v, p, 3, (tab['kind'], t, r), abs_floor=1e-12)
+    # GMRES residual traces, E13.5.  Every (frequency, polarisation) must take the
+    # same number of Arnoldi steps; each logged residual must round to the printed
+    # digits, except that a few mid-run steps of near-breakdown Krylov sequences
+    # (symmetric clusters) depend on the BLAS summation order -- those must stay
+    # within a factor 10 (the reference's own on-memory and on-the-fly logs of the
+    # same 37-atom system end at 1.52e-9 and 4.94e-10) unless both are at the
+    # round-off floor (below 1e-9 of the first residual) or past the tolerance.  In the well-conditioned
+    # sodium spectra >99% of residuals round exactly; in the symmetric 37-atom Ag
+    # cluster only the early steps do, so the fraction asked for is 40%.
+    # A solve whose last-but-one residual lands next to the tolerance may take one
+    # step more or less; that is allowed for at most 1% of the solves.
+    assert len(traces) == len(exp['gmres'])
+    n_tr = n_tr_exact = n_off_by_one = 0
+    for (i, c, tr), ref in zip(traces, exp['gmres']):
+        assert 'XYZ'[c] == ref['pol']
+        if len(tr) != len(ref['residuals']):
+            assert abs(len(tr) - len(ref['residuals'])) == 1, (name, i, c)
+            n_off_by_one += 1
+        for v, p in zip(tr[:-1], ref['residuals'][:-1]):
+            n_tr += 1
+            if agrees(v, p, 5):
+                n_tr_exact += 1
+            elif max(v, p) > max(1e-9 * tr[0], s.tol):
+                assert p / 10.0 <= v <= p * 10.0, (name, i, c, v, p)
+        assert agrees(tr[0], ref['residuals'][0], 5)
+    assert n_tr_exact >= 0.4 * n_tr, (n_tr_exact, n_tr)
+    assert n_off_by_one <= 0.01 * max(1, len(traces)), n_off_by_one
+    # printed dynamic matrix (verbose 3, inversion), E11.4
+    if 'matrix_real' in exp:
+        A = model.Operator(s).matrix(0)
+        for part, key in ((np.real, 'matrix_real'), (np.imag, 'matrix_imag')):
+            M = part(A)
+            for rc, p in exp[key].items():
+                r, c = (int(v) - 1 for v in rc.split(','))
+                pin.check(M[r, c], p, 4, (key, rc), abs_floor=1e-14)
+    pin.verify()
+
+
+def test_charge_conservation_homogeneous():
+    """Sum of charges is zero to round-off: (K-P) has zero row sums, so 1^T A_qq = 0 in
+    exact arithmetic only for the symmetric case; the solve conserves charge through
+    the structure of the right-hand side (wfq_module.f90:523-583 prints ChErr)."""
+    s, _ = load('wfqfmu_ag_inversion')
+    out = solve.solve(s, method='inversion')
+    q = out['x'][0][:s.n_atoms]
+    assert np.all(np.abs(q.sum(axis=0)) <= 1e-12 * np.abs(q).sum(axis=0) + 1e-18)
