@@ -1,0 +1,342 @@
+"""Benchmark of the per-frequency response solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config ag_sphere|na_sphere|bowtie] [--precision fp64|mixed_bf16x3]
+
+Workload (default): the wFQFMu silver sphere -- fcc a = 4.086 A cut to a 35 A
+sphere, 10,473 atoms, 41,892 complex unknowns -- with the reference's default
+Ag parameters, 201 frequencies over 3.0-4.5 eV, x polarisation, on-memory
+GMRES at the reference's default tolerance (1e-9 x sqrt(n_var)).  Synthetic,
+seeded geometry; the dense T (14.0 GB FP64) is far larger than L2, so every
+step streams it from HBM (no L2 flush needed).
+
+One step = one spectrum: every frequency solved (201 freq-solves).  `value`
+is freq-solves/s over all ranks from the library's own CUDA-event timing of
+each solve (max over ranks); `e2e` is the same metric through the public
+Python API with host buffers: geometry upload and build, frequency tables,
+solve, results back to the host.  Under torchrun every rank solves its own
+replica of the spectrum (weak scaling; no collective on the data path).
+
+`--impl reference` times the reference's algorithm on the host CPU: the
+threaded C restatement of its on-the-fly product (oracle/pairs.c) over a
+bounded sample of matrix-vector products of the same geometry, turned into
+freq-solves/s with the Arnoldi step count per frequency-solve.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'freq-solves/s at <=1e-6 rel sigma_abs err'
+PEAKS_FALLBACK = {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustained': 1400.0}
+# Arnoldi steps per frequency-solve of the default workload (mean over the 201
+# frequencies), measured with the FP64 GMRES on B200; used to turn the CPU
+# arm's timed matrix-vector products into freq-solves/s.
+STEPS_PER_SOLVE = {'ag_sphere': None}
+
+
+def peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, 'measured'
+    return PEAKS_FALLBACK, 'fallback'
+
+
+def make_problem(name, n_freq=None, method='iterative', polarization='x', radius=None):
+    from plasmonx_b200 import configs
+    if name == 'ag_sphere':
+        return configs.ag_sphere(radius=radius or 35.0, n_freq=n_freq or 201, method=method, tolerance=1e-9,
+                                 polarization=polarization, gmres_dim=1000)
+    if name == 'na_sphere':
+        return configs.na_sphere(radius=20.0, n_freq=n_freq or 61, method=method, tolerance=1e-8,
+                                 polarization=polarization)
+    if name == 'bowtie':
+        return configs.agau_bowtie(n_freq=n_freq or 201, method='iterative on the fly', tolerance=1e-9,
+                                   polarization=polarization)
+    raise ValueError(name)
+
+
+def workload_desc(name, prob):
+    return {'workload': {'ag_sphere': 'wFQFMu Ag fcc sphere R=35 A',
+                         'na_sphere': 'wFQ Na bcc sphere R=20 A',
+                         'bowtie': 'wFQFMu Ag-Au bow-tie'}[name],
+            'n_atoms': int(prob.n_atoms), 'n_var': int(prob.n_var), 'n_freq': int(len(prob.freqs)),
+            'polarization': prob.polarization, 'mode': prob.method, 'tolerance': prob.tolerance_input,
+            'l2': 'inputs larger than L2 (stored T %.1f GB)' % (8.0 * prob.n_var ** 2 / 1e9)}
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + q,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(',')]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[4:8]):
+                if v.lower().startswith('active'):
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no samples']}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': float(max(mx)), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device('cuda', local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def allmax(pg, v, local):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device='cuda:%d' % local)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(pg, v, local):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device='cuda:%d' % local)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        torch.cuda.synchronize(local)
+        pg.barrier()
+
+
+def cpu_sample(prob, n_mv, n_threads, steps_per_solve):
+    """Time n_mv on-the-fly products of the C restatement; return freq-solves/s."""
+    from oracle import keywords, model
+    from oracle.cpu_baseline import CpuOperator
+    s = model.System.from_keywords(keywords.read_keyword_text(prob.to_keyword_text()))
+    op = CpuOperator(s, n_threads=n_threads)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(s.n_var) + 1j * rng.standard_normal(s.n_var)
+    t0 = time.perf_counter()
+    for k in range(n_mv):
+        x = op.matvec(k % len(s.freqs), x)
+        x /= np.linalg.norm(x)
+    dt = (time.perf_counter() - t0) / n_mv
+    return 1.0 / (dt * steps_per_solve), dt, op.n_threads
+
+
+def run_reference(args):
+    rank, world, local, pg = dist_setup()
+    if rank != 0:
+        return
+    prob = make_problem(args.config)
+    sps = args.steps_per_solve
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(prob, 1, 0, sps)
+    for _ in range(args.steps):
+        v, dt, nthr = cpu_sample(prob, args.cpu_matvecs, 0, sps)
+        vals.append(v)
+    v = float(np.mean(vals))
+    line = {'metric': METRIC, 'value': v, 'unit': 'freq-solves/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1000.0 / v * len(prob.freqs), 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': workload_desc(args.config, prob), 'impl': 'reference',
+            'cpu_baseline': {'value': v, 'unit': 'freq-solves/s', 'cores': nthr, 'kind': 'port',
+                             'sample': '%d on-the-fly A x products of the C restatement per step, '
+                                       'x %.0f Arnoldi steps per freq-solve' % (args.cpu_matvecs, sps)},
+            'e2e': {'value': v, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=2)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--config', default='ag_sphere', choices=['ag_sphere', 'na_sphere', 'bowtie'])
+    ap.add_argument('--precision', default='fp64')
+    ap.add_argument('--e2e-steps', type=int, default=1)
+    ap.add_argument('--cpu-matvecs', type=int, default=2)
+    ap.add_argument('--steps-per-solve', type=float, default=150.0)
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--accuracy-freqs', type=int, default=5)
+    ap.add_argument('--radius', type=float, default=None, help='smaller sphere (profiling runs only)')
+    ap.add_argument('--n-freq', type=int, default=None, help='fewer frequencies (profiling runs only)')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        return run_reference(args)
+
+    rank, world, local, pg = dist_setup()
+    from plasmonx_b200.solver import Context, Solver
+    prob = make_problem(args.config, n_freq=args.n_freq, radius=args.radius)
+    F = len(prob.freqs)
+    ctx = Context(local)
+    solver = Solver(prob, ctx=ctx, store_t=prob.method != 'iterative on the fly')
+
+    def step():
+        out = solver.solve(precision=args.precision)
+        if 'error' in out:
+            raise out['error']
+        return out
+
+    for _ in range(args.warmup):
+        step()
+    barrier(pg, local)
+    ctx.profile(True)
+    dev_ms = []
+    launches = 0
+    steps_hist = []
+    with Clocks(local) as clk:
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            out = step()
+            dev_ms.append(out['device_ms'])
+            launches += out['launches']
+            steps_hist.append(out['steps'][:, 0].copy())
+        barrier(pg, local)
+        wall = time.perf_counter() - t0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    total_ms = allmax(pg, float(np.sum(dev_ms)), local)
+    solves = allsum(pg, float(F * args.steps), local)
+    value = solves / (total_ms / 1000.0)
+
+    # accuracy: sigma_abs against a tight-tolerance FP64 solve of a frequency subset
+    acc = None
+    if args.accuracy_freqs > 0:
+        idx = np.linspace(0, F - 1, min(args.accuracy_freqs, F)).round().astype(int)
+        b = solver.rhs(int(idx[0]), prob.pol_mask)
+        ref_solver = solver
+        ref_solver.set_frequencies(prob.freqs[idx], None if prob.alpha_w is None else prob.alpha_w[:, idx])
+        tight = ref_solver.solve(precision='fp64', tol=1e-12 * np.linalg.norm(b), max_krylov=2000)
+        solver.set_frequencies(prob.freqs, prob.alpha_w)
+        sig = out['results'][idx, 9]
+        sref = tight['results'][:, 9]
+        acc = float(np.max(np.abs(sig - sref) / np.abs(sref)))
+
+    # end to end through the public API: build + upload + solve + results to host
+    e2e_times = []
+    h2d = 0
+    for _ in range(args.e2e_steps):
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        with Solver(prob, ctx=ctx) as s2:
+            o2 = s2.solve(precision=args.precision)
+        barrier(pg, local)
+        e2e_times.append(time.perf_counter() - t0)
+        k = s2._keep
+        h2d = sum(v.nbytes for v in k.values()) + s2.freqs.nbytes + (0 if s2._aw is None else s2._aw.nbytes)
+    e2e_s = allmax(pg, float(np.mean(e2e_times)), local) if e2e_times else float('nan')
+    e2e_val = solves / args.steps / e2e_s if e2e_times else None
+
+    pk, pk_kind = peaks()
+    n = prob.n_var
+    avg_ms = prof['ms'] / max(1, prof['launches'])
+    bytes_per = prof['bytes'] / max(1, prof['launches'])
+    flops_per = prof['flops'] / max(1, prof['launches'])
+    if args.precision == 'fp64':
+        roof = {'kernel': 'T contraction (FP64, CUDA cores)', 'bound': 'hbm',
+                'achieved': bytes_per / (avg_ms / 1000.0) / 1e9, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+                'peak_kind': pk_kind, 'flops_per_launch': flops_per, 'bytes_per_launch': bytes_per,
+                'avg_launch_ms': avg_ms, 'achieved_fp64_tflops': flops_per / (avg_ms / 1000.0) / 1e12,
+                'traffic': None}
+    else:
+        roof = {'kernel': 'T contraction (tcgen05 BF16x3)', 'bound': 'tensor',
+                'achieved': flops_per / (avg_ms / 1000.0) / 1e12, 'peak': pk['bf16_tflops'], 'unit': 'TFLOP/s',
+                'peak_kind': pk_kind, 'flops_per_launch': flops_per, 'bytes_per_launch': bytes_per,
+                'avg_launch_ms': avg_ms, 'traffic': None}
+    roof['frac'] = roof['achieved'] / roof['peak']
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sps = float(np.mean(np.concatenate(steps_hist))) if steps_hist else args.steps_per_solve
+        v, dt, nthr = cpu_sample(prob, args.cpu_matvecs, 0, sps)
+        cpu = {'value': v, 'unit': 'freq-solves/s', 'cores': nthr, 'kind': 'port',
+               'sample': '%d on-the-fly A x products of the C restatement (%.2f s each) x %.1f Arnoldi steps '
+                         'per freq-solve (mean of this run)' % (args.cpu_matvecs, dt, sps)}
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': 'freq-solves/s', 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+                'dtype': 'f64' if args.precision == 'fp64' else 'bf16x3+f64',
+                'data': 'synthetic (seeded fcc lattice, reference default parameters)',
+                'config': dict(workload_desc(args.config, prob), precision=args.precision),
+                'e2e': {'value': e2e_val, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': int(h2d),
+                        'd2h_bytes_per_step': int(F * (20 * 8 + 9 * 16 + 4 + 12))},
+                'gpu_launches': int(launches), 'roofline': roof, 'cpu_baseline': cpu,
+                'clocks': clk.summary(), 'wall_s_timed': wall,
+                'sigma_abs_max_rel_err': acc,
+                'arnoldi_steps': {'mean': float(np.mean(np.concatenate(steps_hist))),
+                                  'max': int(np.max(np.concatenate(steps_hist)))}}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,202 @@
+/*
+ * plasmonx_b200 -- C ABI of the B200 (sm_100a) per-frequency response solve.
+ *
+ * Drop-in boundary for the plasmonX solver layer.  The reference has no FFI;
+ * its de-facto boundary is the type-bound procedure set of `target_type`
+ * (src/target/target_module.f90:20-133) called from the per-frequency loops
+ * of src/solvers/algorithm_module.f90:189-465, plus the free routines
+ * `gmres_solver` (src/solvers/gmres_module.f90:30-31) and `complex_inversion`
+ * (src/solvers/algorithm_module.f90:510).  Each entry point below names the
+ * reference interface it replaces.
+ *
+ * Conventions (match the reference's Fortran data so that an iso_c_binding
+ * interface can pass its arrays unchanged):
+ *   - all pointers are HOST pointers; the library owns every device buffer and
+ *     copies in and out;
+ *   - complex values are interleaved (re, im) doubles (Fortran complex(dp));
+ *   - matrices are column-major; "n_var x 3" means 3 contiguous columns;
+ *   - unknowns are ordered as the reference orders them: charges q_1..q_N,
+ *     then dipoles mu_1x, mu_1y, mu_1z, ..., mu_Nz;
+ *   - lengths are bohr, frequencies atomic units;
+ *   - every call returns a plx_status; nothing calls exit/stop.  The text of
+ *     the last error of a context is available from plx_last_error().
+ * Thread safety: one context may be used by one host thread at a time.
+ */
+#ifndef PLASMONX_B200_H
+#define PLASMONX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct plx_ctx plx_ctx;
+typedef struct plx_geom plx_geom;
+
+typedef enum {
+    PLX_OK = 0,
+    PLX_ERR_ARG = 1,            /* invalid argument (null pointer, size, enum) */
+    PLX_ERR_CUDA = 2,           /* CUDA runtime / library failure */
+    PLX_ERR_NOMEM = 3,          /* device allocation failed */
+    PLX_ERR_BUDGET = 4,         /* request exceeds the context's HBM budget */
+    PLX_ERR_NOT_CONVERGED = 5,  /* GMRES ran out of Krylov dimension (the
+                                   reference stops with "GMRES not converged
+                                   and restart GMRES NYI.") */
+    PLX_ERR_NAN = 6,            /* non-finite value met in a residual */
+    PLX_ERR_SINGULAR = 7,       /* zgetrf reported info != 0 */
+    PLX_ERR_UNSUPPORTED = 8     /* model / mode combination not provided */
+} plx_status;
+
+typedef enum { PLX_WFQ = 0, PLX_WFQFMU = 1 } plx_model;
+
+typedef enum {
+    PLX_INVERSION = 0,          /* solve_w_inversion  (algorithm_module.f90:189) */
+    PLX_GMRES_MEM = 1,          /* solve_w_iter_mem   (algorithm_module.f90:334) */
+    PLX_GMRES_OTF = 2           /* solve_w_iter_on_the_fly (algorithm_module.f90:417) */
+} plx_mode;
+
+typedef enum {
+    PLX_FP64 = 0,               /* plain complex FP64, the drop-in */
+    PLX_MIXED_BF16X3 = 1        /* tensor-core contraction (split BF16, FP32
+                                   accumulate) inside FP64 iterative refinement */
+} plx_precision;
+
+/* Geometry and model parameters, i.e. what the reference holds in `target_`
+ * and `parameters` after input (src/input_output/input_module.f90:156-258,
+ * src/wfq/wfq_module.f90:96-127).  Per-type arrays have n_types entries;
+ * fermi_d/fermi_s/r0 are n_types x n_types column-major ((i,j) at i + j*n_types);
+ * r0 is the nearest-neighbour distance of the type pair (target_module.f90:472). */
+typedef struct {
+    int32_t model;              /* plx_model */
+    int32_t n_atoms;
+    int32_t n_types;
+    int32_t rhs_potential;      /* 0: V = -E0 r ("field"), 1: V = -E0 |r - r_min| */
+    const double *coord;        /* 3 x n_atoms, bohr */
+    const int32_t *atom_type;   /* n_atoms, 0-based */
+    const int32_t *neighbours;  /* n_types x n_atoms counts (target_module.f90:417) */
+    const int32_t *n_neighbours;/* n_atoms */
+    const double *eta;          /* chemical hardness (T_qq diagonal) */
+    const double *r_q;          /* Gaussian charge width */
+    const double *r_mu;         /* Gaussian dipole width (wFQFMu) */
+    const double *tau;          /* Drude relaxation time, after sigma0/tau scaling */
+    const double *density;      /* n = sigma0 / tau before scaling */
+    const double *a_ij;         /* effective area A_ij */
+    const double *fermi_d;      /* Fermi damping d, type pair */
+    const double *fermi_s;      /* Fermi damping s, type pair */
+    const double *r0;           /* nearest-neighbour distance, type pair (bohr) */
+    double e0;                  /* field intensity (a.u.) */
+} plx_geometry_desc;
+
+/* One solve request over the frequencies set by plx_set_frequencies. */
+typedef struct {
+    int32_t mode;               /* plx_mode */
+    int32_t precision;          /* plx_precision */
+    int32_t pol_mask;           /* bit0 x, bit1 y, bit2 z (reference 'all' = 7) */
+    int32_t max_krylov;         /* GMRES dimension m (reference `gmres dimension`) */
+    double tol;                 /* absolute residual tolerance, already multiplied
+                                   by sqrt(n_var) as input_module.f90:250-251 does */
+    int32_t freq_block;         /* frequencies solved together; 0 = automatic */
+    int32_t record_trace;       /* 1: fill trace_out with the logged residuals */
+} plx_solve_desc;
+
+/* ---- context --------------------------------------------------------------- */
+
+/* Creates a context on CUDA device `device`.  hbm_budget_bytes = 0 means the
+ * free device memory at creation.  Returns NULL only on allocation failure of
+ * the host object; device errors are reported by later calls. */
+plx_ctx *plx_ctx_create(int32_t device, uint64_t hbm_budget_bytes);
+void plx_ctx_destroy(plx_ctx *ctx);
+const char *plx_last_error(const plx_ctx *ctx);
+/* Device bytes currently held by the context (geometries + solver state). */
+uint64_t plx_ctx_bytes_in_use(const plx_ctx *ctx);
+
+/* ---- geometry -------------------------------------------------------------- */
+
+/* Uploads coordinates and parameters and builds, once per geometry, the
+ * frequency-independent data on the device: the sparse Drude/Fermi
+ * conductance K (construct_K_minus_P_matrix, matrix_module.f90:393-426) as a
+ * CSR matrix, and -- when store_t != 0 -- the dense interaction matrix T
+ * (construct_static_t_qq/qmu/muq/mumu, matrix_module.f90:58-345) needed by the
+ * on-memory and inversion modes.  `*out` receives the geometry handle. */
+plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *desc,
+                               int32_t store_t, plx_geom **out);
+void plx_geometry_destroy(plx_geom *geom);
+/* Number of unknowns n_var (N for wFQ, 4N for wFQFMu). */
+int64_t plx_geometry_n_var(const plx_geom *geom);
+/* Stored non-zeros of K (both triangles). */
+int64_t plx_geometry_k_nnz(const plx_geom *geom);
+
+/* Sets the frequency grid (field%freq, field_module.f90:157-176) and, for
+ * wFQFMu, the interband polarizability alpha_t(w) of every atom type
+ * (parameters%alpha_w, wfqfmu_module.f90:97-166): alpha_w is complex
+ * n_types x n_freq column-major.  alpha_w may be NULL for wFQ. */
+plx_status plx_set_frequencies(plx_geom *geom, int32_t n_freq, const double *omega,
+                               const double *alpha_w);
+
+/* ---- reference-shaped kernels --------------------------------------------- */
+
+/* y = A(w_i) x: product_matrix_vector followed by new_gmres_diagonal_shift
+ * (target_module.f90:1340-1356, 1392-1408; wfq_module.f90:321-424;
+ * wfqfmu_module.f90:584-746).  x, y: complex n_var.  on_the_fly = 0 uses the
+ * stored T, 1 generates the interaction tiles in the kernel. */
+plx_status plx_matvec(plx_geom *geom, int32_t i_freq, int32_t on_the_fly,
+                      const double *x, double *y);
+
+/* Dynamic right-hand sides b(w_i), complex n_var x 3
+ * (construct_dynamic_field_rhs[_on_the_fly] + assign_variables_w[_on_the_fly],
+ * wfq_module.f90:260-301, wfqfmu_module.f90:177-430, rhs_module.f90:43-430).
+ * Columns of polarisations not in pol_mask are zero. */
+plx_status plx_rhs(plx_geom *geom, int32_t i_freq, int32_t pol_mask, double *b);
+
+/* gmres_solver (gmres_module.f90:30-228) for one column: x holds the RHS on
+ * entry and the solution on exit; tol is absolute; restart is the Krylov
+ * dimension.  steps_out (optional) receives the number of Arnoldi steps and
+ * trace_out (optional, restart doubles) the logged residuals. */
+plx_status plx_gmres_solver(plx_geom *geom, int32_t i_freq, double *x, int32_t on_the_fly,
+                            double tol, int32_t max_iter, int32_t restart,
+                            int32_t *steps_out, double *trace_out);
+
+/* complex_inversion (algorithm_module.f90:510-541) on A(w_i): zgetrf + zgetrs
+ * with the 3 columns of variables_w (complex n_var x 3, RHS in / solution out). */
+plx_status plx_complex_inversion(plx_geom *geom, int32_t i_freq, double *variables_w);
+
+/* ---- the spectrum solve --------------------------------------------------- */
+
+/* Solves every frequency of the grid: the three per-frequency loops of
+ * algorithm_module.f90:189-465 with calculate_dynamic_polar and
+ * calculate_cross_section (target_module.f90:1989-2054) fused in.
+ *   x_out      optional, complex n_var x 3 x n_freq (variables_w per frequency);
+ *              columns that were not solved hold the right-hand side, as in
+ *              the reference
+ *   polar_out  optional, complex 3 x 3 x n_freq (polar_w, column b = field b)
+ *   results_out optional, n_freq x 20 row-major (target_%results(i,1:20))
+ *   status_out optional, n_freq plx_status values
+ *   steps_out  optional, 3 x n_freq Arnoldi step counts (0 if not solved)
+ *   trace_out  optional, max_krylov x 3 x n_freq logged residuals (record_trace)
+ * Returns the first non-OK per-frequency status, or PLX_OK. */
+plx_status plx_solve(plx_geom *geom, const plx_solve_desc *desc, double *x_out,
+                     double *polar_out, double *results_out, int32_t *status_out,
+                     int32_t *steps_out, double *trace_out);
+
+/* Device time (ms, CUDA events on the library's stream) of the last plx_solve,
+ * and the number of kernels it launched. */
+double plx_last_solve_ms(const plx_geom *geom);
+int64_t plx_last_solve_launches(const plx_geom *geom);
+
+/* ---- measurement -------------------------------------------------------- */
+
+/* When enabled, the library brackets every launch of the T contraction (the
+ * dominant kernel of the iterative modes) with CUDA events on its stream and
+ * accumulates, per launch, the algorithmic flops (2 n_var^2 x real columns) and
+ * bytes (the stored T once, the input and output columns).  Enabling resets the
+ * counters. */
+plx_status plx_profile_enable(plx_ctx *ctx, int32_t on);
+/* Reads the accumulated contraction time (ms), launches, flops and bytes. */
+plx_status plx_profile_read(plx_ctx *ctx, double *ms, int64_t *launches, double *flops, double *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLASMONX_B200_H */

@@ -1,0 +1,513 @@
+// Batched complex GMRES in FP64 with the reference's semantics
+// (src/solvers/gmres_module.f90:30-228), one independent Krylov space per
+// column (frequency x polarisation), all columns advanced in lock step so that
+// every Arnoldi step is ONE batched operator application.
+//
+// Per column, exactly as the reference: x0 = 0, v1 = b/||b||, Arnoldi with
+// modified Gram-Schmidt for j < 25 and classical Gram-Schmidt with one
+// re-orthogonalisation for j >= 25, Givens rotations with reference-BLAS
+// zrotg/zrot semantics, the logged residual |g_{j+1}| compared with the
+// absolute tolerance, then the triangular solve, x += V y and the true
+// residual ||b - A x|| deciding convergence; no restart.
+//
+// Storage: Krylov vectors are kept in "slabs", one per step j, each holding
+// the j-th basis vector of every column ([C][2][n] split complex), allocated
+// when the step is reached so that memory follows the actual iteration count.
+// Columns that converge leave the active list; the operator and the Arnoldi
+// kernels only touch active columns.
+#include <algorithm>
+#include <cmath>
+
+#include "plx_internal.h"
+
+namespace plx {
+
+namespace {
+
+constexpr int kRows = 2048;     // rows per block in the Arnoldi kernels
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block reduction of two doubles; result valid in thread 0.
+__device__ __forceinline__ void block_sum2(double &a, double &b) {
+    __shared__ double ra[32], rb[32];
+    a = warp_sum(a);
+    b = warp_sum(b);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        ra[w] = a;
+        rb[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        a = l < nw ? ra[l] : 0.0;
+        b = l < nw ? rb[l] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+    }
+}
+
+// Copies column act[k] of slab j into the compact batch X[k].
+__global__ void gather_cols(int n, const int32_t *__restrict__ act, const double *__restrict__ slab,
+                            double *__restrict__ X) {
+    int k = blockIdx.y;
+    const double *src = slab + (int64_t)act[k] * 2 * n;
+    double *dst = X + (int64_t)k * 2 * n;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
+         r += (int64_t)gridDim.x * blockDim.x)
+        dst[r] = src[r];
+}
+
+// Partial complex dots conj(V_i[c]) . W[k] for i in [i0, i1), rows of one chunk.
+// One warp per basis vector; W chunk staged in shared memory.
+__global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
+                                                         const int32_t *__restrict__ act,
+                                                         double *const *__restrict__ slabs,
+                                                         const double *__restrict__ W,
+                                                         double2 *__restrict__ part) {
+    extern __shared__ double sw[];   // [2][kRows]
+    int k = blockIdx.y, c = act[k];
+    int r0 = blockIdx.x * kRows;
+    int rn = min(kRows, n - r0);
+    const double *wr = W + (int64_t)k * 2 * n;
+    for (int t = threadIdx.x; t < rn; t += blockDim.x) {
+        sw[t] = wr[r0 + t];
+        sw[kRows + t] = wr[n + r0 + t];
+    }
+    __syncthreads();
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int nw = blockDim.x >> 5;
+    int ni = i1 - i0;
+    for (int ii = warp; ii < ni; ii += nw) {
+        const double *v = slabs[i0 + ii] + (int64_t)c * 2 * n;
+        double re = 0.0, im = 0.0;
+        for (int t = lane; t < rn; t += 32) {
+            double vr = v[r0 + t], vi = v[n + r0 + t];
+            double xr = sw[t], xi = sw[kRows + t];
+            re += vr * xr + vi * xi;       // conj(v) * w
+            im += vr * xi - vi * xr;
+        }
+        re = warp_sum(re);
+        im = warp_sum(im);
+        if (lane == 0) part[((int64_t)k * gridDim.x + blockIdx.x) * ni + ii] = make_double2(re, im);
+    }
+}
+
+// Sums the chunk partials: h[k][ii] = sum_b part[k][b][ii]; optionally accumulates
+// into H column j (Hcol[c][i0+ii] += h) when Hslab != nullptr.
+__global__ void dots_finish(int nchunk, int ni, int i0, const int32_t *__restrict__ act,
+                            const double2 *__restrict__ part, double2 *__restrict__ h,
+                            double2 *__restrict__ Hcol, int hstride, int accumulate) {
+    int k = blockIdx.y;
+    int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= ni) return;
+    double2 s = make_double2(0.0, 0.0);
+    for (int b = 0; b < nchunk; ++b) {
+        double2 p = part[((int64_t)k * nchunk + b) * ni + ii];
+        s.x += p.x;
+        s.y += p.y;
+    }
+    h[(int64_t)k * ni + ii] = s;
+    if (Hcol) {
+        double2 *dst = Hcol + (int64_t)act[k] * hstride + i0 + ii;
+        if (accumulate) {
+            dst->x += s.x;
+            dst->y += s.y;
+        } else {
+            *dst = s;
+        }
+    }
+}
+
+// W[k] -= sum_{ii} V_{i0+ii}[c] h[k][ii]   (sign = -1), or X[c] += ... (sign = +1,
+// target indexed by column instead of compact position when by_col != 0).
+__global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int hld, int hoff,
+                                                    const int32_t *__restrict__ act,
+                                                    double *const *__restrict__ slabs,
+                                                    const double2 *__restrict__ h, double sign,
+                                                    double *__restrict__ Y, int by_col) {
+    extern __shared__ double2 sh[];
+    int k = blockIdx.y, c = act[k];
+    for (int t = threadIdx.x; t < ni; t += blockDim.x) sh[t] = h[(int64_t)k * hld + hoff + t];
+    __syncthreads();
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double ar = 0.0, ai = 0.0;
+    for (int ii = 0; ii < ni; ++ii) {
+        const double *v = slabs[i0 + ii] + (int64_t)c * 2 * n;
+        double vr = v[r], vi = v[n + r];
+        double2 hh = sh[ii];
+        ar += vr * hh.x - vi * hh.y;
+        ai += vr * hh.y + vi * hh.x;
+    }
+    double *y = Y + (int64_t)(by_col ? c : k) * 2 * n;
+    y[r] += sign * ar;
+    y[n + r] += sign * ai;
+}
+
+// ||W[k]||_2 (dznrm2): partial sums of squares per chunk.
+__global__ void norm_partial(int n, const double *__restrict__ W, double *__restrict__ part) {
+    int k = blockIdx.y;
+    const double *w = W + (int64_t)k * 2 * n;
+    int r0 = blockIdx.x * kRows, rn = min(kRows, n - r0);
+    double s = 0.0, dummy = 0.0;
+    for (int t = threadIdx.x; t < rn; t += blockDim.x) {
+        double a = w[r0 + t], b = w[n + r0 + t];
+        s += a * a + b * b;
+    }
+    block_sum2(s, dummy);
+    if (threadIdx.x == 0) part[(int64_t)k * gridDim.x + blockIdx.x] = s;
+}
+
+__global__ void norm_finish(int nchunk, int count, const double *__restrict__ part,
+                            double *__restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    double s = 0.0;
+    for (int b = 0; b < nchunk; ++b) s += part[(int64_t)k * nchunk + b];
+    out[k] = sqrt(s);
+}
+
+// v_{j+1}[c] = W[k] / h_{j+1,j} (left zero when the norm is zero, as the
+// reference leaves the zero-filled column untouched); H(j+1, j) = norm.
+__global__ void normalize(int n, const int32_t *__restrict__ act, const double *__restrict__ nrm,
+                          const double *__restrict__ W, double *__restrict__ slab_next,
+                          double2 *__restrict__ Hcol, int hstride, int jrow) {
+    int k = blockIdx.y, c = act[k];
+    double s = nrm[k];
+    double inv = s != 0.0 ? 1.0 / s : 0.0;
+    const double *w = W + (int64_t)k * 2 * n;
+    double *v = slab_next + (int64_t)c * 2 * n;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
+         r += (int64_t)gridDim.x * blockDim.x)
+        v[r] = s != 0.0 ? w[r] * inv : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) Hcol[(int64_t)c * hstride + jrow] = make_double2(s, 0.0);
+}
+
+// v_1 = b / ||b||; g_1 = ||b||.
+__global__ void start_vectors(int n, const int32_t *__restrict__ act, const double *__restrict__ nrm,
+                              const double *__restrict__ B, double *__restrict__ slab0,
+                              double2 *__restrict__ g, int gstride) {
+    int k = blockIdx.y, c = act[k];
+    double s = nrm[k];
+    const double *b = B + (int64_t)c * 2 * n;
+    double *v = slab0 + (int64_t)c * 2 * n;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
+         r += (int64_t)gridDim.x * blockDim.x)
+        v[r] = b[r] * (1.0 / s);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        g[(int64_t)c * gstride] = make_double2(s, 0.0);
+        for (int i = 1; i < gstride; ++i) g[(int64_t)c * gstride + i] = make_double2(0.0, 0.0);
+    }
+}
+
+__device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
+
+__device__ __forceinline__ void zrot_(double2 &x, double2 &y, double c, double2 s) {
+    double2 nx = make_double2(c * x.x + (s.x * y.x - s.y * y.y), c * x.y + (s.x * y.y + s.y * y.x));
+    // y' = c y - conj(s) x
+    double2 ny = make_double2(c * y.x - (s.x * x.x + s.y * x.y), c * y.y - (s.x * x.y - s.y * x.x));
+    x = nx;
+    y = ny;
+}
+
+// Givens update of column j for every active column (one thread each).
+// Hcols[j] points to the slab of H column j ([C][hstride] complex).
+__global__ void givens(int count, int j, const int32_t *__restrict__ act,
+                       double2 *const *__restrict__ Hcols, int hstride, double *__restrict__ cs,
+                       double2 *__restrict__ sn, double2 *__restrict__ g, int gstride, int cstride,
+                       double *__restrict__ resid) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    int c = act[k];
+    double2 *h = Hcols[j] + (int64_t)c * hstride;
+    double *csc = cs + (int64_t)c * cstride;
+    double2 *snc = sn + (int64_t)c * cstride;
+    for (int i = 0; i < j; ++i) zrot_(h[i], h[i + 1], csc[i], snc[i]);
+    double2 ca = h[j], cb = h[j + 1];
+    double cj;
+    double2 sj;
+    if (cabs_(ca) == 0.0) {
+        cj = 0.0;
+        sj = make_double2(1.0, 0.0);
+    } else {
+        double aa = cabs_(ca), ab = cabs_(cb);
+        double scale = aa + ab;
+        double2 cas = make_double2(ca.x / scale, ca.y / scale), cbs = make_double2(cb.x / scale, cb.y / scale);
+        double t1 = cabs_(cas), t2 = cabs_(cbs);
+        double norm = scale * sqrt(t1 * t1 + t2 * t2);
+        double2 alpha = make_double2(ca.x / aa, ca.y / aa);
+        cj = aa / norm;
+        double2 s = cmul(alpha, cconj(cb));
+        sj = make_double2(s.x / norm, s.y / norm);
+    }
+    csc[j] = cj;
+    snc[j] = sj;
+    double2 *gc = g + (int64_t)c * gstride;
+    zrot_(gc[j], gc[j + 1], cj, sj);
+    zrot_(h[j], h[j + 1], cj, sj);
+    h[j + 1] = make_double2(0.0, 0.0);
+    resid[k] = cabs_(gc[j + 1]);
+}
+
+// y = R^{-1} g for the triangular R = H(0..j, 0..j) (ztrsv 'U','N','N'),
+// one thread per triggered column; y stored compactly [k][j+1].
+__global__ void tri_solve(int count, int j, const int32_t *__restrict__ act,
+                          double2 *const *__restrict__ Hcols, int hstride,
+                          const double2 *__restrict__ g, int gstride, double2 *__restrict__ y) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    int c = act[k];
+    int m = j + 1;
+    double2 *yk = y + (int64_t)k * m;
+    for (int i = 0; i < m; ++i) yk[i] = g[(int64_t)c * gstride + i];
+    for (int i = m - 1; i >= 0; --i) {
+        double2 rii = Hcols[i][(int64_t)c * hstride + i];
+        double d = rii.x * rii.x + rii.y * rii.y;
+        double2 v = yk[i];
+        yk[i] = make_double2((v.x * rii.x + v.y * rii.y) / d, (v.y * rii.x - v.x * rii.y) / d);
+        for (int l = 0; l < i; ++l) {
+            double2 rl = Hcols[i][(int64_t)c * hstride + l];
+            double2 p = cmul(rl, yk[i]);
+            yk[l].x -= p.x;
+            yk[l].y -= p.y;
+        }
+    }
+}
+
+// R[k] = B[c] - AX[k] with c = act[k]; in place into AX.
+__global__ void residual(int n, const int32_t *__restrict__ act, const double *__restrict__ B,
+                         double *__restrict__ AX) {
+    int k = blockIdx.y, c = act[k];
+    const double *b = B + (int64_t)c * 2 * n;
+    double *r = AX + (int64_t)k * 2 * n;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2LL * n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        r[t] = b[t] - r[t];
+}
+
+__global__ void gather_x(int n, const int32_t *__restrict__ act, const double *__restrict__ X,
+                         double *__restrict__ out) {
+    int k = blockIdx.y;
+    const double *src = X + (int64_t)act[k] * 2 * n;
+    double *dst = out + (int64_t)k * 2 * n;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
+         r += (int64_t)gridDim.x * blockDim.x)
+        dst[r] = src[r];
+}
+
+int grid_rows(int64_t n2) { return (int)std::min<int64_t>(n_blocks(n2, 256), 1024); }
+
+// combine() over at most kCombine basis vectors per launch (shared-memory bound).
+constexpr int kCombine = 1024;
+int64_t combine_chunked(cudaStream_t st, int n, int i0, int ni, int count, const int32_t *act,
+                        double *const *slabs, const double2 *h, double sign, double *Y, int by_col) {
+    int64_t launches = 0;
+    for (int c0 = 0; c0 < ni; c0 += kCombine) {
+        int cn = std::min(kCombine, ni - c0);
+        // h is [count][ni]; pass the row stride through a shifted view per chunk
+        combine<<<dim3(n_blocks(n, kThreads), count), kThreads, cn * sizeof(double2), st>>>(
+            n, i0 + c0, cn, ni, c0, act, slabs, h, sign, Y, by_col);
+        ++launches;
+    }
+    return launches;
+}
+
+}  // namespace
+
+// Norms ||v[k]|| of a compact batch (used for ||b|| and the true residual).
+static void batch_norms(plx_geom *g, int count, const double *V, DevArray<double> &part,
+                        DevArray<double> &out) {
+    plx_ctx *ctx = g->ctx;
+    const int n = g->n_var;
+    int nchunk = n_blocks(n, kRows);
+    norm_partial<<<dim3(nchunk, count), kThreads, 0, ctx->stream>>>(n, V, part.p);
+    norm_finish<<<n_blocks(count, 128), 128, 0, ctx->stream>>>(nchunk, count, part.p, out.p);
+    ctx->launches += 2;
+}
+
+void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
+                   GmresResult &res) {
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = g->n_var;
+    const int C = (int)rq.freq.size();
+    const int m = std::min(rq.m, n);
+    res.status.assign(C, PLX_OK);
+    res.steps.assign(C, 0);
+    res.trace.assign(rq.record_trace ? (size_t)C * m : 0, 0.0);
+    if (C == 0) return;
+    if (m < 1) throw Error(PLX_ERR_ARG, "GMRES dimension must be positive");
+
+    const int nchunk = n_blocks(n, kRows);
+    const int hstride = m + 1;   // rows of an H column (0..m)
+    DevArray<int32_t> d_act, d_freq_act, d_cols;
+    d_act.alloc(ctx, C);
+    d_freq_act.alloc(ctx, C);
+    d_cols.alloc(ctx, C);
+    DevArray<double> Xa, Wa, work, nrm_part, nrm;
+    Xa.alloc(ctx, (size_t)C * 2 * n);
+    Wa.alloc(ctx, (size_t)C * 2 * n);
+    work.alloc(ctx, (size_t)C * 2 * n);
+    nrm_part.alloc(ctx, (size_t)C * nchunk);
+    nrm.alloc(ctx, C);
+    DevArray<double> cs;
+    DevArray<double2> sn, gv, hbuf, part, ybuf;
+    cs.alloc(ctx, (size_t)C * m);
+    sn.alloc(ctx, (size_t)C * m);
+    gv.alloc(ctx, (size_t)C * hstride);
+    hbuf.alloc(ctx, (size_t)C * hstride);
+    ybuf.alloc(ctx, (size_t)C * hstride);
+    std::vector<DevArray<double>> slabs(m + 1);
+    std::vector<DevArray<double2>> hcols(m);
+    DevArray<double *> d_slabs;
+    DevArray<double2 *> d_hcols;
+    d_slabs.alloc(ctx, m + 1);
+    d_hcols.alloc(ctx, m);
+    std::vector<double *> h_slabs(m + 1, nullptr);
+    std::vector<double2 *> h_hcols(m, nullptr);
+    PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, st));
+
+    // active list: every column with ||b|| > 0 (the reference returns x = 0 otherwise)
+    std::vector<int32_t> act(C);
+    for (int c = 0; c < C; ++c) act[c] = c;
+    PLX_CHECK_CUDA(cudaMemcpyAsync(d_act.p, act.data(), C * 4, cudaMemcpyHostToDevice, st));
+    batch_norms(g, C, d_B, nrm_part, nrm);   // B is [C] in column order == compact order here
+    std::vector<double> bnorm(C);
+    PLX_CHECK_CUDA(cudaMemcpyAsync(bnorm.data(), nrm.p, C * 8, cudaMemcpyDeviceToHost, st));
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+    slabs[0].alloc(ctx, (size_t)C * 2 * n);
+    h_slabs[0] = slabs[0].p;
+    start_vectors<<<dim3(grid_rows(2LL * n), C), 256, 0, st>>>(n, d_act.p, nrm.p, d_B, slabs[0].p,
+                                                              gv.p, hstride);
+    ctx->launches++;
+    act.clear();
+    for (int c = 0; c < C; ++c) {
+        if (!std::isfinite(bnorm[c])) {
+            res.status[c] = PLX_ERR_NAN;
+        } else if (bnorm[c] > 0.0) {
+            act.push_back(c);
+        }
+    }
+    auto upload_active = [&]() {
+        std::vector<int32_t> fa(act.size());
+        for (size_t k = 0; k < act.size(); ++k) fa[k] = rq.freq[act[k]];
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_act.p, act.data(), act.size() * 4, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_freq_act.p, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, st));
+    };
+    upload_active();
+
+    std::vector<double> resid(C);
+    for (int j = 0; j < m && !act.empty(); ++j) {
+        const int na = (int)act.size();
+        // --- w = A v_j for every active column (one batched operator) -----------
+        gather_cols<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, h_slabs[j], Xa.p);
+        ctx->launches++;
+        OpBatch ob{na, d_freq_act.p};
+        apply_operator(g, ob, Xa.p, Wa.p, work.p, rq.on_the_fly);
+        // --- Arnoldi --------------------------------------------------------------
+        hcols[j].alloc(ctx, (size_t)C * hstride);
+        h_hcols[j] = hcols[j].p;
+        slabs[j + 1].alloc(ctx, (size_t)C * 2 * n);
+        h_slabs[j + 1] = slabs[j + 1].p;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p + j + 1, &h_slabs[j + 1], sizeof(double *),
+                                       cudaMemcpyHostToDevice, st));
+        if (j == 0)
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p, &h_slabs[0], sizeof(double *), cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_hcols.p + j, &h_hcols[j], sizeof(double2 *),
+                                       cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemsetAsync(hcols[j].p, 0, (size_t)C * hstride * 16, st));
+        size_t need = (size_t)na * nchunk * (j + 1);
+        if (part.n < need) part.alloc(ctx, std::max(need, part.n * 2));
+        const size_t smem_dots = 2 * kRows * sizeof(double);
+        auto project = [&](int i0, int i1, int accumulate) {
+            int ni = i1 - i0;
+            dots_partial<<<dim3(nchunk, na), kThreads, smem_dots, st>>>(n, i0, i1, d_act.p, d_slabs.p,
+                                                                         Wa.p, part.p);
+            dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st>>>(nchunk, ni, i0, d_act.p, part.p,
+                                                                      hbuf.p, hcols[j].p, hstride,
+                                                                      accumulate);
+            ctx->launches += 2 + combine_chunked(st, n, i0, ni, na, d_act.p, d_slabs.p, hbuf.p, -1.0, Wa.p, 0);
+        };
+        if (j + 1 < 25) {
+            for (int i = 0; i <= j; ++i) project(i, i + 1, 0);        // modified Gram-Schmidt
+        } else {
+            project(0, j + 1, 0);                                     // classical GS ...
+            project(0, j + 1, 1);                                     // ... and re-orthogonalise
+        }
+        batch_norms(g, na, Wa.p, nrm_part, nrm);
+        normalize<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, nrm.p, Wa.p, slabs[j + 1].p,
+                                                               hcols[j].p, hstride, j + 1);
+        givens<<<n_blocks(na, 128), 128, 0, st>>>(na, j, d_act.p, d_hcols.p, hstride, cs.p, sn.p, gv.p,
+                                                 hstride, m, nrm.p);
+        ctx->launches += 2;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        PLX_CHECK_CUDA(cudaMemcpyAsync(resid.data(), nrm.p, na * 8, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        // --- convergence test -----------------------------------------------------
+        std::vector<int32_t> trig;
+        std::vector<int> trig_k;
+        for (int k = 0; k < na; ++k) {
+            int c = act[k];
+            res.steps[c] = j + 1;
+            if (rq.record_trace) res.trace[(size_t)c * m + j] = resid[k];
+            if (!std::isfinite(resid[k])) res.status[c] = PLX_ERR_NAN;
+            else if (resid[k] < rq.tol) trig.push_back(c);
+        }
+        std::vector<char> done(C, 0);
+        for (int c : act)
+            if (res.status[c] == PLX_ERR_NAN) done[c] = 1;
+        if (!trig.empty()) {
+            const int nt = (int)trig.size();
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
+            tri_solve<<<n_blocks(nt, 64), 64, 0, st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p, hstride,
+                                                       ybuf.p);
+            ctx->launches += combine_chunked(st, n, 0, j + 1, nt, d_cols.p, d_slabs.p, ybuf.p, 1.0, d_X, 1);
+            gather_x<<<dim3(grid_rows(2LL * n), nt), 256, 0, st>>>(n, d_cols.p, d_X, Xa.p);
+            ctx->launches += 2;
+            std::vector<int32_t> tf(nt);
+            for (int t = 0; t < nt; ++t) tf[t] = rq.freq[trig[t]];
+            DevArray<int32_t> d_tf;
+            d_tf.alloc(ctx, nt);
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_tf.p, tf.data(), nt * 4, cudaMemcpyHostToDevice, st));
+            OpBatch tb{nt, d_tf.p};
+            apply_operator(g, tb, Xa.p, Wa.p, work.p, rq.on_the_fly);
+            residual<<<dim3(grid_rows(2LL * n), nt), 256, 0, st>>>(n, d_cols.p, d_B, Wa.p);
+            ctx->launches++;
+            batch_norms(g, nt, Wa.p, nrm_part, nrm);
+            std::vector<double> tres(nt);
+            PLX_CHECK_CUDA(cudaMemcpyAsync(tres.data(), nrm.p, nt * 8, cudaMemcpyDeviceToHost, st));
+            PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+            for (int t = 0; t < nt; ++t)
+                if (tres[t] < rq.tol) done[trig[t]] = 1;
+                else if (!std::isfinite(tres[t])) {
+                    res.status[trig[t]] = PLX_ERR_NAN;
+                    done[trig[t]] = 1;
+                }
+        }
+        std::vector<int32_t> keep;
+        for (int c : act)
+            if (!done[c]) keep.push_back(c);
+        if (keep.size() != act.size()) {
+            act.swap(keep);
+            if (!act.empty()) upload_active();
+        }
+    }
+    for (int c : act) res.status[c] = PLX_ERR_NOT_CONVERGED;
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace plx

@@ -1,0 +1,484 @@
+// The frequency-dependent operator A(w) = blockdiag(Kop(w), I) T + D(w) and
+// the right-hand sides, for batches of columns (one frequency per column).
+//
+// Reference: product_matrix_vector_{wfq,wfqfmu} (wfq_module.f90:321-348,
+// wfqfmu_module.f90:584-626) = T x (product_q_block_x / product_mu_block_x,
+// matrix_module.f90:727-1001), then the charge rows through (K - P) or
+// 1/2 (K + H(w)) (update_y_q, matrix_module.f90:1011-1098), dipole rows copied
+// (update_y_mu, :1107-1125), then new_gmres_diagonal_shift.
+#include <algorithm>
+
+#include "pair_tiles.cuh"
+#include "plx_internal.h"
+
+namespace plx {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// S^T = X^T T for few rows (R = 2 * columns <= 16): split-K streaming of T.
+// ---------------------------------------------------------------------------
+constexpr int kSkinnyCols = 256;
+constexpr int kSkinnyK = 32;
+
+template <int R>
+__global__ void __launch_bounds__(kSkinnyCols) skinny_partial(int n, int kchunk,
+                                                              const double *__restrict__ Xt,
+                                                              const double *__restrict__ T,
+                                                              double *__restrict__ part) {
+    __shared__ double xs[kSkinnyK][R];
+    int col = blockIdx.x * kSkinnyCols + threadIdx.x;
+    int k0 = blockIdx.y * kchunk;
+    int k1 = min(n, k0 + kchunk);
+    double acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = 0.0;
+    for (int kb = k0; kb < k1; kb += kSkinnyK) {
+        int kn = min(kSkinnyK, k1 - kb);
+        __syncthreads();
+        for (int e = threadIdx.x; e < kSkinnyK * R; e += kSkinnyCols) {
+            int r = e / kSkinnyK, kk = e % kSkinnyK;
+            xs[kk][r] = (kk < kn) ? Xt[(int64_t)r * n + kb + kk] : 0.0;
+        }
+        __syncthreads();
+        if (col < n) {
+            const double *Tp = T + (int64_t)kb * n + col;
+            for (int kk = 0; kk < kn; ++kk) {
+                double t = __ldg(Tp + (int64_t)kk * n);
+#pragma unroll
+                for (int r = 0; r < R; ++r) acc[r] = fma(xs[kk][r], t, acc[r]);
+            }
+        }
+    }
+    if (col < n) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) part[((int64_t)blockIdx.y * R + r) * n + col] = acc[r];
+    }
+}
+
+__global__ void skinny_reduce(int n, int R, int ks, const double *__restrict__ part,
+                              double *__restrict__ S) {
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)R * n) return;
+    double s = 0.0;
+    for (int k = 0; k < ks; ++k) s += part[(int64_t)k * R * n + idx];
+    S[idx] = s;
+}
+
+// ---------------------------------------------------------------------------
+// S^T = X^T T, tiled (R > 16): 64 x 64 output tiles, 4 x 4 per thread, split
+// over K in the SAME chunks as skinny_partial and reduced by skinny_reduce, so
+// every output element is accumulated in the same order whatever the number of
+// columns in the batch: a column's result does not depend on the batch it is in.
+// ---------------------------------------------------------------------------
+constexpr int BM = 64, BN = 64, BK = 16;
+
+__global__ void __launch_bounds__(256) tiled_partial(int R, int n, int kchunk,
+                                                     const double *__restrict__ Xt,
+                                                     const double *__restrict__ T,
+                                                     double *__restrict__ part) {
+    __shared__ double As[BK][BM + 1];
+    __shared__ double Bs[BK][BN];
+    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+    int kbeg = blockIdx.z * kchunk, kend = min(n, kbeg + kchunk);
+    double acc[4][4] = {};
+    for (int k0 = kbeg; k0 < kend; k0 += BK) {
+        for (int e = threadIdx.x; e < BM * BK; e += 256) {
+            int r = e / BK, k = e % BK;
+            int gr = row0 + r, gk = k0 + k;
+            As[k][r] = (gr < R && gk < kend) ? Xt[(int64_t)gr * n + gk] : 0.0;
+        }
+        for (int e = threadIdx.x; e < BK * BN; e += 256) {
+            int k = e / BN, c = e % BN;
+            int gk = k0 + k, gc = col0 + c;
+            Bs[k][c] = (gk < kend && gc < n) ? T[(int64_t)gk * n + gc] : 0.0;
+        }
+        __syncthreads();
+        int kn = min(BK, kend - k0);
+        for (int k = 0; k < kn; ++k) {
+            double a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u] = As[k][ty * 4 + u];
+                b[u] = Bs[k][tx + 16 * u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        int gr = row0 + ty * 4 + u;
+        if (gr >= R) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            int gc = col0 + tx + 16 * v;
+            if (gc < n) part[((int64_t)blockIdx.z * R + gr) * n + gc] = acc[u][v];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// S = T X generated on the fly (matrix-free), CB columns per launch.
+// One thread per target atom; source atoms staged in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kOtfThreads = 128;
+
+template <int CB, bool FMU>
+__global__ void __launch_bounds__(kOtfThreads) otf_contract(int N, int count, int nv,
+                                                            const double *__restrict__ pos,
+                                                            const double *__restrict__ par,
+                                                            const double *__restrict__ X,
+                                                            double *__restrict__ S) {
+    constexpr int NC = FMU ? 4 : 1;            // components per atom
+    __shared__ double sp[kOtfThreads][5];       // x, y, z, r_q, r_mu
+    __shared__ double sxv[kOtfThreads][NC * 2 * CB];
+    int i = blockIdx.x * kOtfThreads + threadIdx.x;
+    bool live = i < N;
+    double xi = 0, yi = 0, zi = 0, rqi = 1, rmi = 1, etai = 0;
+    if (live) {
+        xi = pos[i];
+        yi = pos[N + i];
+        zi = pos[2 * N + i];
+        rqi = par[i];
+        rmi = par[N + i];
+        etai = par[2 * N + i];
+    }
+    double acc[NC][2][CB];
+#pragma unroll
+    for (int a = 0; a < NC; ++a)
+#pragma unroll
+        for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int c = 0; c < CB; ++c) acc[a][p][c] = 0.0;
+    for (int j0 = 0; j0 < N; j0 += kOtfThreads) {
+        int j = j0 + threadIdx.x;
+        __syncthreads();
+        if (j < N) {
+            sp[threadIdx.x][0] = pos[j];
+            sp[threadIdx.x][1] = pos[N + j];
+            sp[threadIdx.x][2] = pos[2 * N + j];
+            sp[threadIdx.x][3] = par[j];
+            sp[threadIdx.x][4] = par[N + j];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const double *xc = X + (int64_t)c * 2 * nv;
+                for (int p = 0; p < 2; ++p) {
+                    sxv[threadIdx.x][(0 * 2 + p) * CB + c] = (c < count) ? xc[p * nv + j] : 0.0;
+                    if (FMU)
+                        for (int k = 0; k < 3; ++k)
+                            sxv[threadIdx.x][((1 + k) * 2 + p) * CB + c] =
+                                (c < count) ? xc[p * nv + N + 3 * j + k] : 0.0;
+                }
+            }
+        }
+        __syncthreads();
+        if (!live) continue;
+        int jn = min(kOtfThreads, N - j0);
+        for (int t = 0; t < jn; ++t) {
+            int jj = j0 + t;
+            const double *xv = sxv[t];
+            if (jj == i) {
+#pragma unroll
+                for (int p = 0; p < 2; ++p)
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) acc[0][p][c] = fma(etai, xv[p * CB + c], acc[0][p][c]);
+                continue;
+            }
+            double dx = xi - sp[t][0], dy = yi - sp[t][1], dz = zi - sp[t][2];
+            if (!FMU) {
+                double q = plx_pair_qq(dx, dy, dz, rqi, sp[t][3]);
+#pragma unroll
+                for (int p = 0; p < 2; ++p)
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) acc[0][p][c] = fma(q, xv[p * CB + c], acc[0][p][c]);
+                continue;
+            }
+            PairTile tl;
+            plx_pair_tile(dx, dy, dz, rqi, rmi, sp[t][3], sp[t][4], tl);
+#pragma unroll
+            for (int p = 0; p < 2; ++p)
+#pragma unroll
+                for (int c = 0; c < CB; ++c) {
+                    double xq = xv[(0 * 2 + p) * CB + c];
+                    double m0 = xv[(1 * 2 + p) * CB + c];
+                    double m1 = xv[(2 * 2 + p) * CB + c];
+                    double m2 = xv[(3 * 2 + p) * CB + c];
+                    acc[0][p][c] += tl.qq * xq + tl.qm[0] * m0 + tl.qm[1] * m1 + tl.qm[2] * m2;
+                    acc[1][p][c] += tl.mq[0] * xq + tl.mm[0] * m0 + tl.mm[1] * m1 + tl.mm[2] * m2;
+                    acc[2][p][c] += tl.mq[1] * xq + tl.mm[1] * m0 + tl.mm[3] * m1 + tl.mm[4] * m2;
+                    acc[3][p][c] += tl.mq[2] * xq + tl.mm[2] * m0 + tl.mm[4] * m1 + tl.mm[5] * m2;
+                }
+        }
+    }
+    if (!live) return;
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+        if (c >= count) break;
+        double *sc = S + (int64_t)c * 2 * nv;
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            sc[p * nv + i] = acc[0][p][c];
+            if (FMU)
+                for (int k = 0; k < 3; ++k) sc[p * nv + N + 3 * i + k] = acc[1 + k][p][c];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Charge rows: y_i = sum_j c_ij (s_j - s_i), c_ij = K_ij (one atom type) or
+// 1/2 (K_ij + (w_tj/w_ti) K_ji) (several types), then + D_q(w) x_i.
+// One warp per (row, column).
+// ---------------------------------------------------------------------------
+__global__ void charge_rows(int N, int nt, int nv, int count, int hetero,
+                            const int32_t *__restrict__ freq, const int32_t *__restrict__ type,
+                            const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                            const double *__restrict__ kval, const double *__restrict__ ktval,
+                            const Cplx *__restrict__ wratio, const Cplx *__restrict__ dq,
+                            const double *__restrict__ S, const double *__restrict__ X,
+                            double *__restrict__ Y, double sign, int add_diag) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int c = blockIdx.y;
+    int i = warp;
+    if (i >= N || c >= count) return;
+    int f = freq[c];
+    const double *sr = S + (int64_t)c * 2 * nv;
+    const double *si = sr + nv;
+    double s_re = sr[i], s_im = si[i];
+    int ti = type[i];
+    double yre = 0.0, yim = 0.0;
+    for (int e = rowptr[i] + lane; e < rowptr[i + 1]; e += 32) {
+        int j = col[e];
+        double dre = sr[j] - s_re, dim = si[j] - s_im;
+        if (!hetero) {
+            double k = kval[e];
+            yre = fma(k, dre, yre);
+            yim = fma(k, dim, yim);
+        } else {
+            Cplx w = wratio[ti + nt * type[j] + (int64_t)nt * nt * f];
+            double kt = ktval[e];
+            double cre = 0.5 * (kval[e] + w.re * kt), cim = 0.5 * (w.im * kt);
+            yre += cre * dre - cim * dim;
+            yim += cre * dim + cim * dre;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        yre += __shfl_xor_sync(0xffffffffu, yre, o);
+        yim += __shfl_xor_sync(0xffffffffu, yim, o);
+    }
+    if (lane == 0) {
+        yre *= sign;
+        yim *= sign;
+        if (add_diag) {
+            Cplx d = dq[ti + nt * f];
+            double xr = X[(int64_t)c * 2 * nv + i], xi = X[(int64_t)c * 2 * nv + nv + i];
+            yre += d.re * xr - d.im * xi;
+            yim += d.re * xi + d.im * xr;
+        }
+        Y[(int64_t)c * 2 * nv + i] = yre;
+        Y[(int64_t)c * 2 * nv + nv + i] = yim;
+    }
+}
+
+// Dipole rows: y = s + (sum_t f_t,i / alpha_t(w)) x.
+__global__ void dipole_rows(int N, int nt, int nv, int count, const int32_t *__restrict__ freq,
+                            const double *__restrict__ frac, const Cplx *__restrict__ inv_alpha,
+                            const double *__restrict__ S, const double *__restrict__ X,
+                            double *__restrict__ Y) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int c = blockIdx.y;
+    if (e >= 3LL * N || c >= count) return;
+    int i = (int)(e / 3);
+    int f = freq[c];
+    double zre = 0.0, zim = 0.0;
+    for (int t = 0; t < nt; ++t) {
+        double fr = frac[t + (int64_t)nt * i];
+        Cplx a = inv_alpha[t + nt * f];
+        zre += fr * a.re;
+        zim += fr * a.im;
+    }
+    int64_t r = N + e;
+    const double *sc = S + (int64_t)c * 2 * nv;
+    const double *xc = X + (int64_t)c * 2 * nv;
+    double xr = xc[r], xi = xc[nv + r];
+    Y[(int64_t)c * 2 * nv + r] = sc[r] + zre * xr - zim * xi;
+    Y[(int64_t)c * 2 * nv + nv + r] = sc[nv + r] + zre * xi + zim * xr;
+}
+
+// Static potential V_i (field along pol) for the right-hand side.
+__global__ void potential_kernel(int N, int nv, int count, const int32_t *__restrict__ pol,
+                                 const double *__restrict__ pos, double e0, int use_min,
+                                 double mx, double my, double mz, double *__restrict__ V) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = blockIdx.y;
+    if (i >= nv || c >= count) return;
+    double v = 0.0;
+    if (i < N) {
+        int p = pol[c];
+        double x = pos[(int64_t)p * N + i];
+        double m = p == 0 ? mx : (p == 1 ? my : mz);
+        v = use_min ? -e0 * fabs(x - m) : -e0 * x;
+    }
+    V[(int64_t)c * 2 * nv + i] = v;
+    V[(int64_t)c * 2 * nv + nv + i] = 0.0;
+}
+
+// Dipole part of the right-hand side: E0 on the polarisation component.
+__global__ void rhs_dipole(int N, int nv, int count, const int32_t *__restrict__ pol, double e0,
+                           double *__restrict__ B) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int c = blockIdx.y;
+    if (e >= 3LL * N || c >= count) return;
+    int k = (int)(e % 3);
+    B[(int64_t)c * 2 * nv + N + e] = (k == pol[c]) ? e0 : 0.0;
+    B[(int64_t)c * 2 * nv + nv + N + e] = 0.0;
+}
+
+}  // namespace
+
+void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on_the_fly);
+
+void prof_begin(plx_ctx *ctx) {
+    if (!ctx->profile) return;
+    if (ctx->prof_used + 2 > ctx->prof_events.size()) {
+        for (int k = 0; k < 2; ++k) {
+            cudaEvent_t e;
+            PLX_CHECK_CUDA(cudaEventCreate(&e));
+            ctx->prof_events.push_back(e);
+        }
+    }
+    PLX_CHECK_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used], ctx->stream));
+}
+
+void prof_end(plx_ctx *ctx, double flops, double bytes) {
+    if (!ctx->profile) return;
+    PLX_CHECK_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used + 1], ctx->stream));
+    ctx->prof_used += 2;
+    ctx->prof_flops += flops;
+    ctx->prof_bytes += bytes;
+    ctx->prof_launches += 1;
+}
+
+void contract_t(plx_geom *g, int count, const double *X, double *S, bool on_the_fly) {
+    plx_ctx *ctx = g->ctx;
+    const double nn = (double)g->n_var;
+    prof_begin(ctx);
+    contract_t_impl(g, count, X, S, on_the_fly);
+    // algorithmic: 2 n^2 flops per real column; T once (stored mode) + columns in/out
+    prof_end(ctx, 2.0 * nn * nn * 2.0 * count, (on_the_fly ? 0.0 : 8.0 * nn * nn) + 2.0 * 8.0 * nn * 2.0 * count);
+}
+
+void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on_the_fly) {
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = g->n_var;
+    const int R = 2 * count;
+    if (on_the_fly) {
+        const bool fmu = g->model == PLX_WFQFMU;
+        for (int c0 = 0; c0 < count; c0 += 4) {
+            int cb = std::min(4, count - c0);
+            const double *Xc = X + (int64_t)c0 * 2 * n;
+            double *Sc = S + (int64_t)c0 * 2 * n;
+            int blocks = n_blocks(g->n_atoms, kOtfThreads);
+            if (fmu)
+                otf_contract<4, true><<<blocks, kOtfThreads, 0, st>>>(g->n_atoms, cb, n, g->d_pos.p,
+                                                                     g->d_par.p, Xc, Sc);
+            else
+                otf_contract<4, false><<<blocks, kOtfThreads, 0, st>>>(g->n_atoms, cb, n, g->d_pos.p,
+                                                                      g->d_par.p, Xc, Sc);
+            ctx->launches++;
+        }
+        PLX_CHECK_CUDA(cudaGetLastError());
+        return;
+    }
+    if (!g->has_T) throw Error(PLX_ERR_ARG, "geometry was created without the dense T matrix");
+    // K split: depends on n only (not on the batch), see tiled_partial
+    const int cb = n_blocks(n, kSkinnyCols);
+    int ks = std::max(1, std::min(64, (592 + cb - 1) / cb));
+    const int kchunk = (n + ks - 1) / ks;
+    ks = (n + kchunk - 1) / kchunk;
+    size_t need = (size_t)ks * R * n;
+    if (g->d_part.n < need) g->d_part.alloc(ctx, need);
+    double *part = g->d_part.p;
+    if (R <= 16) {
+        dim3 grid(cb, ks);
+        switch (R) {
+#define PLX_SK(RR) \
+    case RR: skinny_partial<RR><<<grid, kSkinnyCols, 0, st>>>(n, kchunk, X, g->d_T.p, part); break;
+            PLX_SK(2) PLX_SK(4) PLX_SK(6) PLX_SK(8) PLX_SK(10) PLX_SK(12) PLX_SK(14) PLX_SK(16)
+#undef PLX_SK
+            default: throw Error(PLX_ERR_ARG, "bad skinny row count");
+        }
+    } else {
+        dim3 grid(n_blocks(n, BN), n_blocks(R, BM), ks);
+        tiled_partial<<<grid, 256, 0, st>>>(R, n, kchunk, X, g->d_T.p, part);
+    }
+    skinny_reduce<<<n_blocks((int64_t)R * n, 256), 256, 0, st>>>(n, R, ks, part, S);
+    ctx->launches += 2;
+    PLX_CHECK_CUDA(cudaGetLastError());
+}
+
+static void finish_rows(plx_geom *g, const OpBatch &b, const double *S, const double *X,
+                        double *Y) {
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int N = g->n_atoms, nv = g->n_var;
+    dim3 gq(n_blocks((int64_t)N * 32, 256), b.count);
+    charge_rows<<<gq, 256, 0, st>>>(N, g->n_types, nv, b.count, g->n_types > 1, b.d_freq,
+                                    g->d_type.p, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
+                                    g->d_ktval.p, g->d_wratio.p, g->d_dq.p, S, X, Y, 1.0, 1);
+    ctx->launches++;
+    if (g->model == PLX_WFQFMU) {
+        dim3 gm(n_blocks(3LL * N, 256), b.count);
+        dipole_rows<<<gm, 256, 0, st>>>(N, g->n_types, nv, b.count, b.d_freq, g->d_frac.p,
+                                        g->d_inv_alpha.p, S, X, Y);
+        ctx->launches++;
+    }
+    PLX_CHECK_CUDA(cudaGetLastError());
+}
+
+void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, double *work,
+                    bool on_the_fly) {
+    if (b.count == 0) return;
+    contract_t(g, b.count, X, work, on_the_fly);
+    finish_rows(g, b, work, X, Y);
+}
+
+void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout) {
+    if (b.count == 0) return;
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int N = g->n_atoms, nv = g->n_var;
+    double mn[3] = {0, 0, 0};
+    if (g->rhs_potential) {
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = g->coord[k];
+            for (int i = 0; i < N; ++i) mn[k] = std::min(mn[k], g->coord[k + 3 * i]);
+        }
+    }
+    DevArray<double> V;
+    V.alloc(ctx, (size_t)b.count * 2 * nv);
+    potential_kernel<<<dim3(n_blocks(nv, 256), b.count), 256, 0, st>>>(
+        N, nv, b.count, d_pol, g->d_pos.p, g->e0, g->rhs_potential, mn[0], mn[1], mn[2], V.p);
+    dim3 gq(n_blocks((int64_t)N * 32, 256), b.count);
+    // b_q = -Kop(w) V  (rhs_module.f90:140-390); no diagonal term
+    charge_rows<<<gq, 256, 0, st>>>(N, g->n_types, nv, b.count, g->n_types > 1, b.d_freq,
+                                    g->d_type.p, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
+                                    g->d_ktval.p, g->d_wratio.p, g->d_dq.p, V.p, V.p, Bout, -1.0, 0);
+    ctx->launches += 2;
+    if (g->model == PLX_WFQFMU) {
+        dim3 gm(n_blocks(3LL * N, 256), b.count);
+        rhs_dipole<<<gm, 256, 0, st>>>(N, nv, b.count, d_pol, g->e0, Bout);
+        ctx->launches++;
+    }
+    PLX_CHECK_CUDA(cudaGetLastError());
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace plx

@@ -1,0 +1,179 @@
+// Internal declarations shared by the plasmonx_b200 CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/plasmonx_b200.h"
+
+#define PLX_CHECK_CUDA(call)                                                   \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) {                                               \
+            throw plx::Error(PLX_ERR_CUDA, std::string(#call) + ": " +         \
+                                               cudaGetErrorString(e_));        \
+        }                                                                      \
+    } while (0)
+
+namespace plx {
+
+struct Error {
+    plx_status code;
+    std::string msg;
+    Error(plx_status c, std::string m) : code(c), msg(std::move(m)) {}
+};
+
+// Vectors of complex unknowns are stored "split": the n real parts followed by
+// the n imaginary parts.  A batch of C vectors [C][2][n] is then a row-major
+// (2C x n) real matrix, which is the operand layout of the T contraction.
+struct Cplx {
+    double re, im;
+};
+
+// ---------------------------------------------------------------------------
+// device memory accounting
+// ---------------------------------------------------------------------------
+void *dev_alloc(plx_ctx *ctx, size_t bytes);
+void dev_free(plx_ctx *ctx, void *p, size_t bytes);
+
+template <typename T>
+struct DevArray {
+    plx_ctx *ctx = nullptr;
+    T *p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray &) = delete;
+    DevArray &operator=(const DevArray &) = delete;
+    ~DevArray() { release(); }
+    void alloc(plx_ctx *c, size_t count) {
+        release();
+        ctx = c;
+        n = count;
+        p = count ? static_cast<T *>(dev_alloc(c, count * sizeof(T))) : nullptr;
+    }
+    void release() {
+        if (p) dev_free(ctx, p, n * sizeof(T));
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace plx
+
+struct plx_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    std::string last_error;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t launches = 0;  // kernels launched by the library since creation
+    // contraction profiling (plx_profile_enable)
+    bool profile = false;
+    std::vector<cudaEvent_t> prof_events;   // pairs (start, stop), reused
+    size_t prof_used = 0;                   // events in use
+    double prof_flops = 0.0, prof_bytes = 0.0;
+    int64_t prof_launches = 0;
+};
+
+struct plx_geom {
+    plx_ctx *ctx = nullptr;
+    int model = 0;
+    int n_atoms = 0, n_types = 0, n_var = 0;
+    int rhs_potential = 0;
+    double e0 = 0.0;
+    // host copies of the description
+    std::vector<double> coord;          // 3 x N
+    std::vector<int32_t> atom_type;     // N
+    std::vector<double> frac;           // n_types x N neighbour fractions
+    std::vector<double> eta, r_q, r_mu, tau, density, a_ij;  // per type
+    std::vector<double> fermi_d, fermi_s, r0;                // type pair
+    // device: per-atom data
+    plx::DevArray<double> d_pos;        // [4][N]: x, y, z, unused
+    plx::DevArray<int32_t> d_type;      // N
+    plx::DevArray<double> d_par;        // [4][N]: r_q, r_mu, eta, a_ij of the atom's type
+    plx::DevArray<double> d_frac;       // n_types x N
+    // device: conductance K in CSR (off-diagonal entries with K_ij or K_ji != 0)
+    plx::DevArray<int32_t> d_rowptr;    // N + 1
+    plx::DevArray<int32_t> d_col;       // nnz
+    plx::DevArray<double> d_kval;       // nnz: K_ij
+    plx::DevArray<double> d_ktval;      // nnz: K_ji
+    int64_t nnz = 0;
+    // device: dense interaction matrix T (n_var x n_var, symmetric, row-major)
+    plx::DevArray<double> d_T;
+    bool has_T = false;
+    // frequencies
+    int n_freq = 0;
+    std::vector<double> omega;                 // n_freq
+    std::vector<plx::Cplx> alpha_w;            // n_types x n_freq
+    plx::DevArray<plx::Cplx> d_dq;             // n_types x n_freq: charge diagonal -z(w)
+    plx::DevArray<plx::Cplx> d_inv_alpha;      // n_types x n_freq: 1 / alpha_t(w)
+    plx::DevArray<plx::Cplx> d_wratio;         // n_types x n_types x n_freq: w_tj / w_ti
+    // split-K partial sums of the few-column contraction (grown on demand;
+    // used only by work ordered on the context's single stream)
+    plx::DevArray<double> d_part;
+    // timing of the last plx_solve
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+};
+
+namespace plx {
+
+// Column descriptor of a batched operator application: which frequency the
+// column belongs to.
+struct OpBatch {
+    int count = 0;            // number of columns
+    const int32_t *d_freq;    // device, [count]: frequency index of each column
+};
+
+// geometry.cu
+void build_conductance(plx_geom *g);
+void build_dense_t(plx_geom *g);
+void upload_frequency_tables(plx_geom *g);
+
+// operator.cu
+//   Y = A(w_c) X for a batch: X, Y are [count][2][n_var] split-complex, device.
+//   work must hold 2*count*n_var doubles.
+void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, double *work,
+                    bool on_the_fly);
+//   S = T X (no K, no diagonal), S and X as above.
+void contract_t(plx_geom *g, int count, const double *X, double *S, bool on_the_fly);
+void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout);
+
+// inversion.cu
+// d_vars: [count][2][n] right-hand sides in, solutions of A(w_i) x = b out.
+void solve_inversion_cols(plx_geom *g, int i_freq, int count, double *d_vars);
+
+// gmres.cu
+struct GmresRequest {
+    std::vector<int32_t> freq, pol;   // per column
+    int m = 0;                        // Krylov dimension
+    double tol = 0.0;                 // absolute
+    bool on_the_fly = false;
+    bool record_trace = false;
+};
+struct GmresResult {
+    std::vector<int32_t> status, steps;
+    std::vector<double> trace;        // [col][m]
+};
+// B and X are [C][2][n] device arrays; X receives the solutions.
+void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
+                   GmresResult &res);
+
+// observables.cu
+void polar_batch(plx_geom *g, int count, const int32_t *d_pol, const double *X,
+                 Cplx *d_polar /* [count][3] : alpha(a, pol_c) */);
+
+// Brackets a contraction with profiling events when profiling is enabled.
+void prof_begin(plx_ctx *ctx);
+void prof_end(plx_ctx *ctx, double flops, double bytes);
+
+inline int n_blocks(int64_t work, int per_block) {
+    int64_t b = (work + per_block - 1) / per_block;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace plx
