@@ -58,9 +58,15 @@ typedef enum {
 } plx_mode;
 
 typedef enum {
-    PLX_FP64 = 0,               /* plain complex FP64, the drop-in */
-    PLX_MIXED_BF16X3 = 1        /* tensor-core contraction (split BF16, FP32
-                                   accumulate) inside FP64 iterative refinement */
+    PLX_FP64 = 0,               /* plain complex FP64 GMRES, the drop-in (the
+                                   reference's algorithm step by step) */
+    PLX_MIXED_BF16X3 = 1,       /* FP64 iterative refinement around an inner
+                                   GMRES whose T contraction runs on the tensor
+                                   cores with BF16-split operands (3 products,
+                                   FP32 accumulation) */
+    PLX_FP64_REFINED = 2,       /* the same refinement with an FP64 inner solve:
+                                   restarted, with explicit FP64 residuals */
+    PLX_MIXED_BF16 = 3          /* refinement with a single BF16 product inside */
 } plx_precision;
 
 /* Geometry and model parameters, i.e. what the reference holds in `target_`
@@ -99,6 +105,12 @@ typedef struct {
                                    by sqrt(n_var) as input_module.f90:250-251 does */
     int32_t freq_block;         /* frequencies solved together; 0 = automatic */
     int32_t record_trace;       /* 1: fill trace_out with the logged residuals */
+    /* refinement (precision != PLX_FP64): inner Krylov dimension, inner
+     * relative tolerance, maximum outer steps; 0 selects the defaults
+     * (64, 1e-4, 60) */
+    int32_t inner_krylov;
+    double inner_tol;
+    int32_t max_outer;
 } plx_solve_desc;
 
 /* ---- context --------------------------------------------------------------- */
@@ -179,6 +191,14 @@ plx_status plx_complex_inversion(plx_geom *geom, int32_t i_freq, double *variabl
 plx_status plx_solve(plx_geom *geom, const plx_solve_desc *desc, double *x_out,
                      double *polar_out, double *results_out, int32_t *status_out,
                      int32_t *steps_out, double *trace_out);
+
+/* S = T X for `count` real columns (X, S: count x n_var, each column
+ * contiguous), the frequency-independent contraction inside
+ * product_q_block_x / product_mu_block_x (matrix_module.f90:727-1001).
+ * how: 0 stored T in FP64, 1 tiles generated on the fly in FP64, 2 tensor
+ * cores with BF16-split operands (3 products), 3 tensor cores, one BF16
+ * product. */
+plx_status plx_contract(plx_geom *geom, int32_t count, const double *X, double *S, int32_t how);
 
 /* Device time (ms, CUDA events on the library's stream) of the last plx_solve,
  * and the number of kernels it launched. */

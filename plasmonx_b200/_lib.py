@@ -14,13 +14,14 @@ STATUS = {0: 'PLX_OK', 1: 'PLX_ERR_ARG', 2: 'PLX_ERR_CUDA', 3: 'PLX_ERR_NOMEM', 
           5: 'PLX_ERR_NOT_CONVERGED', 6: 'PLX_ERR_NAN', 7: 'PLX_ERR_SINGULAR', 8: 'PLX_ERR_UNSUPPORTED'}
 MODEL = {'wfq': 0, 'wfqfmu': 1}
 MODE = {'inversion': 0, 'iterative': 1, 'iterative on the fly': 2}
-PRECISION = {'fp64': 0, 'mixed_bf16x3': 1}
+PRECISION = {'fp64': 0, 'mixed_bf16x3': 1, 'fp64_refined': 2, 'mixed_bf16': 3}
+CONTRACT = {'fp64': 0, 'fp64_otf': 1, 'bf16x3': 2, 'bf16': 3}
 
 EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes_in_use',
            'plx_geometry_create', 'plx_geometry_destroy', 'plx_geometry_n_var', 'plx_geometry_k_nnz',
            'plx_set_frequencies', 'plx_matvec', 'plx_rhs', 'plx_gmres_solver', 'plx_complex_inversion',
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
-           'plx_profile_read']
+           'plx_profile_read', 'plx_contract']
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -37,7 +38,8 @@ class GeometryDesc(C.Structure):
 class SolveDesc(C.Structure):
     _fields_ = [('mode', C.c_int32), ('precision', C.c_int32), ('pol_mask', C.c_int32),
                 ('max_krylov', C.c_int32), ('tol', C.c_double), ('freq_block', C.c_int32),
-                ('record_trace', C.c_int32)]
+                ('record_trace', C.c_int32), ('inner_krylov', C.c_int32), ('inner_tol', C.c_double),
+                ('max_outer', C.c_int32)]
 
 
 class PlxError(RuntimeError):
@@ -82,6 +84,7 @@ def load():
     lib.plx_last_solve_ms.argtypes = [vp]
     lib.plx_last_solve_launches.restype = C.c_int64
     lib.plx_last_solve_launches.argtypes = [vp]
+    lib.plx_contract.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int32]
     lib.plx_profile_enable.argtypes = [vp, C.c_int32]
     lib.plx_profile_read.argtypes = [vp, _dp, C.POINTER(C.c_int64), _dp, _dp]
     _lib = lib

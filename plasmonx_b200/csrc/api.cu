@@ -275,7 +275,7 @@ plx_status plx_matvec(plx_geom *g, int32_t i_freq, int32_t on_the_fly, const dou
         F.alloc(g->ctx, 1);
         PLX_CHECK_CUDA(cudaMemcpyAsync(F.p, &i_freq, 4, cudaMemcpyHostToDevice, g->ctx->stream));
         upload_vec(g->ctx, x, n, X.p);
-        apply_operator(g, OpBatch{1, F.p}, X.p, Y.p, W.p, on_the_fly != 0);
+        apply_operator(g, OpBatch{1, F.p}, X.p, Y.p, W.p, on_the_fly ? Contraction::FP64_OTF : Contraction::FP64);
         download_vec(g->ctx, Y.p, n, y);
     });
 }
@@ -325,7 +325,7 @@ plx_status plx_gmres_solver(plx_geom *g, int32_t i_freq, double *x, int32_t on_t
         rq.pol = {0};
         rq.m = restart;
         rq.tol = tol;
-        rq.on_the_fly = on_the_fly != 0;
+        rq.contraction = on_the_fly ? Contraction::FP64_OTF : Contraction::FP64;
         rq.record_trace = trace_out != nullptr;
         GmresResult res;
         gmres_batched(g, rq, B.p, X.p, res);
@@ -362,9 +362,12 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
         cudaStream_t st = ctx->stream;
         if (g->n_freq < 1) throw Error(PLX_ERR_ARG, "no frequencies set");
         if (desc->mode < PLX_INVERSION || desc->mode > PLX_GMRES_OTF) throw Error(PLX_ERR_ARG, "bad mode");
-        if (desc->precision != PLX_FP64)
-            throw Error(PLX_ERR_UNSUPPORTED, "this entry point solves in FP64; use the mixed-precision solver");
+        if (desc->precision < PLX_FP64 || desc->precision > PLX_MIXED_BF16)
+            throw Error(PLX_ERR_ARG, "bad precision");
         const bool otf = desc->mode == PLX_GMRES_OTF;
+        const bool refined = desc->precision != PLX_FP64 && desc->mode != PLX_INVERSION;
+        if (refined && otf && desc->precision != PLX_FP64_REFINED)
+            throw Error(PLX_ERR_UNSUPPORTED, "tensor-core refinement needs the stored T (on-memory mode)");
         if (!otf && !g->has_T) throw Error(PLX_ERR_ARG, "this mode needs the stored T (store_t at creation)");
         const int n = g->n_var, F = g->n_freq;
         std::vector<int32_t> pols;
@@ -455,10 +458,28 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
                     ctx->launches++;
                     rq.m = m;
                     rq.tol = desc->tol;
-                    rq.on_the_fly = otf;
-                    rq.record_trace = desc->record_trace && trace_out;
+                    rq.contraction = otf ? Contraction::FP64_OTF : Contraction::FP64;
+                    rq.record_trace = desc->record_trace && trace_out && !refined;
                     GmresResult res;
-                    gmres_batched(g, rq, Bg.p, Xg.p, res);
+                    if (refined) {
+                        RefineRequest rr;
+                        rr.freq = rq.freq;
+                        rr.pol = rq.pol;
+                        rr.tol = desc->tol;
+                        rr.inner_m = desc->inner_krylov > 0 ? std::min(desc->inner_krylov, n) : std::min(64, n);
+                        rr.inner_rel = desc->inner_tol > 0 ? desc->inner_tol : 1e-4;
+                        rr.max_outer = desc->max_outer > 0 ? desc->max_outer : 60;
+                        rr.outer_contraction = otf ? Contraction::FP64_OTF : Contraction::FP64;
+                        rr.inner_contraction = desc->precision == PLX_MIXED_BF16X3 ? Contraction::TC3
+                                               : desc->precision == PLX_MIXED_BF16 ? Contraction::TC1
+                                                                                   : rr.outer_contraction;
+                        RefineResult rres;
+                        solve_refined(g, rr, Bg.p, Xg.p, rres);
+                        res.status = rres.status;
+                        res.steps = rres.inner_steps;
+                    } else {
+                        gmres_batched(g, rq, Bg.p, Xg.p, res);
+                    }
                     copy_cols<<<dim3(gr, G), 256, 0, st>>>(n, ddst.p, dsel.p, Xg.p, X.p);
                     ctx->launches++;
                     for (int k = 0; k < G; ++k) {
@@ -546,6 +567,28 @@ plx_status plx_profile_read(plx_ctx *ctx, double *ms, int64_t *launches, double 
         if (launches) *launches = ctx->prof_launches;
         if (flops) *flops = ctx->prof_flops;
         if (bytes) *bytes = ctx->prof_bytes;
+    });
+}
+
+plx_status plx_contract(plx_geom *g, int32_t count, const double *X, double *S, int32_t how) {
+    if (!g || !X || !S) return PLX_ERR_ARG;
+    return guarded(g->ctx, [&] {
+        set_device(g->ctx);
+        if (count < 1 || how < 0 || how > 3) throw Error(PLX_ERR_ARG, "bad column count or contraction kind");
+        const int n = g->n_var;
+        // [count][n] real columns == [count/2][2][n] split-complex columns; an odd
+        // count is padded with one zero column
+        const int padded = count + (count & 1);
+        DevArray<double> dX, dS;
+        dX.alloc(g->ctx, (size_t)padded * n);
+        dS.alloc(g->ctx, (size_t)padded * n);
+        PLX_CHECK_CUDA(cudaMemsetAsync(dX.p, 0, (size_t)padded * n * 8, g->ctx->stream));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(dX.p, X, (size_t)count * n * 8, cudaMemcpyHostToDevice, g->ctx->stream));
+        const Contraction kinds[4] = {Contraction::FP64, Contraction::FP64_OTF, Contraction::TC3, Contraction::TC1};
+        contract_t(g, padded / 2, dX.p, dS.p, kinds[how]);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(S, dS.p, (size_t)count * n * 8, cudaMemcpyDeviceToHost, g->ctx->stream));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+        if (how >= 2 && tc_error(g)) throw Error(PLX_ERR_CUDA, "tensor-core contraction timed out");
     });
 }
 

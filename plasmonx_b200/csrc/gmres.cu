@@ -417,7 +417,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         gather_cols<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, h_slabs[j], Xa.p);
         ctx->launches++;
         OpBatch ob{na, d_freq_act.p};
-        apply_operator(g, ob, Xa.p, Wa.p, work.p, rq.on_the_fly);
+        apply_operator(g, ob, Xa.p, Wa.p, work.p, rq.contraction);
         // --- Arnoldi --------------------------------------------------------------
         hcols[j].alloc(ctx, (size_t)C * hstride);
         h_hcols[j] = hcols[j].p;
@@ -464,13 +464,25 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
             int c = act[k];
             res.steps[c] = j + 1;
             if (rq.record_trace) res.trace[(size_t)c * m + j] = resid[k];
+            const double tc = rq.tols.empty() ? rq.tol : rq.tols[c];
             if (!std::isfinite(resid[k])) res.status[c] = PLX_ERR_NAN;
-            else if (resid[k] < rq.tol) trig.push_back(c);
+            else if (resid[k] < tc || (rq.inner && j == m - 1)) trig.push_back(c);
         }
         std::vector<char> done(C, 0);
         for (int c : act)
             if (res.status[c] == PLX_ERR_NAN) done[c] = 1;
-        if (!trig.empty()) {
+        if (!trig.empty() && rq.inner) {
+            // inner solve of a refinement: take the least-squares solution as is
+            const int nt = (int)trig.size();
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
+            tri_solve<<<n_blocks(nt, 64), 64, 0, st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p, hstride,
+                                                       ybuf.p);
+            ctx->launches += 1 + combine_chunked(st, n, 0, j + 1, nt, d_cols.p, d_slabs.p, ybuf.p, 1.0, d_X, 1);
+            for (int c : trig) done[c] = 1;
+            for (int c : trig)
+                if (resid[std::find(act.begin(), act.end(), c) - act.begin()] >= (rq.tols.empty() ? rq.tol : rq.tols[c]))
+                    res.status[c] = PLX_ERR_NOT_CONVERGED;   // inner dimension used up (not an error)
+        } else if (!trig.empty()) {
             const int nt = (int)trig.size();
             PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
             tri_solve<<<n_blocks(nt, 64), 64, 0, st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p, hstride,
@@ -484,7 +496,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
             d_tf.alloc(ctx, nt);
             PLX_CHECK_CUDA(cudaMemcpyAsync(d_tf.p, tf.data(), nt * 4, cudaMemcpyHostToDevice, st));
             OpBatch tb{nt, d_tf.p};
-            apply_operator(g, tb, Xa.p, Wa.p, work.p, rq.on_the_fly);
+            apply_operator(g, tb, Xa.p, Wa.p, work.p, Contraction::FP64 == rq.contraction || Contraction::FP64_OTF == rq.contraction ? rq.contraction : Contraction::FP64);
             residual<<<dim3(grid_rows(2LL * n), nt), 256, 0, st>>>(n, d_cols.p, d_B, Wa.p);
             ctx->launches++;
             batch_norms(g, nt, Wa.p, nrm_part, nrm);

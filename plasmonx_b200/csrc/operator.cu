@@ -365,13 +365,23 @@ void prof_end(plx_ctx *ctx, double flops, double bytes) {
     ctx->prof_launches += 1;
 }
 
-void contract_t(plx_geom *g, int count, const double *X, double *S, bool on_the_fly) {
+void contract_t(plx_geom *g, int count, const double *X, double *S, Contraction how) {
     plx_ctx *ctx = g->ctx;
     const double nn = (double)g->n_var;
+    const bool otf = how == Contraction::FP64_OTF;
     prof_begin(ctx);
-    contract_t_impl(g, count, X, S, on_the_fly);
-    // algorithmic: 2 n^2 flops per real column; T once (stored mode) + columns in/out
-    prof_end(ctx, 2.0 * nn * nn * 2.0 * count, (on_the_fly ? 0.0 : 8.0 * nn * nn) + 2.0 * 8.0 * nn * 2.0 * count);
+    // algorithmic: 2 n^2 flops per real column (one product, whatever the
+    // emulation); bytes: the stored T once at its storage precision, plus the
+    // columns in and out
+    double tbytes = 0.0;
+    if (how == Contraction::TC3 || how == Contraction::TC1) {
+        tc_contract(g, count, X, S, how == Contraction::TC3 ? 3 : 1);
+        tbytes = (how == Contraction::TC3 ? 4.0 : 2.0) * nn * (double)g->ldk;
+    } else {
+        contract_t_impl(g, count, X, S, otf);
+        tbytes = otf ? 0.0 : 8.0 * nn * nn;
+    }
+    prof_end(ctx, 2.0 * nn * nn * 2.0 * count, tbytes + 2.0 * 8.0 * nn * 2.0 * count);
 }
 
 void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on_the_fly) {
@@ -444,9 +454,9 @@ static void finish_rows(plx_geom *g, const OpBatch &b, const double *S, const do
 }
 
 void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, double *work,
-                    bool on_the_fly) {
+                    Contraction how) {
     if (b.count == 0) return;
-    contract_t(g, b.count, X, work, on_the_fly);
+    contract_t(g, b.count, X, work, how);
     finish_rows(g, b, work, X, Y);
 }
 

@@ -112,6 +112,12 @@ struct plx_geom {
     plx::DevArray<plx::Cplx> d_dq;             // n_types x n_freq: charge diagonal -z(w)
     plx::DevArray<plx::Cplx> d_inv_alpha;      // n_types x n_freq: 1 / alpha_t(w)
     plx::DevArray<plx::Cplx> d_wratio;         // n_types x n_types x n_freq: w_tj / w_ti
+    // mixed precision: T split into BF16 high / low parts ([n_var][ldk], k padded
+    // to a multiple of 64 with zeros), the matching split of the input columns,
+    // and the error word of the tensor-core kernel
+    plx::DevArray<uint16_t> d_Th, d_Tl, d_Xh, d_Xl;
+    int64_t ldk = 0;
+    plx::DevArray<int> d_tc_err;
     // split-K partial sums of the few-column contraction (grown on demand;
     // used only by work ordered on the context's single stream)
     plx::DevArray<double> d_part;
@@ -121,6 +127,14 @@ struct plx_geom {
 };
 
 namespace plx {
+
+// How the T contraction of an operator application is computed.
+enum class Contraction : int {
+    FP64 = 0,       // stored T, FP64 on the CUDA cores
+    FP64_OTF = 1,   // tiles generated in the kernel, FP64
+    TC3 = 2,        // stored T split in BF16 high/low, 3 tensor-core products
+    TC1 = 3         // stored T rounded to BF16, 1 tensor-core product
+};
 
 // Column descriptor of a batched operator application: which frequency the
 // column belongs to.
@@ -138,10 +152,16 @@ void upload_frequency_tables(plx_geom *g);
 //   Y = A(w_c) X for a batch: X, Y are [count][2][n_var] split-complex, device.
 //   work must hold 2*count*n_var doubles.
 void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, double *work,
-                    bool on_the_fly);
+                    Contraction how);
 //   S = T X (no K, no diagonal), S and X as above.
-void contract_t(plx_geom *g, int count, const double *X, double *S, bool on_the_fly);
+void contract_t(plx_geom *g, int count, const double *X, double *S, Contraction how);
 void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout);
+
+// tc_contract.cu: S = T X with BF16-split operands on the tensor cores
+// (nprod 3: Th Xh + Th Xl + Tl Xh; nprod 1: Th Xh).  X, S: [count][2][n] FP64.
+void build_t_split(plx_geom *g);
+void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod);
+int tc_error(plx_geom *g);   // non-zero when a tensor-core CTA gave up waiting
 
 // inversion.cu
 // d_vars: [count][2][n] right-hand sides in, solutions of A(w_i) x = b out.
@@ -152,8 +172,13 @@ struct GmresRequest {
     std::vector<int32_t> freq, pol;   // per column
     int m = 0;                        // Krylov dimension
     double tol = 0.0;                 // absolute
-    bool on_the_fly = false;
+    std::vector<double> tols;         // per-column absolute tolerance (overrides tol)
+    Contraction contraction = Contraction::FP64;
     bool record_trace = false;
+    // inner solve of iterative refinement: the least-squares solution is taken
+    // when the residual estimate passes the tolerance or at the last step, with
+    // no true-residual check (the caller forms the FP64 residual)
+    bool inner = false;
 };
 struct GmresResult {
     std::vector<int32_t> status, steps;
@@ -162,6 +187,24 @@ struct GmresResult {
 // B and X are [C][2][n] device arrays; X receives the solutions.
 void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
                    GmresResult &res);
+
+// refine.cu: iterative refinement -- FP64 residuals r = b - A x outside, an
+// inner GMRES of dimension inner_m with `inner` contraction on A d = r to a
+// relative tolerance inner_rel, x += d; stops when ||r|| < tol (absolute).
+struct RefineRequest {
+    std::vector<int32_t> freq, pol;
+    double tol = 0.0;
+    int inner_m = 64;
+    double inner_rel = 1e-5;
+    int max_outer = 50;
+    Contraction inner_contraction = Contraction::TC3;
+    Contraction outer_contraction = Contraction::FP64;
+};
+struct RefineResult {
+    std::vector<int32_t> status, inner_steps, outer;
+    std::vector<double> residual;     // final ||b - A x||
+};
+void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, double *d_X, RefineResult &res);
 
 // observables.cu
 void polar_batch(plx_geom *g, int count, const int32_t *d_pol, const double *X,

@@ -1,0 +1,396 @@
+// Tensor-core T contraction for the mixed-precision solve (sm_100a, tcgen05).
+//
+// S = T X for a batch of R real columns, with T (n x n, symmetric) and X split
+// into BF16 high and low parts, T = Th + Tl, X = Xh + Xl, and
+//     S = Th Xh + Th Xl + Tl Xh        (FP32 accumulation in tensor memory),
+// i.e. every product carries ~16 significant bits of each operand; the dropped
+// Tl Xl term is below 2^-16 of the result.  The result is written as FP64 so the
+// rest of the operator (conductance rows, frequency diagonal) stays unchanged.
+//
+// GEMM mapping (all operands K-major, the layout tcgen05 reads natively):
+//   A = T   rows m of T, contiguous along k         (M = n_var)
+//   B = X^T column c of X, contiguous along k        (N = R real columns)
+//   D = TMEM accumulator 128 x BN (FP32), lane = row m, column = c
+// One CTA computes a 128 x BN tile of S; 4 warps: thread 0 issues the TMA
+// loads, thread 32 issues the MMAs, all 128 threads drain TMEM in the
+// epilogue.  Operand tiles are 64 elements (128 bytes) deep along k and are
+// loaded by TMA with the 128-byte swizzle that the UMMA descriptors describe.
+// Every wait on an mbarrier is bounded; a CTA that gives up records an error
+// code, waits (bounded) for its outstanding loads, frees its tensor memory and
+// returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "plx_internal.h"
+
+namespace plx {
+
+namespace {
+
+constexpr int kBM = 128;          // rows of T per CTA (TMEM lanes)
+constexpr int kBK = 64;           // k per stage (128 bytes of BF16)
+constexpr int kUmmaK = 16;        // k per tcgen05.mma (kind::f16)
+constexpr uint32_t kSpinLimit = 1u << 22;   // bounded waits (seconds at most)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: returns false (and records `code`) when the limit is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+    for (uint32_t it = 0; it < kSpinLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicCAS(err, 0, code);
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *bar, void *dst, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major operand with the 128-byte swizzle:
+// 8-row x 128-byte swizzle atoms stacked every 1024 bytes (stride byte offset),
+// leading byte offset 16 bytes (unused for this layout), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw128(const void *smem) {
+    uint64_t addr = smem_u32(smem);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;           // start address, bits [0,14)
+    d |= (uint64_t)(16 >> 4) << 16;         // leading byte offset, bits [16,30)
+    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset, bits [32,46)
+    d |= (uint64_t)1 << 46;                 // version, bits [46,48)
+    d |= (uint64_t)2 << 61;                 // layout: 128-byte swizzle
+    return d;
+}
+
+// Instruction descriptor, kind::f16: BF16 x BF16 -> FP32, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4)                        // D format F32
+           | (1u << 7)                      // A format BF16
+           | (1u << 10)                     // B format BF16
+           | ((uint32_t)(N >> 3) << 17)     // N / 8
+           | ((uint32_t)(M >> 4) << 24);    // M / 16
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+template <int BN, int STAGES>
+struct TcSmem {
+    static constexpr int kA = kBM * kBK * 2;      // bytes of one A operand tile
+    static constexpr int kB = BN * kBK * 2;       // bytes of one B operand tile
+    static constexpr int kStage = 2 * kA + 2 * kB;
+    static constexpr int kBytes = STAGES * kStage + 1024 /* align */ + 256 /* barriers */;
+};
+
+template <int BN>
+constexpr int tc_stages() {
+    return std::min(4, (200 * 1024) / TcSmem<BN, 1>::kStage);
+}
+
+template <int BN, int STAGES, int NPROD>
+__global__ void __launch_bounds__(128, 1)
+    tc_contract_kernel(const __grid_constant__ CUtensorMap mapTh, const __grid_constant__ CUtensorMap mapTl,
+                       const __grid_constant__ CUtensorMap mapXh, const __grid_constant__ CUtensorMap mapXl,
+                       int M, int R, int ktiles, double *__restrict__ S, int ldS, int *__restrict__ err) {
+    using L = TcSmem<BN, STAGES>;
+    constexpr uint32_t kTmemCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * L::kStage);
+    uint64_t *empty = full + STAGES;
+    uint64_t *done = empty + STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = blockIdx.x * BN;
+    const int m0 = blockIdx.y * kBM;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    auto stage_ptr = [&](int s, int which) -> uint8_t * {
+        // which: 0 Th, 1 Tl, 2 Xh, 3 Xl
+        uint8_t *st = base + s * L::kStage;
+        return which < 2 ? st + which * L::kA : st + 2 * L::kA + (which - 2) * L::kB;
+    };
+
+    if (threadIdx.x == 0) {
+        // ---------------- TMA producer ----------------
+        int issued = 0;
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int s = kt % STAGES;
+            if (kt >= STAGES) {
+                if (!mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1, err, 1) || *abort_flag) {
+                    *abort_flag = 1;
+                    break;
+                }
+            }
+            mbar_expect_tx(&full[s], (uint32_t)L::kStage);
+            const int kx = kt * kBK;
+            tma_load_2d(&mapTh, &full[s], stage_ptr(s, 0), kx, m0);
+            tma_load_2d(&mapTl, &full[s], stage_ptr(s, 1), kx, m0);
+            tma_load_2d(&mapXh, &full[s], stage_ptr(s, 2), kx, n0);
+            tma_load_2d(&mapXl, &full[s], stage_ptr(s, 3), kx, n0);
+            issued = kt + 1;
+        }
+        if (*abort_flag) {
+            // let the loads already issued land before the CTA can exit
+            for (int kt = std::max(0, issued - STAGES); kt < issued; ++kt)
+                mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, nullptr, 0);
+        }
+    } else if (threadIdx.x == 32) {
+        // ---------------- MMA issuer ----------------
+        constexpr uint32_t idesc = umma_idesc_bf16(kBM, BN);
+        bool ok = true;
+        for (int kt = 0; kt < ktiles && ok; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(&full[s], (kt / STAGES) & 1, err, 2) || *abort_flag) {
+                *abort_flag = 1;
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t dTh = umma_desc_sw128(stage_ptr(s, 0));
+            const uint64_t dTl = umma_desc_sw128(stage_ptr(s, 1));
+            const uint64_t dXh = umma_desc_sw128(stage_ptr(s, 2));
+            const uint64_t dXl = umma_desc_sw128(stage_ptr(s, 3));
+#pragma unroll
+            for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
+                // advance 16 elements = 32 bytes = 2 descriptor units along k
+                const uint64_t off = (uint64_t)(kk * kUmmaK * 2) >> 4;
+                const uint32_t acc0 = (kt > 0 || kk > 0) ? 1u : 0u;
+                umma_bf16(tmem, dTh + off, dXh + off, idesc, acc0);
+                if (NPROD > 1) {
+                    umma_bf16(tmem, dTh + off, dXl + off, idesc, 1u);
+                    umma_bf16(tmem, dTl + off, dXh + off, idesc, 1u);
+                }
+            }
+            umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(done);
+    }
+    __syncwarp();
+
+    // ---------------- epilogue: TMEM -> S (FP64) ----------------
+    bool have = mbar_wait(done, 0, err, 3) && !*abort_flag;
+    have = __all_sync(0xffffffffu, have);     // tcgen05.ld below is warp-collective
+    if (!have) *abort_flag = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (have) {
+        const int row = m0 + warp * 32 + lane;
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                  "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                  "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int c = n0 + c0 + j;
+                    if (c < R) S[(int64_t)c * ldS + row] = (double)__uint_as_float(v[j]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// FP64 -> (BF16 high, BF16 low) split of a row-major [rows][cols] array into a
+// zero-padded [rows_pad][ld] pair.
+__global__ void split_bf16(int rows, int cols, int64_t ld_in, const double *__restrict__ in, int rows_pad,
+                           int64_t ld_out, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+    int64_t total = (int64_t)rows_pad * ld_out;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = e / ld_out, c = e % ld_out;
+        float x = (r < rows && c < cols) ? (float)in[r * ld_in + c] : 0.0f;
+        __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi[e] = h;
+        lo[e] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        PLX_CHECK_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess) throw Error(PLX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 2-D BF16 tensor [outer][inner] with leading dimension ld (elements), boxes of
+// (64 inner x box_outer), 128-byte swizzle, zero fill out of bounds.
+CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t ld, uint32_t box_outer) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {ld * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, box_outer};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(PLX_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return m;
+}
+
+template <int BN, int NPROD>
+void launch_bn(plx_geom *g, int R, const CUtensorMap &th, const CUtensorMap &tl, const CUtensorMap &xh,
+               const CUtensorMap &xl, int ktiles, double *S, int *err) {
+    constexpr int ST = tc_stages<BN>();
+    using L = TcSmem<BN, ST>;
+    auto kern = tc_contract_kernel<BN, ST, NPROD>;
+    static bool attr = false;
+    if (!attr) {
+        PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
+        attr = true;
+    }
+    dim3 grid((R + BN - 1) / BN, (g->n_var + kBM - 1) / kBM);
+    kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, g->n_var, R, ktiles, S, g->n_var, err);
+    g->ctx->launches++;
+    PLX_CHECK_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void build_t_split(plx_geom *g) {
+    if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
+    if (g->d_Th.p) return;
+    const int64_t n = g->n_var;
+    const int64_t ld = (n + kBK - 1) / kBK * kBK;
+    g->ldk = ld;
+    g->d_Th.alloc(g->ctx, (size_t)(n * ld));
+    g->d_Tl.alloc(g->ctx, (size_t)(n * ld));
+    split_bf16<<<2048, 256, 0, g->ctx->stream>>>((int)n, (int)n, n, g->d_T.p, (int)n, ld,
+                                                 reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p),
+                                                 reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p));
+    g->ctx->launches++;
+    PLX_CHECK_CUDA(cudaGetLastError());
+    g->d_tc_err.alloc(g->ctx, 1);
+    PLX_CHECK_CUDA(cudaMemsetAsync(g->d_tc_err.p, 0, sizeof(int), g->ctx->stream));
+}
+
+void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod) {
+    build_t_split(g);
+    plx_ctx *ctx = g->ctx;
+    const int n = g->n_var;
+    const int R = 2 * count;
+    const int64_t ld = g->ldk;
+    // column tiles: as few as possible, each a multiple of 32 columns (<= 256)
+    const int ntile = (R + 255) / 256;
+    int bn = ((R + ntile - 1) / ntile + 31) / 32 * 32;
+    const int Rpad = ntile * bn;
+    size_t need = (size_t)Rpad * ld;
+    if (g->d_Xh.n < need) {
+        g->d_Xh.alloc(ctx, need);
+        g->d_Xl.alloc(ctx, need);
+    }
+    split_bf16<<<std::min<int64_t>(4096, n_blocks((int64_t)Rpad * ld, 256)), 256, 0, ctx->stream>>>(
+        R, n, n, X, Rpad, ld, reinterpret_cast<__nv_bfloat16 *>(g->d_Xh.p),
+        reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
+    ctx->launches++;
+    CUtensorMap th = make_map(g->d_Th.p, ld, n, ld, kBM);
+    CUtensorMap tl = make_map(g->d_Tl.p, ld, n, ld, kBM);
+    CUtensorMap xh = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
+    CUtensorMap xl = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
+    const int ktiles = (int)(ld / kBK);
+    int *err = g->d_tc_err.p;
+#define PLX_TC(BNV)                                                                       \
+    case BNV:                                                                             \
+        if (nprod == 1) launch_bn<BNV, 1>(g, R, th, tl, xh, xl, ktiles, S, err);           \
+        else launch_bn<BNV, 3>(g, R, th, tl, xh, xl, ktiles, S, err);                      \
+        break;
+    switch (bn) {
+        PLX_TC(32) PLX_TC(64) PLX_TC(96) PLX_TC(128) PLX_TC(160) PLX_TC(192) PLX_TC(224) PLX_TC(256)
+        default: throw Error(PLX_ERR_ARG, "bad column tile");
+    }
+#undef PLX_TC
+}
+
+int tc_error(plx_geom *g) {
+    if (!g->d_tc_err.p) return 0;
+    int h = 0;
+    PLX_CHECK_CUDA(cudaMemcpyAsync(&h, g->d_tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, g->ctx->stream));
+    PLX_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return h;
+}
+
+}  // namespace plx

@@ -136,15 +136,23 @@ class Solver:
         return buf.T.copy()
 
     # ---- the spectrum -------------------------------------------------------
+    def contract(self, X, how='fp64'):
+        """S = T X for real columns X (count x n_var)."""
+        X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, self.n_var)
+        S = np.zeros_like(X)
+        self.ctx.check(self.lib.plx_contract(self.g, X.shape[0], ptr(X), ptr(S), _lib.CONTRACT[how]))
+        return S
+
     def solve(self, mode=None, precision='fp64', pol_mask=None, tol=None, max_krylov=None,
-              freq_block=0, want_x=False, trace=False):
+              freq_block=0, want_x=False, trace=False, inner_krylov=0, inner_tol=0.0, max_outer=0):
         p = self.prob
         mode = mode or p.method
         pol_mask = p.pol_mask if pol_mask is None else pol_mask
         F = len(self.freqs)
         m = int(max_krylov or p.gmres_dim or 1000)
         desc = _lib.SolveDesc(_lib.MODE[mode], _lib.PRECISION[precision], pol_mask, m,
-                              float(p.tol if tol is None else tol), int(freq_block), int(bool(trace)))
+                              float(p.tol if tol is None else tol), int(freq_block), int(bool(trace)),
+                              int(inner_krylov), float(inner_tol), int(max_outer))
         x = np.zeros((F, 3, self.n_var), dtype=np.complex128) if want_x else None
         polar = np.zeros((F, 3, 3), dtype=np.complex128)
         res = np.zeros((F, 20))
