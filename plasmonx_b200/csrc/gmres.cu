@@ -71,38 +71,61 @@ __global__ void gather_cols(int n, const int32_t *__restrict__ act, const double
         dst[r] = src[r];
 }
 
-// Partial complex dots conj(V_i[c]) . W[k] for i in [i0, i1), rows of one chunk.
-// One warp per basis vector; W chunk staged in shared memory.
+// Partial complex dots conj(V_i[c]) . W[k] for i in [i0, i1) over one chunk of
+// kDotRows rows: every thread keeps kDotPT entries of W in registers and all
+// eight warps work on every basis vector (warp reduction, then a fixed-order
+// sum over the warps), so the kernel is bandwidth-bound for any number of
+// basis vectors, including the single-vector projections of modified
+// Gram-Schmidt.
+constexpr int kDotPT = 4;
+constexpr int kDotRows = kThreads * kDotPT;
+
 __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
                                                          const int32_t *__restrict__ act,
                                                          double *const *__restrict__ slabs,
                                                          const double *__restrict__ W,
                                                          double2 *__restrict__ part) {
-    extern __shared__ double sw[];   // [2][kRows]
-    int k = blockIdx.y, c = act[k];
-    int r0 = blockIdx.x * kRows;
-    int rn = min(kRows, n - r0);
+    __shared__ double2 red[kThreads / 32][32];
+    const int k = blockIdx.y, c = act[k];
+    const int r0 = blockIdx.x * kDotRows;
     const double *wr = W + (int64_t)k * 2 * n;
-    for (int t = threadIdx.x; t < rn; t += blockDim.x) {
-        sw[t] = wr[r0 + t];
-        sw[kRows + t] = wr[n + r0 + t];
+    double wre[kDotPT], wim[kDotPT];
+#pragma unroll
+    for (int q = 0; q < kDotPT; ++q) {
+        int r = r0 + threadIdx.x + kThreads * q;
+        wre[q] = r < n ? wr[r] : 0.0;
+        wim[q] = r < n ? wr[n + r] : 0.0;
     }
-    __syncthreads();
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int nw = blockDim.x >> 5;
-    int ni = i1 - i0;
-    for (int ii = warp; ii < ni; ii += nw) {
-        const double *v = slabs[i0 + ii] + (int64_t)c * 2 * n;
-        double re = 0.0, im = 0.0;
-        for (int t = lane; t < rn; t += 32) {
-            double vr = v[r0 + t], vi = v[n + r0 + t];
-            double xr = sw[t], xi = sw[kRows + t];
-            re += vr * xr + vi * xi;       // conj(v) * w
-            im += vr * xi - vi * xr;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ni = i1 - i0;
+    for (int g0 = 0; g0 < ni; g0 += 32) {
+        const int gn = min(32, ni - g0);
+        for (int t = 0; t < gn; ++t) {
+            const double *v = slabs[i0 + g0 + t] + (int64_t)c * 2 * n;
+            double re = 0.0, im = 0.0;
+#pragma unroll
+            for (int q = 0; q < kDotPT; ++q) {
+                int r = r0 + threadIdx.x + kThreads * q;
+                if (r < n) {
+                    double vr = v[r], vi = v[n + r];
+                    re += vr * wre[q] + vi * wim[q];      // conj(v) * w
+                    im += vr * wim[q] - vi * wre[q];
+                }
+            }
+            re = warp_sum(re);
+            im = warp_sum(im);
+            if (lane == 0) red[warp][t] = make_double2(re, im);
         }
-        re = warp_sum(re);
-        im = warp_sum(im);
-        if (lane == 0) part[((int64_t)k * gridDim.x + blockIdx.x) * ni + ii] = make_double2(re, im);
+        __syncthreads();
+        if (threadIdx.x < gn) {
+            double2 s = make_double2(0.0, 0.0);
+            for (int w = 0; w < kThreads / 32; ++w) {
+                s.x += red[w][threadIdx.x].x;
+                s.y += red[w][threadIdx.x].y;
+            }
+            part[((int64_t)k * gridDim.x + blockIdx.x) * ni + g0 + threadIdx.x] = s;
+        }
+        __syncthreads();
     }
 }
 
@@ -263,29 +286,35 @@ __global__ void givens(int count, int j, const int32_t *__restrict__ act,
     resid[k] = cabs_(gc[j + 1]);
 }
 
-// y = R^{-1} g for the triangular R = H(0..j, 0..j) (ztrsv 'U','N','N'),
-// one thread per triggered column; y stored compactly [k][j+1].
+// y = R^{-1} g for the triangular R = H(0..j, 0..j) (ztrsv 'U','N','N'): one
+// warp per triggered column, column-oriented back substitution with the
+// updates of y spread over the lanes; y stored compactly [k][j+1].
 __global__ void tri_solve(int count, int j, const int32_t *__restrict__ act,
                           double2 *const *__restrict__ Hcols, int hstride,
                           const double2 *__restrict__ g, int gstride, double2 *__restrict__ y) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ double2 ys[];
+    int k = blockIdx.x;
     if (k >= count) return;
     int c = act[k];
     int m = j + 1;
-    double2 *yk = y + (int64_t)k * m;
-    for (int i = 0; i < m; ++i) yk[i] = g[(int64_t)c * gstride + i];
+    for (int i = threadIdx.x; i < m; i += 32) ys[i] = g[(int64_t)c * gstride + i];
+    __syncwarp();
     for (int i = m - 1; i >= 0; --i) {
-        double2 rii = Hcols[i][(int64_t)c * hstride + i];
+        const double2 *col = Hcols[i] + (int64_t)c * hstride;
+        double2 rii = col[i];
         double d = rii.x * rii.x + rii.y * rii.y;
-        double2 v = yk[i];
-        yk[i] = make_double2((v.x * rii.x + v.y * rii.y) / d, (v.y * rii.x - v.x * rii.y) / d);
-        for (int l = 0; l < i; ++l) {
-            double2 rl = Hcols[i][(int64_t)c * hstride + l];
-            double2 p = cmul(rl, yk[i]);
-            yk[l].x -= p.x;
-            yk[l].y -= p.y;
+        double2 v = ys[i];
+        double2 yi = make_double2((v.x * rii.x + v.y * rii.y) / d, (v.y * rii.x - v.x * rii.y) / d);
+        __syncwarp();
+        if (threadIdx.x == 0) ys[i] = yi;
+        for (int l = threadIdx.x; l < i; l += 32) {
+            double2 p = cmul(col[l], yi);
+            ys[l].x -= p.x;
+            ys[l].y -= p.y;
         }
+        __syncwarp();
     }
+    for (int i = threadIdx.x; i < m; i += 32) y[(int64_t)k * m + i] = ys[i];
 }
 
 // R[k] = B[c] - AX[k] with c = act[k]; in place into AX.
@@ -307,6 +336,20 @@ __global__ void gather_x(int n, const int32_t *__restrict__ act, const double *_
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
          r += (int64_t)gridDim.x * blockDim.x)
         dst[r] = src[r];
+}
+
+// Y[k] *= P[idx[k]] elementwise (complex), or in place on the column itself
+// when by_col (Y indexed by idx[k]).
+__global__ void scale_cols(int n, const int32_t *__restrict__ idx, const double *__restrict__ P,
+                           double *__restrict__ Y, int by_col) {
+    int k = blockIdx.y, c = idx[k];
+    const double *p = P + (int64_t)c * 2 * n;
+    double *y = Y + (int64_t)(by_col ? c : k) * 2 * n;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double pr = p[r], pi = p[n + r], yr = y[r], yi = y[n + r];
+        y[r] = pr * yr - pi * yi;
+        y[n + r] = pr * yi + pi * yr;
+    }
 }
 
 int grid_rows(int64_t n2) { return (int)std::min<int64_t>(n_blocks(n2, 256), 1024); }
@@ -353,6 +396,14 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     if (m < 1) throw Error(PLX_ERR_ARG, "GMRES dimension must be positive");
 
     const int nchunk = n_blocks(n, kRows);
+    const int ndot = n_blocks(n, kDotRows);
+    if ((size_t)(m + 1) * sizeof(double2) > 200 * 1024) throw Error(PLX_ERR_ARG, "GMRES dimension above 12800");
+    static bool tri_attr = false;
+    if (!tri_attr) {
+        PLX_CHECK_CUDA(cudaFuncSetAttribute(tri_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        PLX_CHECK_CUDA(cudaFuncSetAttribute(combine, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        tri_attr = true;
+    }
     const int hstride = m + 1;   // rows of an H column (0..m)
     DevArray<int32_t> d_act, d_freq_act, d_cols;
     d_act.alloc(ctx, C);
@@ -380,6 +431,15 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     std::vector<double *> h_slabs(m + 1, nullptr);
     std::vector<double2 *> h_hcols(m, nullptr);
     PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, st));
+    DevArray<double> Pinv;
+    const bool jac = rq.jacobi && rq.inner;
+    if (jac) {
+        DevArray<int32_t> d_fall;
+        d_fall.alloc(ctx, C);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_fall.p, rq.freq.data(), C * 4, cudaMemcpyHostToDevice, st));
+        Pinv.alloc(ctx, (size_t)C * 2 * n);
+        diagonal_inverse(g, OpBatch{C, d_fall.p}, Pinv.p);
+    }
 
     // active list: every column with ||b|| > 0 (the reference returns x = 0 otherwise)
     std::vector<int32_t> act(C);
@@ -416,6 +476,10 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         // --- w = A v_j for every active column (one batched operator) -----------
         gather_cols<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, h_slabs[j], Xa.p);
         ctx->launches++;
+        if (jac) {
+            scale_cols<<<dim3(grid_rows(n), na), 256, 0, st>>>(n, d_act.p, Pinv.p, Xa.p, 0);
+            ctx->launches++;
+        }
         OpBatch ob{na, d_freq_act.p};
         apply_operator(g, ob, Xa.p, Wa.p, work.p, rq.contraction);
         // --- Arnoldi --------------------------------------------------------------
@@ -430,19 +494,17 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         PLX_CHECK_CUDA(cudaMemcpyAsync(d_hcols.p + j, &h_hcols[j], sizeof(double2 *),
                                        cudaMemcpyHostToDevice, st));
         PLX_CHECK_CUDA(cudaMemsetAsync(hcols[j].p, 0, (size_t)C * hstride * 16, st));
-        size_t need = (size_t)na * nchunk * (j + 1);
+        size_t need = (size_t)na * ndot * (j + 1);
         if (part.n < need) part.alloc(ctx, std::max(need, part.n * 2));
-        const size_t smem_dots = 2 * kRows * sizeof(double);
         auto project = [&](int i0, int i1, int accumulate) {
             int ni = i1 - i0;
-            dots_partial<<<dim3(nchunk, na), kThreads, smem_dots, st>>>(n, i0, i1, d_act.p, d_slabs.p,
-                                                                         Wa.p, part.p);
-            dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st>>>(nchunk, ni, i0, d_act.p, part.p,
+            dots_partial<<<dim3(ndot, na), kThreads, 0, st>>>(n, i0, i1, d_act.p, d_slabs.p, Wa.p, part.p);
+            dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st>>>(ndot, ni, i0, d_act.p, part.p,
                                                                       hbuf.p, hcols[j].p, hstride,
                                                                       accumulate);
             ctx->launches += 2 + combine_chunked(st, n, i0, ni, na, d_act.p, d_slabs.p, hbuf.p, -1.0, Wa.p, 0);
         };
-        if (j + 1 < 25) {
+        if (j + 1 < 25 && !rq.inner) {
             for (int i = 0; i <= j; ++i) project(i, i + 1, 0);        // modified Gram-Schmidt
         } else {
             project(0, j + 1, 0);                                     // classical GS ...
@@ -475,9 +537,13 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
             // inner solve of a refinement: take the least-squares solution as is
             const int nt = (int)trig.size();
             PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
-            tri_solve<<<n_blocks(nt, 64), 64, 0, st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p, hstride,
-                                                       ybuf.p);
+            tri_solve<<<nt, 32, (j + 1) * sizeof(double2), st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p,
+                                                                 hstride, ybuf.p);
             ctx->launches += 1 + combine_chunked(st, n, 0, j + 1, nt, d_cols.p, d_slabs.p, ybuf.p, 1.0, d_X, 1);
+            if (jac) {
+                scale_cols<<<dim3(grid_rows(n), nt), 256, 0, st>>>(n, d_cols.p, Pinv.p, d_X, 1);
+                ctx->launches++;
+            }
             for (int c : trig) done[c] = 1;
             for (int c : trig)
                 if (resid[std::find(act.begin(), act.end(), c) - act.begin()] >= (rq.tols.empty() ? rq.tol : rq.tols[c]))
@@ -485,8 +551,8 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         } else if (!trig.empty()) {
             const int nt = (int)trig.size();
             PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
-            tri_solve<<<n_blocks(nt, 64), 64, 0, st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p, hstride,
-                                                       ybuf.p);
+            tri_solve<<<nt, 32, (j + 1) * sizeof(double2), st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p,
+                                                                 hstride, ybuf.p);
             ctx->launches += combine_chunked(st, n, 0, j + 1, nt, d_cols.p, d_slabs.p, ybuf.p, 1.0, d_X, 1);
             gather_x<<<dim3(grid_rows(2LL * n), nt), 256, 0, st>>>(n, d_cols.p, d_X, Xa.p);
             ctx->launches += 2;

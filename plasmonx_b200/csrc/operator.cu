@@ -340,7 +340,93 @@ __global__ void rhs_dipole(int N, int nv, int count, const int32_t *__restrict__
     B[(int64_t)c * 2 * nv + nv + N + e] = 0.0;
 }
 
+// Frequency-independent parts of diag(blockdiag(Kop, I) T) on the charge rows.
+__global__ void diag_parts(int N, int nt, const double *__restrict__ pos, const double *__restrict__ par,
+                           const int32_t *__restrict__ type, const int32_t *__restrict__ rowptr,
+                           const int32_t *__restrict__ col, const double *__restrict__ kval,
+                           const double *__restrict__ ktval, double *__restrict__ a, double *__restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double eta = par[2 * N + i], rq = par[i];
+    double sa = 0.0;
+    for (int t = 0; t < nt; ++t) b[(int64_t)i * nt + t] = 0.0;
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+        int j = col[e];
+        double tij = plx_pair_qq(pos[i] - pos[j], pos[N + i] - pos[N + j], pos[2 * N + i] - pos[2 * N + j], rq,
+                                 par[j]);
+        sa += kval[e] * (tij - eta);
+        b[(int64_t)i * nt + type[j]] += ktval[e] * (tij - eta);
+    }
+    a[i] = sa;
+}
+
+// 1 / diag(A(w)) per column.
+__global__ void diag_inverse_kernel(int N, int nt, int nv, int count, int hetero, const int32_t *__restrict__ freq,
+                                    const int32_t *__restrict__ type, const double *__restrict__ a,
+                                    const double *__restrict__ b, const Cplx *__restrict__ wratio,
+                                    const Cplx *__restrict__ dq, const double *__restrict__ frac,
+                                    const Cplx *__restrict__ inv_alpha, double *__restrict__ P) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = blockIdx.y;
+    if (r >= nv || c >= count) return;
+    int f = freq[c];
+    double re, im;
+    if (r < N) {
+        int ti = type[r];
+        if (!hetero) {
+            re = a[r];
+            im = 0.0;
+        } else {
+            re = a[r];
+            im = 0.0;
+            for (int t = 0; t < nt; ++t) {
+                Cplx w = wratio[ti + nt * t + (int64_t)nt * nt * f];
+                double bt = b[(int64_t)r * nt + t];
+                re += w.re * bt;
+                im += w.im * bt;
+            }
+            re *= 0.5;
+            im *= 0.5;
+        }
+        Cplx d = dq[ti + nt * f];
+        re += d.re;
+        im += d.im;
+    } else {
+        int i = (r - N) / 3;
+        re = 0.0;
+        im = 0.0;
+        for (int t = 0; t < nt; ++t) {
+            double fr = frac[t + (int64_t)nt * i];
+            Cplx al = inv_alpha[t + nt * f];
+            re += fr * al.re;
+            im += fr * al.im;
+        }
+    }
+    double m = re * re + im * im;
+    double *pc = P + (int64_t)c * 2 * nv;
+    pc[r] = m > 0.0 ? re / m : 1.0;
+    pc[nv + r] = m > 0.0 ? -im / m : 0.0;
+}
+
 }  // namespace
+
+void diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv) {
+    plx_ctx *ctx = g->ctx;
+    const int N = g->n_atoms, nt = g->n_types;
+    if (!g->d_diag_a.p) {
+        g->d_diag_a.alloc(ctx, N);
+        g->d_diag_b.alloc(ctx, (size_t)N * nt);
+        diag_parts<<<n_blocks(N, 128), 128, 0, ctx->stream>>>(N, nt, g->d_pos.p, g->d_par.p, g->d_type.p,
+                                                              g->d_rowptr.p, g->d_col.p, g->d_kval.p,
+                                                              g->d_ktval.p, g->d_diag_a.p, g->d_diag_b.p);
+        ctx->launches++;
+    }
+    diag_inverse_kernel<<<dim3(n_blocks(g->n_var, 256), b.count), 256, 0, ctx->stream>>>(
+        N, nt, g->n_var, b.count, nt > 1, b.d_freq, g->d_type.p, g->d_diag_a.p, g->d_diag_b.p, g->d_wratio.p,
+        g->d_dq.p, g->d_frac.p, g->d_inv_alpha.p, Pinv);
+    ctx->launches++;
+    PLX_CHECK_CUDA(cudaGetLastError());
+}
 
 void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on_the_fly);
 

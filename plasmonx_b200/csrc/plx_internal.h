@@ -118,6 +118,9 @@ struct plx_geom {
     plx::DevArray<uint16_t> d_Th, d_Tl, d_Xh, d_Xl;
     int64_t ldk = 0;
     plx::DevArray<int> d_tc_err;
+    // diagonal of blockdiag(Kop, I) T on the charge rows, frequency independent parts:
+    // a_i = sum_j K_ij (T_ij - T_ii), b_i,t = sum_{j of type t} K_ji (T_ij - T_ii)
+    plx::DevArray<double> d_diag_a, d_diag_b;
     // split-K partial sums of the few-column contraction (grown on demand;
     // used only by work ordered on the context's single stream)
     plx::DevArray<double> d_part;
@@ -156,6 +159,8 @@ void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, d
 //   S = T X (no K, no diagonal), S and X as above.
 void contract_t(plx_geom *g, int count, const double *X, double *S, Contraction how);
 void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout);
+//   1 / diag(A(w_c)) for every column, [count][2][n] split complex.
+void diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv);
 
 // tc_contract.cu: S = T X with BF16-split operands on the tensor cores
 // (nprod 3: Th Xh + Th Xl + Tl Xh; nprod 1: Th Xh).  X, S: [count][2][n] FP64.
@@ -179,6 +184,9 @@ struct GmresRequest {
     // when the residual estimate passes the tolerance or at the last step, with
     // no true-residual check (the caller forms the FP64 residual)
     bool inner = false;
+    // right preconditioning by the inverse diagonal of A(w) (inner solves only):
+    // the operator becomes A P^-1 and the returned correction P^-1 y
+    bool jacobi = false;
 };
 struct GmresResult {
     std::vector<int32_t> status, steps;
@@ -199,6 +207,7 @@ struct RefineRequest {
     int max_outer = 50;
     Contraction inner_contraction = Contraction::TC3;
     Contraction outer_contraction = Contraction::FP64;
+    bool jacobi = true;      // diagonal right preconditioning of the inner solves
 };
 struct RefineResult {
     std::vector<int32_t> status, inner_steps, outer;

@@ -120,6 +120,7 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
         in.m = rq.inner_m;
         in.contraction = rq.inner_contraction;
         in.inner = true;
+        in.jacobi = rq.jacobi;
         for (int k = 0; k < na; ++k) {
             int c = act[k];
             fa[k] = rq.freq[c];
