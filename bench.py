@@ -6,9 +6,18 @@
 Workload (default): the wFQFMu silver sphere -- fcc a = 4.086 A cut to a 35 A
 sphere, 10,473 atoms, 41,892 complex unknowns -- with the reference's default
 Ag parameters, 201 frequencies over 3.0-4.5 eV, x polarisation, on-memory
-GMRES at the reference's default tolerance (1e-9 x sqrt(n_var)).  Synthetic,
-seeded geometry; the dense T (14.0 GB FP64) is far larger than L2, so every
-step streams it from HBM (no L2 flush needed).
+mode.  Synthetic, seeded geometry; the dense T (14.0 GB FP64) is far larger
+than L2, so every step streams it from HBM (no L2 flush needed).
+
+Accuracy: the metric is quoted at <= 1e-6 relative error of sigma_abs.  The
+reference's default input tolerance (1e-9, i.e. ||b - A x|| < 1e-9 sqrt(n_var),
+a relative residual of ~2e-5 here) leaves sigma_abs errors of ~3e-5, so the
+benchmark uses an input tolerance of 1e-12 (same absolute test, 1000x
+tighter) for both forms; each line reports the measured sigma_abs error of
+five frequencies against an FP64 refinement solved to a 1e-11 relative
+residual.  The headline form is the mixed-precision refinement
+(--precision mixed_bf16x3); the plain FP64 GMRES of the reference's
+algorithm is timed on the same spectrum in the same run.
 
 One step = one spectrum: every frequency solved (201 freq-solves).  `value`
 is freq-solves/s over all ranks from the library's own CUDA-event timing of
@@ -217,7 +226,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', default='ag_sphere', choices=['ag_sphere', 'na_sphere', 'bowtie'])
     ap.add_argument('--precision', default='mixed_bf16x3')
-    ap.add_argument('--tolerance', type=float, default=1e-9, help='input tolerance (times sqrt(n_var))')
+    ap.add_argument('--tolerance', type=float, default=1e-12, help='input tolerance (times sqrt(n_var))')
     ap.add_argument('--no-fp64-compare', action='store_true')
     ap.add_argument('--inner-krylov', type=int, default=0)
     ap.add_argument('--ref-rel', type=float, default=1e-11)
@@ -265,7 +274,8 @@ def main():
             steps_hist.append(out['steps'][:, 0].copy())
         barrier(pg, local)
         wall = time.perf_counter() - t0
-    prof = ctx.profile_read()
+    breakdown = ctx.profile_breakdown()
+    prof = breakdown['tc_contraction'] if args.precision.startswith('mixed') else breakdown['fp64_contraction']
     ctx.profile(False)
     total_ms = allmax(pg, float(np.sum(dev_ms)), local)
     solves = allsum(pg, float(F * args.steps), local)
@@ -358,6 +368,7 @@ def main():
                         'd2h_bytes_per_step': int(F * (20 * 8 + 9 * 16 + 4 + 12))},
                 'gpu_launches': int(launches), 'roofline': roof, 'cpu_baseline': cpu,
                 'clocks': clk.summary(), 'wall_s_timed': wall,
+                'device_ms_breakdown': {k: round(v['ms'], 3) for k, v in breakdown.items()},
                 'sigma_abs_max_rel_err': None if acc is None else acc['headline_max_rel_err'],
                 'accuracy': acc, 'fp64_plain_gmres': fp64,
                 'speedup_vs_fp64_plain': None if fp64 is None else value / fp64['value'],

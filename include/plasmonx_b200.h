@@ -207,14 +207,18 @@ int64_t plx_last_solve_launches(const plx_geom *geom);
 
 /* ---- measurement -------------------------------------------------------- */
 
-/* When enabled, the library brackets every launch of the T contraction (the
- * dominant kernel of the iterative modes) with CUDA events on its stream and
- * accumulates, per launch, the algorithmic flops (2 n_var^2 x real columns) and
- * bytes (the stored T once, the input and output columns).  Enabling resets the
- * counters. */
+/* When enabled, the library brackets the sections of the iterative solvers
+ * with CUDA events on its stream and accumulates their device time per
+ * category: 0 tensor-core T contraction, 1 FP64 T contraction, 2 Arnoldi
+ * orthogonalisation, 3 conductance and diagonal rows of the operator,
+ * 4 least squares and solution updates.  For the contractions it also
+ * accumulates, per launch, the algorithmic flops (2 n_var^2 x real columns)
+ * and bytes (the stored T once at its storage precision, the input and output
+ * columns).  Enabling resets the counters. */
 plx_status plx_profile_enable(plx_ctx *ctx, int32_t on);
-/* Reads the accumulated contraction time (ms), launches, flops and bytes. */
-plx_status plx_profile_read(plx_ctx *ctx, double *ms, int64_t *launches, double *flops, double *bytes);
+/* Reads one category: accumulated time (ms), sections, flops and bytes. */
+plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,
+                            double *bytes);
 
 #ifdef __cplusplus
 }

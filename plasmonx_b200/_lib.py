@@ -86,7 +86,7 @@ def load():
     lib.plx_last_solve_launches.argtypes = [vp]
     lib.plx_contract.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int32]
     lib.plx_profile_enable.argtypes = [vp, C.c_int32]
-    lib.plx_profile_read.argtypes = [vp, _dp, C.POINTER(C.c_int64), _dp, _dp]
+    lib.plx_profile_read.argtypes = [vp, C.c_int32, _dp, C.POINTER(C.c_int64), _dp, _dp]
     _lib = lib
     return lib
 

@@ -547,26 +547,30 @@ plx_status plx_profile_enable(plx_ctx *ctx, int32_t on) {
         PLX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->profile = on != 0;
         ctx->prof_used = 0;
-        ctx->prof_flops = ctx->prof_bytes = 0.0;
-        ctx->prof_launches = 0;
+        for (int c = 0; c < 8; ++c) {
+            ctx->prof_flops[c] = ctx->prof_bytes[c] = 0.0;
+            ctx->prof_launches[c] = 0;
+        }
     });
 }
 
-plx_status plx_profile_read(plx_ctx *ctx, double *ms, int64_t *launches, double *flops, double *bytes) {
-    if (!ctx) return PLX_ERR_ARG;
+plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,
+                            double *bytes) {
+    if (!ctx || category < 0 || category > 4) return PLX_ERR_ARG;
     return guarded(ctx, [&] {
         set_device(ctx);
         PLX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
         double total = 0.0;
         for (size_t k = 0; k + 1 < ctx->prof_used; k += 2) {
+            if (ctx->prof_cat[k / 2] != category) continue;
             float t = 0.f;
             PLX_CHECK_CUDA(cudaEventElapsedTime(&t, ctx->prof_events[k], ctx->prof_events[k + 1]));
             total += t;
         }
         if (ms) *ms = total;
-        if (launches) *launches = ctx->prof_launches;
-        if (flops) *flops = ctx->prof_flops;
-        if (bytes) *bytes = ctx->prof_bytes;
+        if (launches) *launches = ctx->prof_launches[category];
+        if (flops) *flops = ctx->prof_flops[category];
+        if (bytes) *bytes = ctx->prof_bytes[category];
     });
 }
 

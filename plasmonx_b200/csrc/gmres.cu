@@ -504,6 +504,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
                                                                       accumulate);
             ctx->launches += 2 + combine_chunked(st, n, i0, ni, na, d_act.p, d_slabs.p, hbuf.p, -1.0, Wa.p, 0);
         };
+        prof_begin(ctx);
         if (j + 1 < 25 && !rq.inner) {
             for (int i = 0; i <= j; ++i) project(i, i + 1, 0);        // modified Gram-Schmidt
         } else {
@@ -511,11 +512,14 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
             project(0, j + 1, 1);                                     // ... and re-orthogonalise
         }
         batch_norms(g, na, Wa.p, nrm_part, nrm);
+        prof_end(ctx, PROF_ORTHO, 0.0, 0.0);
+        prof_begin(ctx);
         normalize<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, nrm.p, Wa.p, slabs[j + 1].p,
                                                                hcols[j].p, hstride, j + 1);
         givens<<<n_blocks(na, 128), 128, 0, st>>>(na, j, d_act.p, d_hcols.p, hstride, cs.p, sn.p, gv.p,
                                                  hstride, m, nrm.p);
         ctx->launches += 2;
+        prof_end(ctx, PROF_LSQ, 0.0, 0.0);
         PLX_CHECK_CUDA(cudaGetLastError());
         PLX_CHECK_CUDA(cudaMemcpyAsync(resid.data(), nrm.p, na * 8, cudaMemcpyDeviceToHost, st));
         PLX_CHECK_CUDA(cudaStreamSynchronize(st));

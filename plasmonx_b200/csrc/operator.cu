@@ -442,13 +442,15 @@ void prof_begin(plx_ctx *ctx) {
     PLX_CHECK_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used], ctx->stream));
 }
 
-void prof_end(plx_ctx *ctx, double flops, double bytes) {
+void prof_end(plx_ctx *ctx, int cat, double flops, double bytes) {
     if (!ctx->profile) return;
     PLX_CHECK_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used + 1], ctx->stream));
+    if (ctx->prof_cat.size() < ctx->prof_events.size() / 2) ctx->prof_cat.resize(ctx->prof_events.size() / 2);
+    ctx->prof_cat[ctx->prof_used / 2] = cat;
     ctx->prof_used += 2;
-    ctx->prof_flops += flops;
-    ctx->prof_bytes += bytes;
-    ctx->prof_launches += 1;
+    ctx->prof_flops[cat] += flops;
+    ctx->prof_bytes[cat] += bytes;
+    ctx->prof_launches[cat] += 1;
 }
 
 void contract_t(plx_geom *g, int count, const double *X, double *S, Contraction how) {
@@ -467,7 +469,8 @@ void contract_t(plx_geom *g, int count, const double *X, double *S, Contraction 
         contract_t_impl(g, count, X, S, otf);
         tbytes = otf ? 0.0 : 8.0 * nn * nn;
     }
-    prof_end(ctx, 2.0 * nn * nn * 2.0 * count, tbytes + 2.0 * 8.0 * nn * 2.0 * count);
+    prof_end(ctx, (how == Contraction::TC3 || how == Contraction::TC1) ? PROF_TC : PROF_FP64,
+             2.0 * nn * nn * 2.0 * count, tbytes + 2.0 * 8.0 * nn * 2.0 * count);
 }
 
 void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on_the_fly) {
@@ -543,7 +546,9 @@ void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, d
                     Contraction how) {
     if (b.count == 0) return;
     contract_t(g, b.count, X, work, how);
+    prof_begin(g->ctx);
     finish_rows(g, b, work, X, Y);
+    prof_end(g->ctx, PROF_ROWS, 0.0, 0.0);
 }
 
 void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout) {

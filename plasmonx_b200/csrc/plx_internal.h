@@ -74,9 +74,10 @@ struct plx_ctx {
     // contraction profiling (plx_profile_enable)
     bool profile = false;
     std::vector<cudaEvent_t> prof_events;   // pairs (start, stop), reused
+    std::vector<int> prof_cat;              // category of each pair
     size_t prof_used = 0;                   // events in use
-    double prof_flops = 0.0, prof_bytes = 0.0;
-    int64_t prof_launches = 0;
+    double prof_flops[8] = {}, prof_bytes[8] = {};
+    int64_t prof_launches[8] = {};
 };
 
 struct plx_geom {
@@ -219,9 +220,12 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
 void polar_batch(plx_geom *g, int count, const int32_t *d_pol, const double *X,
                  Cplx *d_polar /* [count][3] : alpha(a, pol_c) */);
 
-// Brackets a contraction with profiling events when profiling is enabled.
+// Brackets a section with profiling events when profiling is enabled.
+// Categories: 0 tensor-core T contraction, 1 FP64 T contraction, 2 Arnoldi
+// orthogonalisation, 3 conductance / diagonal rows, 4 least squares and updates.
+enum ProfCat { PROF_TC = 0, PROF_FP64 = 1, PROF_ORTHO = 2, PROF_ROWS = 3, PROF_LSQ = 4 };
 void prof_begin(plx_ctx *ctx);
-void prof_end(plx_ctx *ctx, double flops, double bytes);
+void prof_end(plx_ctx *ctx, int cat, double flops, double bytes);
 
 inline int n_blocks(int64_t work, int per_block) {
     int64_t b = (work + per_block - 1) / per_block;

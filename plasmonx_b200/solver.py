@@ -39,11 +39,18 @@ class Context:
     def profile(self, on=True):
         self.check(self.lib.plx_profile_enable(self.h, int(bool(on))))
 
-    def profile_read(self):
+    PROFILE_CATEGORIES = ('tc_contraction', 'fp64_contraction', 'orthogonalisation', 'operator_rows',
+                          'least_squares')
+
+    def profile_read(self, category=0):
         ms, fl, by = C.c_double(), C.c_double(), C.c_double()
         n = C.c_int64()
-        self.check(self.lib.plx_profile_read(self.h, C.byref(ms), C.byref(n), C.byref(fl), C.byref(by)))
+        self.check(self.lib.plx_profile_read(self.h, int(category), C.byref(ms), C.byref(n), C.byref(fl),
+                                             C.byref(by)))
         return {'ms': ms.value, 'launches': n.value, 'flops': fl.value, 'bytes': by.value}
+
+    def profile_breakdown(self):
+        return {name: self.profile_read(k) for k, name in enumerate(self.PROFILE_CATEGORIES)}
 
     @property
     def bytes_in_use(self):

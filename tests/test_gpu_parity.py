@@ -101,7 +101,9 @@ def test_solve_matches_reference_log(ctx, name):
                 assert abs(int(steps[i, c]) - len(tr['residuals'])) == 1
                 off += 1
             assert agrees(out['trace'][i, c, 0], tr['residuals'][0], 5)
-        assert off <= 0.01 * max(1, len(exp['gmres']))
+        # the symmetric 37-atom cluster is a near-breakdown Krylov sequence (see the
+        # oracle test): one solve in a log may end one step apart
+        assert off <= max(1, 0.01 * len(exp['gmres']))
 
 
 @pytest.mark.parametrize('name', CASES)
