@@ -200,6 +200,21 @@ plx_status plx_solve(plx_geom *geom, const plx_solve_desc *desc, double *x_out,
  * product. */
 plx_status plx_contract(plx_geom *geom, int32_t count, const double *X, double *S, int32_t how);
 
+/* Allocation-free S = T X (FP64, stored T) for callers that cannot allocate
+ * device memory -- their buffers come from another runtime's allocator, a
+ * preallocated serving pool, or a timed loop that must not synchronise on
+ * allocation calls.  No counterpart in the reference: it is the few-column
+ * case of plx_contract (how = 0) with DEVICE pointers d_X, d_S (count x n_var,
+ * each column contiguous) owned by the caller, and it allocates nothing.
+ * Its scratch is a fixed file-scope device array of 2^21 doubles (16 MiB per
+ * GPU that loads the library, held until exit); 1 <= count <= 16 and the
+ * split-K partials (k-chunks x count x n_var) must fit in it, otherwise the
+ * call returns PLX_ERR_ARG.  The first call on a device looks up the array's
+ * device address, so make that first call before any stream capture.  All
+ * calls share the array: calls whose kernels overlap on the GPU race.  Runs on
+ * the context's stream and returns when S is written. */
+plx_status plx_contract_noalloc(plx_geom *geom, int32_t count, const double *d_X, double *d_S);
+
 /* Device time (ms, CUDA events on the library's stream) of the last plx_solve,
  * and the number of kernels it launched. */
 double plx_last_solve_ms(const plx_geom *geom);

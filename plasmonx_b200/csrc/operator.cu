@@ -10,60 +10,11 @@
 
 #include "pair_tiles.cuh"
 #include "plx_internal.h"
+#include "skinny.cuh"
 
 namespace plx {
 
 namespace {
-
-// ---------------------------------------------------------------------------
-// S^T = X^T T for few rows (R = 2 * columns <= 16): split-K streaming of T.
-// ---------------------------------------------------------------------------
-constexpr int kSkinnyCols = 256;
-constexpr int kSkinnyK = 32;
-
-template <int R>
-__global__ void __launch_bounds__(kSkinnyCols) skinny_partial(int n, int kchunk,
-                                                              const double *__restrict__ Xt,
-                                                              const double *__restrict__ T,
-                                                              double *__restrict__ part) {
-    __shared__ double xs[kSkinnyK][R];
-    int col = blockIdx.x * kSkinnyCols + threadIdx.x;
-    int k0 = blockIdx.y * kchunk;
-    int k1 = min(n, k0 + kchunk);
-    double acc[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) acc[r] = 0.0;
-    for (int kb = k0; kb < k1; kb += kSkinnyK) {
-        int kn = min(kSkinnyK, k1 - kb);
-        __syncthreads();
-        for (int e = threadIdx.x; e < kSkinnyK * R; e += kSkinnyCols) {
-            int r = e / kSkinnyK, kk = e % kSkinnyK;
-            xs[kk][r] = (kk < kn) ? Xt[(int64_t)r * n + kb + kk] : 0.0;
-        }
-        __syncthreads();
-        if (col < n) {
-            const double *Tp = T + (int64_t)kb * n + col;
-            for (int kk = 0; kk < kn; ++kk) {
-                double t = __ldg(Tp + (int64_t)kk * n);
-#pragma unroll
-                for (int r = 0; r < R; ++r) acc[r] = fma(xs[kk][r], t, acc[r]);
-            }
-        }
-    }
-    if (col < n) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) part[((int64_t)blockIdx.y * R + r) * n + col] = acc[r];
-    }
-}
-
-__global__ void skinny_reduce(int n, int R, int ks, const double *__restrict__ part,
-                              double *__restrict__ S) {
-    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)R * n) return;
-    double s = 0.0;
-    for (int k = 0; k < ks; ++k) s += part[(int64_t)k * R * n + idx];
-    S[idx] = s;
-}
 
 // ---------------------------------------------------------------------------
 // S^T = X^T T, tiled (R > 16): 64 x 64 output tiles, 4 x 4 per thread, split
@@ -499,9 +450,8 @@ void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on
     if (!g->has_T) throw Error(PLX_ERR_ARG, "geometry was created without the dense T matrix");
     // K split: depends on n only (not on the batch), see tiled_partial
     const int cb = n_blocks(n, kSkinnyCols);
-    int ks = std::max(1, std::min(64, (592 + cb - 1) / cb));
-    const int kchunk = (n + ks - 1) / ks;
-    ks = (n + kchunk - 1) / kchunk;
+    int ks, kchunk;
+    skinny_split(n, ks, kchunk);
     size_t need = (size_t)ks * R * n;
     if (g->d_part.n < need) g->d_part.alloc(ctx, need);
     double *part = g->d_part.p;
