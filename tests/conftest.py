@@ -15,5 +15,13 @@ def pytest_configure(config):
     config.addinivalue_line('markers', 'slow: takes more than a few seconds on CPU')
 
 
-def golden_dirs():
-    return sorted(d for d in os.listdir(GOLDEN) if os.path.isfile(os.path.join(GOLDEN, d, 'expected.json')))
+def golden_dirs(kind=None):
+    """Fixture directories; kind 'atomistic' (wFQ/wFQFMu) or 'bem' filters them."""
+    out = []
+    for d in sorted(os.listdir(GOLDEN)):
+        if not os.path.isfile(os.path.join(GOLDEN, d, 'expected.json')):
+            continue
+        is_bem = d.startswith('bem_')
+        if kind is None or (kind == 'bem') == is_bem:
+            out.append(d)
+    return out

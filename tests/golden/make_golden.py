@@ -45,6 +45,10 @@ TESTS = [
     'wfqfmu_hetero_agau_default_int_param_inversion',
     'wfqfmu_hetero_agau_read_1param_inversion',
     'wfqfmu_hetero_agau_minimal_input',
+    'bem_ief_approximate_inversion',
+    'bem_ief_accurate_inversion',
+    'bem_dpcm_accurate_inversion',
+    'bem_dpcm_accurate_iterative_on_memory',
 ]
 
 NUM = r'[-+]?\d*\.\d+(?:[EeDd][-+]?\d+)?'
@@ -89,7 +93,7 @@ def parse_log(text):
     out['results'] = res
     # charge / dipole tables (verbose >= 2)
     tables = []
-    for m in re.finditer(r'(wFQ Charges|wFMu Dipoles)\n(.*?)(?:\n -{20,}|\nChErr)', text, re.S):
+    for m in re.finditer(r'(wFQ Charges|wFMu Dipoles|BEM Charges)\n(.*?)(?:\n -{20,}|\nChErr)', text, re.S):
         rows = []
         for line in m.group(2).splitlines():
             nums = re.findall(NUM, line)
@@ -126,6 +130,18 @@ def parse_log(text):
                 for c, v in zip(cols, toks[1:]):
                     entries['%d,%d' % (r, c)] = float(v.replace('D', 'E'))
         out[key] = entries
+    return out
+
+
+def filters(text):
+    """Argument strings of every get_filter(...) call (balanced parentheses)."""
+    out = []
+    for m in re.finditer(r'get_filter\(', text):
+        depth, i = 1, m.end()
+        while depth and i < len(text):
+            depth += {'(': 1, ')': -1}.get(text[i], 0)
+            i += 1
+        out.append(text[m.end():i - 1])
     return out
 
 
@@ -171,6 +187,10 @@ def one(name, ref):
             fr = [fmin + fstep * i for i in range(nf)]
         fev = [w * 27.211386245981 for w in fr]
         for line in kw.splitlines():
+            if line.startswith('bem mesh file:'):
+                fn = line.split(':', 1)[1].strip()
+                if fn != 'none':
+                    shutil.copy(os.path.join(tdir, fn), os.path.join(odir, os.path.basename(fn)))
             if 'wfqfmu file:' in line:
                 fn = line.split(':', 1)[1].strip()
                 if fn != 'none':
@@ -180,7 +200,7 @@ def one(name, ref):
         with open(os.path.join(tdir, 'reference', name + '.log')) as f:
             parsed = parse_log(f.read())
         with open(os.path.join(tdir, 'test')) as f:
-            parsed['runtest_filter'] = re.findall(r'get_filter\((.*?)\)', f.read(), re.S)
+            parsed['runtest_filter'] = filters(f.read())
         with open(os.path.join(odir, 'expected.json'), 'w') as f:
             json.dump(parsed, f, indent=0)
         print(name, len(parsed['results']), 'results,', len(parsed['tables']), 'tables,',
