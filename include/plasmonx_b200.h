@@ -49,7 +49,12 @@ typedef enum {
     PLX_ERR_UNSUPPORTED = 8     /* model / mode combination not provided */
 } plx_status;
 
-typedef enum { PLX_WFQ = 0, PLX_WFQFMU = 1 } plx_model;
+typedef enum {
+    PLX_WFQ = 0,
+    PLX_WFQFMU = 1,
+    PLX_BEM_DPCM = 2,           /* bem variant dpcm   (src/bem/bem_module.f90) */
+    PLX_BEM_IEF = 3             /* bem variant iefpcm */
+} plx_model;
 
 typedef enum {
     PLX_INVERSION = 0,          /* solve_w_inversion  (algorithm_module.f90:189) */
@@ -95,6 +100,23 @@ typedef struct {
     double e0;                  /* field intensity (a.u.) */
 } plx_geometry_desc;
 
+/* Boundary-element surface (bem_type after read_gmsh_file and create_tesserae,
+ * src/bem/bem_module.f90:224-491).  The triangles are given by their three
+ * corners, [n_tess][3 vertices][x, y, z] in bohr, in the order of the mesh's
+ * element block; the normal of a tessera is normal_factor * (v1-v0) x (v2-v0). */
+typedef struct {
+    int32_t variant;            /* PLX_BEM_DPCM or PLX_BEM_IEF */
+    int32_t n_tess;
+    int32_t accurate;           /* Green function: 0 approximate (diagonal
+                                   1.0694 sqrt(4 pi a) / (2 R)), 1 accurate
+                                   (accurate_green_function.f90) */
+    const double *triangles;
+    double normal_factor;       /* +1 or -1 (`bem normal scalar factor`) */
+    double sphere_radius;       /* R of the approximate diagonal (bohr) */
+    double eps_solvent;         /* `bem epsilon solvent` */
+    double e0;                  /* field intensity (a.u.) */
+} plx_bem_desc;
+
 /* One solve request over the frequencies set by plx_set_frequencies. */
 typedef struct {
     int32_t mode;               /* plx_mode */
@@ -135,7 +157,13 @@ uint64_t plx_ctx_bytes_in_use(const plx_ctx *ctx);
 plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *desc,
                                int32_t store_t, plx_geom **out);
 void plx_geometry_destroy(plx_geom *geom);
-/* Number of unknowns n_var (N for wFQ, 4N for wFQFMu). */
+/* BEM counterpart of plx_geometry_create: builds the Green-function derivative
+ * D (construct_constant_matrix_bem, bem_module.f90:678-782) once; with
+ * PLX_BEM_IEF the direct solve also builds S A^-1 and D S A^-1 on first use.
+ * plx_set_frequencies then takes eps(w) (complex, one per frequency) in alpha_w.
+ * The reference has no on-the-fly BEM product; PLX_GMRES_OTF is refused. */
+plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *desc, plx_geom **out);
+/* Number of unknowns n_var (N for wFQ, 4N for wFQFMu, n_tess for BEM). */
 int64_t plx_geometry_n_var(const plx_geom *geom);
 /* Stored non-zeros of K (both triangles). */
 int64_t plx_geometry_k_nnz(const plx_geom *geom);

@@ -12,13 +12,13 @@ LIB_PATH = os.path.join(HERE, 'libplasmonx_b200.so')
 PLX_OK = 0
 STATUS = {0: 'PLX_OK', 1: 'PLX_ERR_ARG', 2: 'PLX_ERR_CUDA', 3: 'PLX_ERR_NOMEM', 4: 'PLX_ERR_BUDGET',
           5: 'PLX_ERR_NOT_CONVERGED', 6: 'PLX_ERR_NAN', 7: 'PLX_ERR_SINGULAR', 8: 'PLX_ERR_UNSUPPORTED'}
-MODEL = {'wfq': 0, 'wfqfmu': 1}
+MODEL = {'wfq': 0, 'wfqfmu': 1, 'bem_dpcm': 2, 'bem_ief': 3}
 MODE = {'inversion': 0, 'iterative': 1, 'iterative on the fly': 2}
 PRECISION = {'fp64': 0, 'mixed_bf16x3': 1, 'fp64_refined': 2, 'mixed_bf16': 3}
 CONTRACT = {'fp64': 0, 'fp64_otf': 1, 'bf16x3': 2, 'bf16': 3}
 
 EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes_in_use',
-           'plx_geometry_create', 'plx_geometry_destroy', 'plx_geometry_n_var', 'plx_geometry_k_nnz',
+           'plx_geometry_create', 'plx_bem_create', 'plx_geometry_destroy', 'plx_geometry_n_var', 'plx_geometry_k_nnz',
            'plx_set_frequencies', 'plx_matvec', 'plx_rhs', 'plx_gmres_solver', 'plx_complex_inversion',
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
            'plx_profile_read', 'plx_contract', 'plx_contract_noalloc']
@@ -32,6 +32,12 @@ class GeometryDesc(C.Structure):
                 ('rhs_potential', C.c_int32), ('coord', _dp), ('atom_type', _ip), ('neighbours', _ip),
                 ('n_neighbours', _ip), ('eta', _dp), ('r_q', _dp), ('r_mu', _dp), ('tau', _dp),
                 ('density', _dp), ('a_ij', _dp), ('fermi_d', _dp), ('fermi_s', _dp), ('r0', _dp),
+                ('e0', C.c_double)]
+
+
+class BemDesc(C.Structure):
+    _fields_ = [('variant', C.c_int32), ('n_tess', C.c_int32), ('accurate', C.c_int32), ('triangles', _dp),
+                ('normal_factor', C.c_double), ('sphere_radius', C.c_double), ('eps_solvent', C.c_double),
                 ('e0', C.c_double)]
 
 
@@ -68,6 +74,7 @@ def load():
     lib.plx_ctx_bytes_in_use.restype = C.c_uint64
     lib.plx_ctx_bytes_in_use.argtypes = [vp]
     lib.plx_geometry_create.argtypes = [vp, C.POINTER(GeometryDesc), C.c_int32, C.POINTER(vp)]
+    lib.plx_bem_create.argtypes = [vp, C.POINTER(BemDesc), C.POINTER(vp)]
     lib.plx_geometry_destroy.argtypes = [vp]
     lib.plx_geometry_n_var.restype = C.c_int64
     lib.plx_geometry_n_var.argtypes = [vp]

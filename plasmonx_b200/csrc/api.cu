@@ -235,6 +235,35 @@ plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *d, int32_t
     return PLX_OK;
 }
 
+plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *d, plx_geom **out) {
+    if (!ctx || !d || !out) return PLX_ERR_ARG;
+    *out = nullptr;
+    plx_geom *g = new plx_geom();
+    plx_status s = guarded(ctx, [&] {
+        if (!ctx->stream) throw Error(PLX_ERR_CUDA, "context has no CUDA stream: " + ctx->last_error);
+        set_device(ctx);
+        if (d->variant != PLX_BEM_DPCM && d->variant != PLX_BEM_IEF) throw Error(PLX_ERR_ARG, "unknown BEM variant");
+        if (d->n_tess < 1 || !d->triangles) throw Error(PLX_ERR_ARG, "no tesserae");
+        if (d->n_tess > 65535) throw Error(PLX_ERR_UNSUPPORTED, "more than 65535 tesserae");
+        if (!d->accurate && !(d->sphere_radius > 0.0))
+            throw Error(PLX_ERR_ARG, "the approximate Green function needs a positive sphere radius");
+        g->ctx = ctx;
+        g->model = d->variant;
+        g->n_atoms = d->n_tess;
+        g->n_var = d->n_tess;
+        g->n_types = 1;
+        g->e0 = d->e0;
+        g->eps_solvent = d->eps_solvent;
+        build_bem(g, d->triangles, d->normal_factor, d->sphere_radius, d->accurate);
+    });
+    if (s != PLX_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return PLX_OK;
+}
+
 void plx_geometry_destroy(plx_geom *g) {
     if (!g) return;
     if (g->ctx) cudaSetDevice(g->ctx->device);
@@ -250,6 +279,7 @@ plx_status plx_set_frequencies(plx_geom *g, int32_t n_freq, const double *omega,
         set_device(g->ctx);
         if (n_freq < 1 || !omega) throw Error(PLX_ERR_ARG, "need at least one frequency");
         if (g->model == PLX_WFQFMU && !alpha_w) throw Error(PLX_ERR_ARG, "alpha_w is required for wFQFMu");
+        if (is_bem(g) && !alpha_w) throw Error(PLX_ERR_ARG, "eps(w) (alpha_w) is required for BEM");
         g->n_freq = n_freq;
         g->omega.assign(omega, omega + n_freq);
         g->alpha_w.clear();
@@ -365,6 +395,9 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
         if (desc->precision < PLX_FP64 || desc->precision > PLX_MIXED_BF16)
             throw Error(PLX_ERR_ARG, "bad precision");
         const bool otf = desc->mode == PLX_GMRES_OTF;
+        if (otf && is_bem(g))
+            throw Error(PLX_ERR_UNSUPPORTED, "BEM on the fly is not provided (the reference's BEM has no "
+                                             "on-the-fly product either); use the on-memory mode");
         const bool refined = desc->precision != PLX_FP64 && desc->mode != PLX_INVERSION;
         if (refined && otf && desc->precision != PLX_FP64_REFINED)
             throw Error(PLX_ERR_UNSUPPORTED, "tensor-core refinement needs the stored T (on-memory mode)");

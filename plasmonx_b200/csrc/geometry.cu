@@ -183,6 +183,25 @@ void build_dense_t(plx_geom *g) {
 // (construct_H_minus_L_matrix, matrix_module.f90:435-482).
 void upload_frequency_tables(plx_geom *g) {
     const int nt = g->n_types, F = g->n_freq;
+    if (is_bem(g)) {
+        // z(w) = 2 pi (eps_s + eps(w)) / (eps_s - eps(w)) (new_gmres_diagonal_shift_bem,
+        // bem_module.f90:977-997); alpha_w carries eps(w)
+        g->bem_z.resize(F);
+        for (int f = 0; f < F; ++f) {
+            Cplx e = g->alpha_w[f];
+            double nr = g->eps_solvent + e.re, ni = e.im;        // eps_s + eps
+            double dr = g->eps_solvent - e.re, di = -e.im;       // eps_s - eps
+            double m = dr * dr + di * di;
+            double qr = (nr * dr + ni * di) / m, qi = (ni * dr - nr * di) / m;
+            const double twopi = 6.283185307179586476925286766559;
+            g->bem_z[f] = {twopi * qr, twopi * qi};
+        }
+        g->d_dq.alloc(g->ctx, F);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(g->d_dq.p, g->bem_z.data(), F * sizeof(Cplx), cudaMemcpyHostToDevice,
+                                       g->ctx->stream));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+        return;
+    }
     std::vector<Cplx> dq(nt * F), ia(nt * F), wr((size_t)nt * nt * F);
     for (int f = 0; f < F; ++f) {
         double w = g->omega[f];

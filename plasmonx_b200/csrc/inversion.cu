@@ -7,6 +7,7 @@
 // frequency diagonal, written row-major (which cuSOLVER sees as A^T in
 // column-major order), factored with cusolverDnZgetrf and solved with
 // cusolverDnZgetrs(op = T).
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -81,14 +82,22 @@ __global__ void interleaved_to_split(int n, int count, const double2 *__restrict
     S[(int64_t)c * 2 * n + n + r] = Z[idx].y;
 }
 
-// alpha(a, pol_c) = sum_i q_i r_ia / E0 + sum_i mu_ia / E0, one block per (column, a).
-__global__ void polar_kernel(int N, int nv, int fmu, double e0, const double *__restrict__ pos,
+// alpha(a, pol_c) = sum_i w_i q_i r_ia / E0 (+ sum_i mu_ia / E0), one block per
+// (column, a); w_i = 1, or the tessera area for DPCM (calculate_dynamic_polar_bem,
+// bem_module.f90:1051-1142).
+__global__ void polar_kernel(int N, int nv, int fmu, int area_weight, double e0, const double *__restrict__ pos,
                              const double *__restrict__ X, Cplx *__restrict__ out) {
     int c = blockIdx.y, a = blockIdx.x;
     const double *xr = X + (int64_t)c * 2 * nv, *xi = xr + nv;
     double sr = 0.0, si = 0.0;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         double p = pos[(int64_t)a * N + i];
+        if (area_weight) {
+            double w = pos[3LL * N + i];
+            sr += w * xr[i] * p / e0;
+            si += w * xi[i] * p / e0;
+            continue;
+        }
         sr += xr[i] * p / e0;
         si += xi[i] * p / e0;
         if (fmu) {
@@ -121,6 +130,10 @@ struct SolverHandle {
     cusolverDnHandle_t h = nullptr;
 };
 
+struct BlasHandle {
+    cublasHandle_t h = nullptr;
+};
+
 cusolverDnHandle_t solver_handle(plx_ctx *ctx) {
     static thread_local SolverHandle sh;
     if (!sh.h) {
@@ -133,10 +146,21 @@ cusolverDnHandle_t solver_handle(plx_ctx *ctx) {
 
 }  // namespace
 
+void bem_dgemm(plx_geom *g, const double *A, const double *B, double *C) {
+    static thread_local BlasHandle bh;
+    if (!bh.h && cublasCreate(&bh.h) != CUBLAS_STATUS_SUCCESS) throw Error(PLX_ERR_CUDA, "cublasCreate failed");
+    cublasSetStream(bh.h, g->ctx->stream);
+    const int n = g->n_var;
+    const double one = 1.0, zero = 0.0;
+    if (cublasDgemm(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, A, n, B, n, &zero, C, n) != CUBLAS_STATUS_SUCCESS)
+        throw Error(PLX_ERR_CUDA, "cublasDgemm failed");
+}
+
 void polar_batch(plx_geom *g, int count, const int32_t * /*d_pol*/, const double *X, Cplx *d_polar) {
     if (count == 0) return;
     polar_kernel<<<dim3(3, count), 256, 0, g->ctx->stream>>>(g->n_atoms, g->n_var, g->model == PLX_WFQFMU,
-                                                            g->e0, g->d_pos.p, X, d_polar);
+                                                            g->model == PLX_BEM_DPCM, g->e0, g->d_pos.p, X,
+                                                            d_polar);
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
 }
@@ -151,10 +175,16 @@ void solve_inversion_cols(plx_geom *g, int i_freq, int count, double *d_vars) {
     DevArray<double2> A, B;
     A.alloc(ctx, (size_t)n * n);
     B.alloc(ctx, (size_t)n * std::max(count, 1));
-    assemble_rows<<<dim3(n_blocks(n, 128), n), 128, 0, st>>>(
-        g->n_atoms, g->n_types, n, i_freq, g->n_types > 1, g->d_type.p, g->d_rowptr.p, g->d_col.p,
-        g->d_kval.p, g->d_ktval.p, g->d_wratio.p, g->d_dq.p, g->d_frac.p, g->d_inv_alpha.p, g->d_T.p,
-        A.p);
+    // atomistic: A row-major (cuSOLVER sees A^T, solve with op T); BEM: column-major (op N)
+    const bool colmajor = is_bem(g);
+    if (colmajor) {
+        bem_assemble_matrix(g, i_freq, A.p);
+    } else {
+        assemble_rows<<<dim3(n_blocks(n, 128), n), 128, 0, st>>>(
+            g->n_atoms, g->n_types, n, i_freq, g->n_types > 1, g->d_type.p, g->d_rowptr.p, g->d_col.p,
+            g->d_kval.p, g->d_ktval.p, g->d_wratio.p, g->d_dq.p, g->d_frac.p, g->d_inv_alpha.p, g->d_T.p,
+            A.p);
+    }
     split_to_interleaved<<<n_blocks((int64_t)n * count, 256), 256, 0, st>>>(n, count, d_vars, B.p);
     ctx->launches += 2;
     PLX_CHECK_CUDA(cudaGetLastError());
@@ -176,8 +206,8 @@ void solve_inversion_cols(plx_geom *g, int i_freq, int count, double *d_vars) {
     PLX_CHECK_CUDA(cudaStreamSynchronize(st));
     if (hinfo != 0) throw Error(PLX_ERR_SINGULAR, "INFO.ne.0 in ZGETRF in complex inversion");
     if (count > 0) {
-        // the buffer holds A^T (row-major A read column-major): solve A x = b
-        if (cusolverDnZgetrs(h, CUBLAS_OP_T, n, count, reinterpret_cast<cuDoubleComplex *>(A.p), n, ipiv.p,
+        // atomistic: the buffer holds A^T (row-major A read column-major): solve A x = b
+        if (cusolverDnZgetrs(h, colmajor ? CUBLAS_OP_N : CUBLAS_OP_T, n, count, reinterpret_cast<cuDoubleComplex *>(A.p), n, ipiv.p,
                              reinterpret_cast<cuDoubleComplex *>(B.p), n, info.p) != CUSOLVER_STATUS_SUCCESS)
             throw Error(PLX_ERR_CUDA, "cusolverDnZgetrs failed");
         interleaved_to_split<<<n_blocks((int64_t)n * count, 256), 256, 0, st>>>(n, count, B.p, d_vars);

@@ -362,6 +362,10 @@ __global__ void diag_inverse_kernel(int N, int nt, int nv, int count, int hetero
 }  // namespace
 
 void diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv) {
+    if (is_bem(g)) {
+        bem_diagonal_inverse(g, b, Pinv);
+        return;
+    }
     plx_ctx *ctx = g->ctx;
     const int N = g->n_atoms, nt = g->n_types;
     if (!g->d_diag_a.p) {
@@ -408,6 +412,9 @@ void contract_t(plx_geom *g, int count, const double *X, double *S, Contraction 
     plx_ctx *ctx = g->ctx;
     const double nn = (double)g->n_var;
     const bool otf = how == Contraction::FP64_OTF;
+    if (otf && is_bem(g))
+        throw Error(PLX_ERR_UNSUPPORTED, "BEM on the fly is not provided (the reference's BEM has no "
+                                         "on-the-fly product either); use the on-memory mode");
     prof_begin(ctx);
     // algorithmic: 2 n^2 flops per real column (one product, whatever the
     // emulation); bytes: the stored T once at its storage precision, plus the
@@ -497,12 +504,19 @@ void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, d
     if (b.count == 0) return;
     contract_t(g, b.count, X, work, how);
     prof_begin(g->ctx);
-    finish_rows(g, b, work, X, Y);
+    if (is_bem(g))
+        bem_apply_rows(g, b, work, X, Y);
+    else
+        finish_rows(g, b, work, X, Y);
     prof_end(g->ctx, PROF_ROWS, 0.0, 0.0);
 }
 
 void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout) {
     if (b.count == 0) return;
+    if (is_bem(g)) {
+        bem_rhs(g, b, d_pol, Bout);
+        return;
+    }
     plx_ctx *ctx = g->ctx;
     cudaStream_t st = ctx->stream;
     const int N = g->n_atoms, nv = g->n_var;

@@ -103,9 +103,18 @@ struct plx_geom {
     plx::DevArray<double> d_kval;       // nnz: K_ij
     plx::DevArray<double> d_ktval;      // nnz: K_ji
     int64_t nnz = 0;
-    // device: dense interaction matrix T (n_var x n_var, symmetric, row-major)
+    // device: dense interaction matrix T (n_var x n_var, row-major; symmetric
+    // for wFQ / wFQFMu; for BEM the Green-function derivative stored transposed,
+    // d_T[j][i] = D(i, j))
     plx::DevArray<double> d_T;
     bool has_T = false;
+    bool t_symmetric = true;
+    // BEM: tessera frame [9][n] (normal, tangent 1, tangent 2), the diagonal of D
+    // before the accurate closure (IEFPCM right-hand side), S A^-1 and D S A^-1
+    // (column-major, IEFPCM direct solve), solvent permittivity, z(w) per frequency
+    plx::DevArray<double> d_frame, d_dpre, d_M, d_DM;
+    double eps_solvent = 1.0;
+    std::vector<plx::Cplx> bem_z;
     // frequencies
     int n_freq = 0;
     std::vector<double> omega;                 // n_freq
@@ -147,6 +156,8 @@ struct OpBatch {
     const int32_t *d_freq;    // device, [count]: frequency index of each column
 };
 
+inline bool is_bem(const plx_geom *g) { return g->model == PLX_BEM_DPCM || g->model == PLX_BEM_IEF; }
+
 // geometry.cu
 void build_conductance(plx_geom *g);
 void build_dense_t(plx_geom *g);
@@ -172,6 +183,19 @@ int tc_error(plx_geom *g);   // non-zero when a tensor-core CTA gave up waiting
 // inversion.cu
 // d_vars: [count][2][n] right-hand sides in, solutions of A(w_i) x = b out.
 void solve_inversion_cols(plx_geom *g, int i_freq, int count, double *d_vars);
+// C = A B for column-major n_var x n_var FP64 matrices (cuBLAS)
+void bem_dgemm(plx_geom *g, const double *A, const double *B, double *C);
+
+// bem.cu: tesserae, the Green-function derivative D (approximate or accurate),
+// the BEM operator rows (S + z x), right-hand sides and the direct-solve matrix.
+// tri_host: [n][3 vertices][3] bohr.
+void build_bem(plx_geom *g, const double *tri_host, double normal_factor, double sphere_r, int accurate);
+void build_bem_ief(plx_geom *g);
+void bem_apply_rows(plx_geom *g, const OpBatch &b, const double *S, const double *X, double *Y);
+void bem_rhs(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout);
+void bem_diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv);
+// column-major complex A(w_i) into A (n x n)
+void bem_assemble_matrix(plx_geom *g, int i_freq, double2 *A);
 
 // gmres.cu
 struct GmresRequest {

@@ -267,6 +267,28 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
+// Transposed split for a non-symmetric stored matrix: out[r][c] = in[c][r]
+// (square n x n input), through a shared-memory tile.
+__global__ void split_bf16_t(int n, const double *__restrict__ in, int64_t ld_out, __nv_bfloat16 *__restrict__ hi,
+                             __nv_bfloat16 *__restrict__ lo) {
+    __shared__ float tile[32][33];
+    int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        int r = by + k, c = bx + threadIdx.x;          // read in[r][c]
+        tile[k][threadIdx.x] = (r < n && c < n) ? (float)in[(int64_t)r * n + c] : 0.0f;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        int orow = bx + k, ocol = by + threadIdx.x;     // out[orow][ocol] = in[ocol][orow]
+        if (orow < n && ocol < ld_out) {
+            float x = tile[threadIdx.x][k];
+            __nv_bfloat16 h = __float2bfloat16_rn(x);
+            hi[(int64_t)orow * ld_out + ocol] = h;
+            lo[(int64_t)orow * ld_out + ocol] = __float2bfloat16_rn(x - __bfloat162float(h));
+        }
+    }
+}
+
 // FP64 -> (BF16 high, BF16 low) split of a row-major [rows][cols] array into a
 // zero-padded [rows_pad][ld] pair.
 __global__ void split_bf16(int rows, int cols, int64_t ld_in, const double *__restrict__ in, int rows_pad,
@@ -339,9 +361,19 @@ void build_t_split(plx_geom *g) {
     g->ldk = ld;
     g->d_Th.alloc(g->ctx, (size_t)(n * ld));
     g->d_Tl.alloc(g->ctx, (size_t)(n * ld));
-    split_bf16<<<2048, 256, 0, g->ctx->stream>>>((int)n, (int)n, n, g->d_T.p, (int)n, ld,
-                                                 reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p),
-                                                 reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p));
+    if (g->t_symmetric) {
+        split_bf16<<<2048, 256, 0, g->ctx->stream>>>((int)n, (int)n, n, g->d_T.p, (int)n, ld,
+                                                     reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p),
+                                                     reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p));
+    } else {
+        // stored transposed (BEM): split the transpose; the padded k columns stay zero
+        PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Th.p, 0, (size_t)(n * ld) * 2, g->ctx->stream));
+        PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Tl.p, 0, (size_t)(n * ld) * 2, g->ctx->stream));
+        dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
+        split_bf16_t<<<grid, dim3(32, 8), 0, g->ctx->stream>>>((int)n, g->d_T.p, ld,
+                                                                reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p),
+                                                                reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p));
+    }
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
     g->d_tc_err.alloc(g->ctx, 1);

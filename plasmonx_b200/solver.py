@@ -1,7 +1,7 @@
 """Host-side driver of the B200 solve: the per-frequency loop of the reference
 (src/solvers/algorithm_module.f90:150-465) over the C ABI.
 
-    prob = Problem.from_keyword_file('input.kw')
+    prob = Problem.from_keyword_file('input.kw')   # or BemProblem.from_keyword_file (bem.py)
     with Solver(prob) as s:
         out = s.solve()            # mode taken from the input ('inversion' / 'iterative' /
                                    # 'iterative on the fly'), FP64
@@ -76,6 +76,9 @@ class Solver:
         self.own_ctx = ctx is None
         self.ctx = ctx or Context(device)
         self.lib = self.ctx.lib
+        if getattr(prob, 'triangles', None) is not None:
+            self._init_bem(prob)
+            return
         if store_t is None:
             store_t = prob.method != 'iterative on the fly'
         nt = len(prob.type_names)
@@ -98,6 +101,16 @@ class Solver:
             ptr(k['density']), ptr(k['a_ij']), ptr(k['fermi_d']), ptr(k['fermi_s']), ptr(k['r0']), prob.e0)
         h = C.c_void_p()
         self.ctx.check(self.lib.plx_geometry_create(self.ctx.h, C.byref(d), int(bool(store_t)), C.byref(h)))
+        self.g = h
+        self.n_var = int(self.lib.plx_geometry_n_var(self.g))
+        self.set_frequencies(prob.freqs, prob.alpha_w)
+
+    def _init_bem(self, prob):
+        self._keep = dict(tri=np.ascontiguousarray(prob.triangles, dtype=np.float64))
+        d = _lib.BemDesc(_lib.MODEL[prob.model], prob.n_tess, int(prob.accurate), ptr(self._keep['tri']),
+                         prob.normal_factor, prob.sphere_radius, prob.eps_solvent, prob.e0)
+        h = C.c_void_p()
+        self.ctx.check(self.lib.plx_bem_create(self.ctx.h, C.byref(d), C.byref(h)))
         self.g = h
         self.n_var = int(self.lib.plx_geometry_n_var(self.g))
         self.set_frequencies(prob.freqs, prob.alpha_w)

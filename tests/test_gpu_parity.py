@@ -25,7 +25,7 @@ from tests.printed import agrees
 
 pytestmark = pytest.mark.gpu
 
-CASES = golden_dirs()
+CASES = golden_dirs('atomistic')
 
 
 @pytest.fixture(scope='module')
