@@ -1,7 +1,8 @@
 """Benchmark of the per-frequency response solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config ag_sphere|na_sphere|bowtie] [--precision fp64|mixed_bf16x3]
+                    [--config ag_sphere|na_sphere|bowtie|bem_sphere|bem_rod]
+                    [--precision fp64|mixed_bf16x3] [--n-tess 2000] [--bem-variant dpcm|iefpcm]
 
 Workload (default): the wFQFMu silver sphere -- fcc a = 4.086 A cut to a 35 A
 sphere, 10,473 atoms, 41,892 complex unknowns -- with the reference's default
@@ -30,6 +31,12 @@ replica of the spectrum (weak scaling; no collective on the data path).
 threaded C restatement of its on-the-fly product (oracle/pairs.c) over a
 bounded sample of matrix-vector products of the same geometry, turned into
 freq-solves/s with the Arnoldi step count per frequency-solve.
+
+BEM workloads (--config bem_sphere / bem_rod): a 10 nm sphere or a 40 x 10 nm
+prolate rod meshed into --n-tess tesserae (20 nu^2; 2000, 8000, 20480) with a
+seeded 2% radial jitter, Drude-Lorentz eps(w) in vacuum, 301 frequencies over
+1.5-4.5 eV, x polarisation, on-memory GMRES.  The CPU arm there times the
+reference's on-memory product, the dense D x of the oracle (threaded BLAS).
 """
 import argparse
 import json
@@ -61,8 +68,13 @@ def peaks():
     return PEAKS_FALLBACK, 'fallback'
 
 
-def make_problem(name, n_freq=None, method='iterative', polarization='x', radius=None):
+def make_problem(name, n_freq=None, method='iterative', polarization='x', radius=None, n_tess=2000,
+                 bem_variant='dpcm'):
     from plasmonx_b200 import configs
+    if name in ('bem_sphere', 'bem_rod'):
+        from plasmonx_b200.bem import bem_surface
+        return bem_surface(n_tess, variant=bem_variant, shape=name[4:], n_freq=n_freq or 301, method=method,
+                           tolerance=1e-9, polarization=polarization, gmres_dim=1000)
     if name == 'ag_sphere':
         return configs.ag_sphere(radius=radius or 35.0, n_freq=n_freq or 201, method=method, tolerance=1e-9,
                                  polarization=polarization, gmres_dim=1000)
@@ -75,7 +87,21 @@ def make_problem(name, n_freq=None, method='iterative', polarization='x', radius
     raise ValueError(name)
 
 
+def is_bem(prob):
+    return getattr(prob, 'triangles', None) is not None
+
+
 def workload_desc(name, prob):
+    if is_bem(prob):
+        return {'workload': 'BEM %s %s, %s Green function' % (prob.variant.upper(),
+                                                               {'bem_sphere': 'sphere R=10 nm',
+                                                                'bem_rod': 'prolate rod 40 x 10 nm'}[name],
+                                                               prob.green),
+                'n_tess': int(prob.n_tess), 'n_var': int(prob.n_var), 'n_freq': int(len(prob.freqs)),
+                'polarization': prob.polarization, 'mode': prob.method, 'tolerance': prob.tolerance_input,
+                'l2': 'inputs larger than L2 (stored D %.2f GB)' % (8.0 * prob.n_var ** 2 / 1e9)
+                if 8.0 * prob.n_var ** 2 > 126e6 else 'stored D %.0f MB fits in L2 (not flushed)'
+                % (8.0 * prob.n_var ** 2 / 1e6)}
     return {'workload': {'ag_sphere': 'wFQFMu Ag fcc sphere R=35 A',
                          'na_sphere': 'wFQ Na bcc sphere R=20 A',
                          'bowtie': 'wFQFMu Ag-Au bow-tie'}[name],
@@ -194,8 +220,34 @@ def job_throughput(pg, local, solves, device_ms):
     return total / (slowest / 1000.0), total, slowest
 
 
+def cpu_sample_bem(prob, n_mv, steps_per_solve):
+    """Time n_mv dense D x products (threaded BLAS) of the oracle's BEM operator."""
+    import tempfile
+    from oracle import bem as obem
+    with tempfile.TemporaryDirectory() as d:
+        o = obem.Bem(prob.write_keyword_files(d, 'bench'))
+    D = np.ascontiguousarray(o.D)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(o.n_var) + 1j * rng.standard_normal(o.n_var)
+
+    def matvec(i, v):
+        # the real D applied to the real and imaginary parts at once (one n x 2 GEMM)
+        Y = D @ np.stack([v.real, v.imag], axis=1)
+        return Y[:, 0] + 1j * Y[:, 1] + o.z(i) * v
+
+    matvec(0, x)
+    t0 = time.perf_counter()
+    for k in range(n_mv):
+        x = matvec(k % len(o.freqs), x)
+        x /= np.linalg.norm(x)
+    dt = (time.perf_counter() - t0) / n_mv
+    return 1.0 / (dt * steps_per_solve), dt, os.cpu_count()
+
+
 def cpu_sample(prob, n_mv, n_threads, steps_per_solve):
     """Time n_mv on-the-fly products of the C restatement; return freq-solves/s."""
+    if is_bem(prob):
+        return cpu_sample_bem(prob, max(n_mv, 20), steps_per_solve)
     from oracle import keywords, model
     from oracle.cpu_baseline import CpuOperator
     s = model.System.from_keywords(keywords.read_keyword_text(prob.to_keyword_text()))
@@ -214,7 +266,7 @@ def run_reference(args):
     rank, world, local, pg = dist_setup()
     if rank != 0:
         return
-    prob = make_problem(args.config)
+    prob = make_problem(args.config, n_tess=args.n_tess, bem_variant=args.bem_variant)
     sps = args.steps_per_solve
     vals = []
     for _ in range(args.warmup):
@@ -228,8 +280,10 @@ def run_reference(args):
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
             'config': workload_desc(args.config, prob), 'impl': 'reference',
             'cpu_baseline': {'value': v, 'unit': 'freq-solves/s', 'cores': nthr, 'kind': 'port',
-                             'sample': '%d on-the-fly A x products of the C restatement per step, '
-                                       'x %.0f Arnoldi steps per freq-solve' % (args.cpu_matvecs, sps)},
+                             'sample': ('%d dense D x products (threaded BLAS) per step' % max(args.cpu_matvecs, 20)
+                                        if is_bem(prob) else
+                                        '%d on-the-fly A x products of the C restatement per step'
+                                        % args.cpu_matvecs) + ', x %.0f Arnoldi steps per freq-solve' % sps},
             'e2e': {'value': v, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
@@ -240,7 +294,10 @@ def main():
     ap.add_argument('--steps', type=int, default=2)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--config', default='ag_sphere', choices=['ag_sphere', 'na_sphere', 'bowtie'])
+    ap.add_argument('--config', default='ag_sphere',
+                    choices=['ag_sphere', 'na_sphere', 'bowtie', 'bem_sphere', 'bem_rod'])
+    ap.add_argument('--n-tess', type=int, default=2000, help='BEM tesserae (20 nu^2)')
+    ap.add_argument('--bem-variant', default='dpcm', choices=['dpcm', 'iefpcm'])
     ap.add_argument('--precision', default='mixed_bf16x3')
     ap.add_argument('--tolerance', type=float, default=1e-12, help='input tolerance (times sqrt(n_var))')
     ap.add_argument('--no-fp64-compare', action='store_true')
@@ -260,7 +317,8 @@ def main():
 
     rank, world, local, pg = dist_setup()
     from plasmonx_b200.solver import Context, Solver
-    prob = make_problem(args.config, n_freq=args.n_freq, radius=args.radius)
+    prob = make_problem(args.config, n_freq=args.n_freq, radius=args.radius, n_tess=args.n_tess,
+                        bem_variant=args.bem_variant)
     prob.tolerance_input = args.tolerance
     prob.tol = args.tolerance * np.sqrt(prob.n_var)
     F = len(prob.freqs)
@@ -367,16 +425,19 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         sps = float(np.mean(np.concatenate(steps_hist))) if steps_hist else args.steps_per_solve
         v, dt, nthr = cpu_sample(prob, args.cpu_matvecs, 0, sps)
+        what = ('%d dense D x products of the oracle (threaded BLAS, %.4f s each)' % (max(args.cpu_matvecs, 20), dt)
+                if is_bem(prob) else
+                '%d on-the-fly A x products of the C restatement (%.2f s each)' % (args.cpu_matvecs, dt))
         cpu = {'value': v, 'unit': 'freq-solves/s', 'cores': nthr, 'kind': 'port',
-               'sample': '%d on-the-fly A x products of the C restatement (%.2f s each) x %.1f Arnoldi steps '
-                         'per freq-solve (mean of this run)' % (args.cpu_matvecs, dt, sps)}
+               'sample': what + ' x %.1f Arnoldi steps per freq-solve (mean of this run)' % sps}
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': 'freq-solves/s', 'n_gpus': world,
                 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
                 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
                 'dtype': {'fp64': 'f64', 'mixed_bf16x3': 'bf16x3 (fp32 acc) + f64 refinement',
                           'mixed_bf16': 'bf16 (fp32 acc) + f64 refinement', 'fp64_refined': 'f64'}[args.precision],
-                'data': 'synthetic (seeded fcc lattice, reference default parameters)',
+                'data': ('synthetic (seeded geodesic surface, Drude-Lorentz eps)' if is_bem(prob) else
+                         'synthetic (seeded fcc lattice, reference default parameters)'),
                 'config': dict(workload_desc(args.config, prob), precision=args.precision),
                 'e2e': {'value': e2e_val, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': int(h2d),
                         'd2h_bytes_per_step': int(F * (20 * 8 + 9 * 16 + 4 + 12))},
