@@ -13,6 +13,9 @@
 // Storage: Krylov vectors are kept in "slabs", one per step j, each holding
 // the j-th basis vector of every column ([C][2][n] split complex), allocated
 // when the step is reached so that memory follows the actual iteration count.
+// The inner solves of a refinement may keep their basis in FP32 (half the
+// projection traffic); dot products, Hessenberg, rotations and the iterate stay
+// FP64, and the refinement's FP64 residual absorbs the storage rounding.
 // Columns that converge leave the active list; the operator and the Arnoldi
 // kernels only touch active columns.
 #include <algorithm>
@@ -61,10 +64,11 @@ __device__ __forceinline__ void block_sum2(double &a, double &b) {
 }
 
 // Copies column act[k] of slab j into the compact batch X[k].
-__global__ void gather_cols(int n, const int32_t *__restrict__ act, const double *__restrict__ slab,
+template <typename VT>
+__global__ void gather_cols(int n, const int32_t *__restrict__ act, const VT *__restrict__ slab,
                             double *__restrict__ X) {
     int k = blockIdx.y;
-    const double *src = slab + (int64_t)act[k] * 2 * n;
+    const VT *src = slab + (int64_t)act[k] * 2 * n;
     double *dst = X + (int64_t)k * 2 * n;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
          r += (int64_t)gridDim.x * blockDim.x)
@@ -80,9 +84,10 @@ __global__ void gather_cols(int n, const int32_t *__restrict__ act, const double
 constexpr int kDotPT = 4;
 constexpr int kDotRows = kThreads * kDotPT;
 
+template <typename VT>
 __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
                                                          const int32_t *__restrict__ act,
-                                                         double *const *__restrict__ slabs,
+                                                         VT *const *__restrict__ slabs,
                                                          const double *__restrict__ W,
                                                          double2 *__restrict__ part) {
     __shared__ double2 red[kThreads / 32][32];
@@ -101,13 +106,13 @@ __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
     for (int g0 = 0; g0 < ni; g0 += 32) {
         const int gn = min(32, ni - g0);
         for (int t = 0; t < gn; ++t) {
-            const double *v = slabs[i0 + g0 + t] + (int64_t)c * 2 * n;
+            const VT *v = slabs[i0 + g0 + t] + (int64_t)c * 2 * n;
             double re = 0.0, im = 0.0;
 #pragma unroll
             for (int q = 0; q < kDotPT; ++q) {
                 int r = r0 + threadIdx.x + kThreads * q;
                 if (r < n) {
-                    double vr = v[r], vi = v[n + r];
+                    double vr = (double)v[r], vi = (double)v[n + r];
                     re += vr * wre[q] + vi * wim[q];      // conj(v) * w
                     im += vr * wim[q] - vi * wre[q];
                 }
@@ -157,9 +162,10 @@ __global__ void dots_finish(int nchunk, int ni, int i0, const int32_t *__restric
 
 // W[k] -= sum_{ii} V_{i0+ii}[c] h[k][ii]   (sign = -1), or X[c] += ... (sign = +1,
 // target indexed by column instead of compact position when by_col != 0).
+template <typename VT>
 __global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int hld, int hoff,
                                                     const int32_t *__restrict__ act,
-                                                    double *const *__restrict__ slabs,
+                                                    VT *const *__restrict__ slabs,
                                                     const double2 *__restrict__ h, double sign,
                                                     double *__restrict__ Y, int by_col) {
     extern __shared__ double2 sh[];
@@ -170,8 +176,8 @@ __global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int h
     if (r >= n) return;
     double ar = 0.0, ai = 0.0;
     for (int ii = 0; ii < ni; ++ii) {
-        const double *v = slabs[i0 + ii] + (int64_t)c * 2 * n;
-        double vr = v[r], vi = v[n + r];
+        const VT *v = slabs[i0 + ii] + (int64_t)c * 2 * n;
+        double vr = (double)v[r], vi = (double)v[n + r];
         double2 hh = sh[ii];
         ar += vr * hh.x - vi * hh.y;
         ai += vr * hh.y + vi * hh.x;
@@ -206,31 +212,33 @@ __global__ void norm_finish(int nchunk, int count, const double *__restrict__ pa
 
 // v_{j+1}[c] = W[k] / h_{j+1,j} (left zero when the norm is zero, as the
 // reference leaves the zero-filled column untouched); H(j+1, j) = norm.
+template <typename VT>
 __global__ void normalize(int n, const int32_t *__restrict__ act, const double *__restrict__ nrm,
-                          const double *__restrict__ W, double *__restrict__ slab_next,
+                          const double *__restrict__ W, VT *__restrict__ slab_next,
                           double2 *__restrict__ Hcol, int hstride, int jrow) {
     int k = blockIdx.y, c = act[k];
     double s = nrm[k];
     double inv = s != 0.0 ? 1.0 / s : 0.0;
     const double *w = W + (int64_t)k * 2 * n;
-    double *v = slab_next + (int64_t)c * 2 * n;
+    VT *v = slab_next + (int64_t)c * 2 * n;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
          r += (int64_t)gridDim.x * blockDim.x)
-        v[r] = s != 0.0 ? w[r] * inv : 0.0;
+        v[r] = (VT)(s != 0.0 ? w[r] * inv : 0.0);
     if (blockIdx.x == 0 && threadIdx.x == 0) Hcol[(int64_t)c * hstride + jrow] = make_double2(s, 0.0);
 }
 
 // v_1 = b / ||b||; g_1 = ||b||.
+template <typename VT>
 __global__ void start_vectors(int n, const int32_t *__restrict__ act, const double *__restrict__ nrm,
-                              const double *__restrict__ B, double *__restrict__ slab0,
+                              const double *__restrict__ B, VT *__restrict__ slab0,
                               double2 *__restrict__ g, int gstride) {
     int k = blockIdx.y, c = act[k];
     double s = nrm[k];
     const double *b = B + (int64_t)c * 2 * n;
-    double *v = slab0 + (int64_t)c * 2 * n;
+    VT *v = slab0 + (int64_t)c * 2 * n;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
          r += (int64_t)gridDim.x * blockDim.x)
-        v[r] = b[r] * (1.0 / s);
+        v[r] = (VT)(b[r] * (1.0 / s));
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         g[(int64_t)c * gstride] = make_double2(s, 0.0);
         for (int i = 1; i < gstride; ++i) g[(int64_t)c * gstride + i] = make_double2(0.0, 0.0);
@@ -356,13 +364,14 @@ int grid_rows(int64_t n2) { return (int)std::min<int64_t>(n_blocks(n2, 256), 102
 
 // combine() over at most kCombine basis vectors per launch (shared-memory bound).
 constexpr int kCombine = 1024;
+template <typename VT>
 int64_t combine_chunked(cudaStream_t st, int n, int i0, int ni, int count, const int32_t *act,
-                        double *const *slabs, const double2 *h, double sign, double *Y, int by_col) {
+                        VT *const *slabs, const double2 *h, double sign, double *Y, int by_col) {
     int64_t launches = 0;
     for (int c0 = 0; c0 < ni; c0 += kCombine) {
         int cn = std::min(kCombine, ni - c0);
         // h is [count][ni]; pass the row stride through a shifted view per chunk
-        combine<<<dim3(n_blocks(n, kThreads), count), kThreads, cn * sizeof(double2), st>>>(
+        combine<VT><<<dim3(n_blocks(n, kThreads), count), kThreads, cn * sizeof(double2), st>>>(
             n, i0 + c0, cn, ni, c0, act, slabs, h, sign, Y, by_col);
         ++launches;
     }
@@ -382,8 +391,8 @@ static void batch_norms(plx_geom *g, int count, const double *V, DevArray<double
     ctx->launches += 2;
 }
 
-void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
-                   GmresResult &res) {
+template <typename VT>
+static void gmres_impl(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X, GmresResult &res) {
     plx_ctx *ctx = g->ctx;
     cudaStream_t st = ctx->stream;
     const int n = g->n_var;
@@ -401,7 +410,8 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     static bool tri_attr = false;
     if (!tri_attr) {
         PLX_CHECK_CUDA(cudaFuncSetAttribute(tri_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        PLX_CHECK_CUDA(cudaFuncSetAttribute(combine, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         tri_attr = true;
     }
     const int hstride = m + 1;   // rows of an H column (0..m)
@@ -422,13 +432,13 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     gv.alloc(ctx, (size_t)C * hstride);
     hbuf.alloc(ctx, (size_t)C * hstride);
     ybuf.alloc(ctx, (size_t)C * hstride);
-    std::vector<DevArray<double>> slabs(m + 1);
+    std::vector<DevArray<VT>> slabs(m + 1);
     std::vector<DevArray<double2>> hcols(m);
-    DevArray<double *> d_slabs;
+    DevArray<VT *> d_slabs;
     DevArray<double2 *> d_hcols;
     d_slabs.alloc(ctx, m + 1);
     d_hcols.alloc(ctx, m);
-    std::vector<double *> h_slabs(m + 1, nullptr);
+    std::vector<VT *> h_slabs(m + 1, nullptr);
     std::vector<double2 *> h_hcols(m, nullptr);
     PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, st));
     DevArray<double> Pinv;
@@ -451,7 +461,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     PLX_CHECK_CUDA(cudaStreamSynchronize(st));
     slabs[0].alloc(ctx, (size_t)C * 2 * n);
     h_slabs[0] = slabs[0].p;
-    start_vectors<<<dim3(grid_rows(2LL * n), C), 256, 0, st>>>(n, d_act.p, nrm.p, d_B, slabs[0].p,
+    start_vectors<VT><<<dim3(grid_rows(2LL * n), C), 256, 0, st>>>(n, d_act.p, nrm.p, d_B, slabs[0].p,
                                                               gv.p, hstride);
     ctx->launches++;
     act.clear();
@@ -474,7 +484,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     for (int j = 0; j < m && !act.empty(); ++j) {
         const int na = (int)act.size();
         // --- w = A v_j for every active column (one batched operator) -----------
-        gather_cols<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, h_slabs[j], Xa.p);
+        gather_cols<VT><<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, h_slabs[j], Xa.p);
         ctx->launches++;
         if (jac) {
             scale_cols<<<dim3(grid_rows(n), na), 256, 0, st>>>(n, d_act.p, Pinv.p, Xa.p, 0);
@@ -487,10 +497,10 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         h_hcols[j] = hcols[j].p;
         slabs[j + 1].alloc(ctx, (size_t)C * 2 * n);
         h_slabs[j + 1] = slabs[j + 1].p;
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p + j + 1, &h_slabs[j + 1], sizeof(double *),
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p + j + 1, &h_slabs[j + 1], sizeof(VT *),
                                        cudaMemcpyHostToDevice, st));
         if (j == 0)
-            PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p, &h_slabs[0], sizeof(double *), cudaMemcpyHostToDevice, st));
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p, &h_slabs[0], sizeof(VT *), cudaMemcpyHostToDevice, st));
         PLX_CHECK_CUDA(cudaMemcpyAsync(d_hcols.p + j, &h_hcols[j], sizeof(double2 *),
                                        cudaMemcpyHostToDevice, st));
         PLX_CHECK_CUDA(cudaMemsetAsync(hcols[j].p, 0, (size_t)C * hstride * 16, st));
@@ -498,7 +508,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         if (part.n < need) part.alloc(ctx, std::max(need, part.n * 2));
         auto project = [&](int i0, int i1, int accumulate) {
             int ni = i1 - i0;
-            dots_partial<<<dim3(ndot, na), kThreads, 0, st>>>(n, i0, i1, d_act.p, d_slabs.p, Wa.p, part.p);
+            dots_partial<VT><<<dim3(ndot, na), kThreads, 0, st>>>(n, i0, i1, d_act.p, d_slabs.p, Wa.p, part.p);
             dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st>>>(ndot, ni, i0, d_act.p, part.p,
                                                                       hbuf.p, hcols[j].p, hstride,
                                                                       accumulate);
@@ -514,7 +524,7 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
         batch_norms(g, na, Wa.p, nrm_part, nrm);
         prof_end(ctx, PROF_ORTHO, 0.0, 0.0);
         prof_begin(ctx);
-        normalize<<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, nrm.p, Wa.p, slabs[j + 1].p,
+        normalize<VT><<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, nrm.p, Wa.p, slabs[j + 1].p,
                                                                hcols[j].p, hstride, j + 1);
         givens<<<n_blocks(na, 128), 128, 0, st>>>(na, j, d_act.p, d_hcols.p, hstride, cs.p, sn.p, gv.p,
                                                  hstride, m, nrm.p);
@@ -590,6 +600,14 @@ void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, doubl
     }
     for (int c : act) res.status[c] = PLX_ERR_NOT_CONVERGED;
     PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+}
+
+void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
+                   GmresResult &res) {
+    if (rq.inner && rq.basis_fp32)
+        gmres_impl<float>(g, rq, d_B, d_X, res);
+    else
+        gmres_impl<double>(g, rq, d_B, d_X, res);
 }
 
 }  // namespace plx

@@ -183,57 +183,104 @@ __global__ void __launch_bounds__(kOtfThreads) otf_contract(int N, int count, in
 // ---------------------------------------------------------------------------
 // Charge rows: y_i = sum_j c_ij (s_j - s_i), c_ij = K_ij (one atom type) or
 // 1/2 (K_ij + (w_tj/w_ti) K_ji) (several types), then + D_q(w) x_i.
-// One warp per (row, column).
+// One warp per row and a chunk of kChargeCols columns.  A row of K holds a few
+// hundred entries (the Fermi damping reaches ~4 nearest-neighbour distances);
+// each lane keeps its share of the row (entries lane, lane + 32, ...) in
+// registers and reuses it for every column, so the CSR is read once per row
+// and chunk instead of once per column.  Per column every lane sums its
+// entries in CSR order and the warp adds the lanes with a fixed butterfly, so
+// a column's result does not depend on the batch it is in.
 // ---------------------------------------------------------------------------
-__global__ void charge_rows(int N, int nt, int nv, int count, int hetero,
-                            const int32_t *__restrict__ freq, const int32_t *__restrict__ type,
-                            const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
-                            const double *__restrict__ kval, const double *__restrict__ ktval,
-                            const Cplx *__restrict__ wratio, const Cplx *__restrict__ dq,
-                            const double *__restrict__ S, const double *__restrict__ X,
-                            double *__restrict__ Y, double sign, int add_diag) {
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    int c = blockIdx.y;
-    int i = warp;
-    if (i >= N || c >= count) return;
-    int f = freq[c];
-    const double *sr = S + (int64_t)c * 2 * nv;
-    const double *si = sr + nv;
-    double s_re = sr[i], s_im = si[i];
-    int ti = type[i];
-    double yre = 0.0, yim = 0.0;
-    for (int e = rowptr[i] + lane; e < rowptr[i + 1]; e += 32) {
-        int j = col[e];
-        double dre = sr[j] - s_re, dim = si[j] - s_im;
-        if (!hetero) {
-            double k = kval[e];
-            yre = fma(k, dre, yre);
-            yim = fma(k, dim, yim);
-        } else {
-            Cplx w = wratio[ti + nt * type[j] + (int64_t)nt * nt * f];
-            double kt = ktval[e];
-            double cre = 0.5 * (kval[e] + w.re * kt), cim = 0.5 * (w.im * kt);
-            yre += cre * dre - cim * dim;
-            yim += cre * dim + cim * dre;
-        }
+constexpr int kChargeCols = 32;
+constexpr int kChargeReg = 16;              // entries per lane held in registers (rows up to 512)
+
+template <bool HETERO>
+__device__ __forceinline__ void charge_term(int nt, int ti, int tj, int f, double k, double kt,
+                                            const Cplx *__restrict__ wratio, double dre, double dim,
+                                            double &yre, double &yim) {
+    if (!HETERO) {
+        yre = fma(k, dre, yre);
+        yim = fma(k, dim, yim);
+    } else {
+        Cplx w = wratio[ti + nt * tj + (int64_t)nt * nt * f];
+        double cre = 0.5 * (k + w.re * kt), cim = 0.5 * (w.im * kt);
+        yre += cre * dre - cim * dim;
+        yim += cre * dim + cim * dre;
     }
+}
+
+template <bool HETERO>
+__global__ void __launch_bounds__(256) charge_rows(int N, int nt, int nv, int count,
+                                                   const int32_t *__restrict__ freq,
+                                                   const int32_t *__restrict__ type,
+                                                   const int32_t *__restrict__ rowptr,
+                                                   const int32_t *__restrict__ col,
+                                                   const double *__restrict__ kval,
+                                                   const double *__restrict__ ktval,
+                                                   const Cplx *__restrict__ wratio, const Cplx *__restrict__ dq,
+                                                   const double *__restrict__ S, const double *__restrict__ X,
+                                                   double *__restrict__ Y, double sign, int add_diag) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    const int c0 = blockIdx.y * kChargeCols;
+    const int c1 = min(count, c0 + kChargeCols);
+    const int e0 = rowptr[i], e1 = rowptr[i + 1];
+    const bool in_reg = e1 - e0 <= 32 * kChargeReg;
+    const int ti = type[i];
+    constexpr int HR = HETERO ? kChargeReg : 1;
+    int rj[kChargeReg], rt[HR];
+    double rk[kChargeReg], rkt[HR];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        yre += __shfl_xor_sync(0xffffffffu, yre, o);
-        yim += __shfl_xor_sync(0xffffffffu, yim, o);
-    }
-    if (lane == 0) {
-        yre *= sign;
-        yim *= sign;
-        if (add_diag) {
-            Cplx d = dq[ti + nt * f];
-            double xr = X[(int64_t)c * 2 * nv + i], xi = X[(int64_t)c * 2 * nv + nv + i];
-            yre += d.re * xr - d.im * xi;
-            yim += d.re * xi + d.im * xr;
+    for (int t = 0; t < kChargeReg; ++t) {
+        const int e = e0 + lane + 32 * t;
+        const bool live = in_reg && e < e1;
+        rj[t] = live ? col[e] : 0;
+        rk[t] = live ? kval[e] : 0.0;
+        if (HETERO) {
+            rkt[t % HR] = live ? ktval[e] : 0.0;
+            rt[t % HR] = live ? type[rj[t]] : 0;
         }
-        Y[(int64_t)c * 2 * nv + i] = yre;
-        Y[(int64_t)c * 2 * nv + nv + i] = yim;
+    }
+    for (int c = c0; c < c1; ++c) {
+        const int f = freq[c];
+        const double *sr = S + (int64_t)c * 2 * nv;
+        const double *si = sr + nv;
+        const double s_re = sr[i], s_im = si[i];
+        double yre = 0.0, yim = 0.0;
+        if (in_reg) {
+#pragma unroll
+            for (int t = 0; t < kChargeReg; ++t) {
+                if (e0 + lane + 32 * t < e1) {
+                    const int j = rj[t];
+                    charge_term<HETERO>(nt, ti, HETERO ? rt[t % HR] : 0, f, rk[t], HETERO ? rkt[t % HR] : 0.0,
+                                        wratio, sr[j] - s_re, si[j] - s_im, yre, yim);
+                }
+            }
+        } else {
+            for (int e = e0 + lane; e < e1; e += 32) {
+                const int j = col[e];
+                charge_term<HETERO>(nt, ti, HETERO ? type[j] : 0, f, kval[e], HETERO ? ktval[e] : 0.0, wratio,
+                                    sr[j] - s_re, si[j] - s_im, yre, yim);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            yre += __shfl_xor_sync(0xffffffffu, yre, o);
+            yim += __shfl_xor_sync(0xffffffffu, yim, o);
+        }
+        if (lane == 0) {
+            yre *= sign;
+            yim *= sign;
+            if (add_diag) {
+                const Cplx d = dq[ti + nt * f];
+                const double xr = X[(int64_t)c * 2 * nv + i], xi = X[(int64_t)c * 2 * nv + nv + i];
+                yre += d.re * xr - d.im * xi;
+                yim += d.re * xi + d.im * xr;
+            }
+            Y[(int64_t)c * 2 * nv + i] = yre;
+            Y[(int64_t)c * 2 * nv + nv + i] = yim;
+        }
     }
 }
 
@@ -260,6 +307,36 @@ __global__ void dipole_rows(int N, int nt, int nv, int count, const int32_t *__r
     double xr = xc[r], xi = xc[nv + r];
     Y[(int64_t)c * 2 * nv + r] = sc[r] + zre * xr - zim * xi;
     Y[(int64_t)c * 2 * nv + nv + r] = sc[nv + r] + zre * xi + zim * xr;
+}
+
+// Rows after a contraction with the folded A0 = blockdiag(K - P, I) T (one atom
+// type): only the diagonal D(w) is left, y = s + D(w) x, with -z(w) on the
+// charge rows and sum_t f_t,i / alpha_t(w) on the dipole rows.
+__global__ void folded_rows(int N, int nt, int nv, int count, const int32_t *__restrict__ freq,
+                            const int32_t *__restrict__ type, const Cplx *__restrict__ dq,
+                            const double *__restrict__ frac, const Cplx *__restrict__ inv_alpha,
+                            const double *__restrict__ S, const double *__restrict__ X,
+                            double *__restrict__ Y) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= nv || c >= count) return;
+    const int f = freq[c];
+    Cplx d = {0.0, 0.0};
+    if (r < N) {
+        d = dq[type[r] + nt * f];
+    } else {
+        const int i = (r - N) / 3;
+        for (int t = 0; t < nt; ++t) {
+            const double fr = frac[t + (int64_t)nt * i];
+            const Cplx a = inv_alpha[t + nt * f];
+            d.re += fr * a.re;
+            d.im += fr * a.im;
+        }
+    }
+    const int64_t base = (int64_t)c * 2 * nv;
+    const double xr = X[base + r], xi = X[base + nv + r];
+    Y[base + r] = S[base + r] + d.re * xr - d.im * xi;
+    Y[base + nv + r] = S[base + nv + r] + d.re * xi + d.im * xr;
 }
 
 // Static potential V_i (field along pol) for the right-hand side.
@@ -485,8 +562,8 @@ static void finish_rows(plx_geom *g, const OpBatch &b, const double *S, const do
     plx_ctx *ctx = g->ctx;
     cudaStream_t st = ctx->stream;
     const int N = g->n_atoms, nv = g->n_var;
-    dim3 gq(n_blocks((int64_t)N * 32, 256), b.count);
-    charge_rows<<<gq, 256, 0, st>>>(N, g->n_types, nv, b.count, g->n_types > 1, b.d_freq,
+    dim3 gq(n_blocks((int64_t)N * 32, 256), n_blocks(b.count, kChargeCols));
+    (g->n_types > 1 ? charge_rows<true> : charge_rows<false>)<<<gq, 256, 0, st>>>(N, g->n_types, nv, b.count, b.d_freq,
                                     g->d_type.p, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
                                     g->d_ktval.p, g->d_wratio.p, g->d_dq.p, S, X, Y, 1.0, 1);
     ctx->launches++;
@@ -502,6 +579,24 @@ static void finish_rows(plx_geom *g, const OpBatch &b, const double *S, const do
 void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, double *work,
                     Contraction how) {
     if (b.count == 0) return;
+    if ((how == Contraction::TC3 || how == Contraction::TC1) && tc_folds_operator(g)) {
+        // A(w) X = A0 X + D(w) X: one tensor-core contraction with the folded
+        // matrix and a diagonal pass (no conductance rows per application)
+        plx_ctx *ctx = g->ctx;
+        const double nn = (double)g->n_var;
+        prof_begin(ctx);
+        tc_contract(g, b.count, X, work, how == Contraction::TC3 ? 3 : 1, true);
+        prof_end(ctx, PROF_TC, 2.0 * nn * nn * 2.0 * b.count,
+                 (how == Contraction::TC3 ? 4.0 : 2.0) * nn * (double)g->ldk + 2.0 * 8.0 * nn * 2.0 * b.count);
+        prof_begin(ctx);
+        folded_rows<<<dim3(n_blocks(g->n_var, 256), b.count), 256, 0, ctx->stream>>>(
+            g->n_atoms, g->n_types, g->n_var, b.count, b.d_freq, g->d_type.p, g->d_dq.p, g->d_frac.p,
+            g->d_inv_alpha.p, work, X, Y);
+        ctx->launches++;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        prof_end(ctx, PROF_ROWS, 0.0, 0.0);
+        return;
+    }
     contract_t(g, b.count, X, work, how);
     prof_begin(g->ctx);
     if (is_bem(g))
@@ -531,9 +626,9 @@ void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout
     V.alloc(ctx, (size_t)b.count * 2 * nv);
     potential_kernel<<<dim3(n_blocks(nv, 256), b.count), 256, 0, st>>>(
         N, nv, b.count, d_pol, g->d_pos.p, g->e0, g->rhs_potential, mn[0], mn[1], mn[2], V.p);
-    dim3 gq(n_blocks((int64_t)N * 32, 256), b.count);
+    dim3 gq(n_blocks((int64_t)N * 32, 256), n_blocks(b.count, kChargeCols));
     // b_q = -Kop(w) V  (rhs_module.f90:140-390); no diagonal term
-    charge_rows<<<gq, 256, 0, st>>>(N, g->n_types, nv, b.count, g->n_types > 1, b.d_freq,
+    (g->n_types > 1 ? charge_rows<true> : charge_rows<false>)<<<gq, 256, 0, st>>>(N, g->n_types, nv, b.count, b.d_freq,
                                     g->d_type.p, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
                                     g->d_ktval.p, g->d_wratio.p, g->d_dq.p, V.p, V.p, Bout, -1.0, 0);
     ctx->launches += 2;

@@ -127,6 +127,10 @@ struct plx_geom {
     // and the error word of the tensor-core kernel
     plx::DevArray<uint16_t> d_Th, d_Tl, d_Xh, d_Xl;
     int64_t ldk = 0;
+    // one atom type: the operator's frequency-independent matrix
+    // A0 = blockdiag(K - P, I) T folded once and split like T, so that a
+    // tensor-core application of A(w) is one contraction plus the diagonal
+    plx::DevArray<uint16_t> d_Ah, d_Al;
     plx::DevArray<int> d_tc_err;
     // diagonal of blockdiag(Kop, I) T on the charge rows, frequency independent parts:
     // a_i = sum_j K_ij (T_ij - T_ii), b_i,t = sum_{j of type t} K_ji (T_ij - T_ii)
@@ -177,7 +181,11 @@ void diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv);
 // tc_contract.cu: S = T X with BF16-split operands on the tensor cores
 // (nprod 3: Th Xh + Th Xl + Tl Xh; nprod 1: Th Xh).  X, S: [count][2][n] FP64.
 void build_t_split(plx_geom *g);
-void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod);
+void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded = false);
+// true when apply_operator contracts with the folded A0 on the tensor cores
+inline bool tc_folds_operator(const plx_geom *g) {
+    return (g->model == PLX_WFQ || g->model == PLX_WFQFMU) && g->n_types == 1 && g->has_T;
+}
 int tc_error(plx_geom *g);   // non-zero when a tensor-core CTA gave up waiting
 
 // inversion.cu
@@ -212,6 +220,8 @@ struct GmresRequest {
     // right preconditioning by the inverse diagonal of A(w) (inner solves only):
     // the operator becomes A P^-1 and the returned correction P^-1 y
     bool jacobi = false;
+    // inner solves only: Krylov basis stored in FP32
+    bool basis_fp32 = false;
 };
 struct GmresResult {
     std::vector<int32_t> status, steps;

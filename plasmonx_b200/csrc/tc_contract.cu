@@ -289,6 +289,34 @@ __global__ void split_bf16_t(int n, const double *__restrict__ in, int64_t ld_ou
     }
 }
 
+// Folded operator rows, split like T: for a charge row i < N
+//   A0[i][k] = sum_e K_e (T[j_e][k] - T[i][k])      (CSR order, FP64)
+// (the charge rows of (K - P) T, update_y_q of matrix_module.f90:1011-1098
+// applied to T itself), for a dipole row A0[r][k] = T[r][k]; zero for k >= n.
+// One block per (row, column chunk); rows vary fastest over the grid, so the
+// blocks running together share their neighbours' rows of T in L2.
+__global__ void fold_split(int N, int n, int64_t ld, const int32_t *__restrict__ rowptr,
+                           const int32_t *__restrict__ col, const double *__restrict__ kval,
+                           const double *__restrict__ T, __nv_bfloat16 *__restrict__ hi,
+                           __nv_bfloat16 *__restrict__ lo) {
+    const int r = blockIdx.x;
+    const int64_t k = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+    if (k >= ld) return;
+    double a = 0.0;
+    if (k < n) {
+        const double trk = T[(int64_t)r * n + k];
+        if (r < N) {
+            for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) a = fma(kval[e], T[(int64_t)col[e] * n + k] - trk, a);
+        } else {
+            a = trk;
+        }
+    }
+    float x = (float)a;
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi[(int64_t)r * ld + k] = h;
+    lo[(int64_t)r * ld + k] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
 // FP64 -> (BF16 high, BF16 low) split of a row-major [rows][cols] array into a
 // zero-padded [rows_pad][ld] pair.
 __global__ void split_bf16(int rows, int cols, int64_t ld_in, const double *__restrict__ in, int rows_pad,
@@ -376,12 +404,37 @@ void build_t_split(plx_geom *g) {
     }
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
-    g->d_tc_err.alloc(g->ctx, 1);
-    PLX_CHECK_CUDA(cudaMemsetAsync(g->d_tc_err.p, 0, sizeof(int), g->ctx->stream));
+    if (!g->d_tc_err.p) {
+        g->d_tc_err.alloc(g->ctx, 1);
+        PLX_CHECK_CUDA(cudaMemsetAsync(g->d_tc_err.p, 0, sizeof(int), g->ctx->stream));
+    }
 }
 
-void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod) {
-    build_t_split(g);
+static void build_a_split(plx_geom *g) {
+    if (g->d_Ah.p) return;
+    if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
+    const int64_t n = g->n_var;
+    const int64_t ld = (n + kBK - 1) / kBK * kBK;
+    g->ldk = ld;
+    g->d_Ah.alloc(g->ctx, (size_t)(n * ld));
+    g->d_Al.alloc(g->ctx, (size_t)(n * ld));
+    dim3 grid((unsigned)n, (unsigned)((ld + 255) / 256));
+    fold_split<<<grid, 256, 0, g->ctx->stream>>>(g->n_atoms, (int)n, ld, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
+                                                  g->d_T.p, reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p),
+                                                  reinterpret_cast<__nv_bfloat16 *>(g->d_Al.p));
+    g->ctx->launches++;
+    PLX_CHECK_CUDA(cudaGetLastError());
+    if (!g->d_tc_err.p) {
+        g->d_tc_err.alloc(g->ctx, 1);
+        PLX_CHECK_CUDA(cudaMemsetAsync(g->d_tc_err.p, 0, sizeof(int), g->ctx->stream));
+    }
+}
+
+void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded) {
+    if (folded)
+        build_a_split(g);
+    else
+        build_t_split(g);
     plx_ctx *ctx = g->ctx;
     const int n = g->n_var;
     const int R = 2 * count;
@@ -399,8 +452,8 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod) 
         R, n, n, X, Rpad, ld, reinterpret_cast<__nv_bfloat16 *>(g->d_Xh.p),
         reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
     ctx->launches++;
-    CUtensorMap th = make_map(g->d_Th.p, ld, n, ld, kBM);
-    CUtensorMap tl = make_map(g->d_Tl.p, ld, n, ld, kBM);
+    CUtensorMap th = make_map(folded ? g->d_Ah.p : g->d_Th.p, ld, n, ld, kBM);
+    CUtensorMap tl = make_map(folded ? g->d_Al.p : g->d_Tl.p, ld, n, ld, kBM);
     CUtensorMap xh = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
     CUtensorMap xl = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
     const int ktiles = (int)(ld / kBK);

@@ -137,7 +137,10 @@ def test_solve_matches_oracle(ctx, name):
 def test_tight_gmres_matches_lu(ctx, name, mode):
     """sigma_abs of the FP64 GPU solves at tight tolerances against the oracle LU:
     the reference's (unrestarted) GMRES at a 1e-11 relative residual within 1e-9,
-    and the FP64 refinement (restarted, explicit FP64 residuals) at 1e-13 within 1e-10."""
+    and the FP64 refinement (restarted, explicit FP64 residuals) at 1e-12 within 1e-10.
+    (The explicit FP64 residual of the sodium operator bottoms out near 1e-13 of |b|,
+    since the charge rows difference neighbouring potentials: 1e-13 is not reliably
+    attainable there, while the answer is already accurate to ~2e-13.)"""
     p, s = _pair(name)
     F = len(p.freqs)
     freqs = list(range(F // 2, F, max(1, F // 10)))      # away from the w -> 0 singularity
@@ -148,7 +151,7 @@ def test_tight_gmres_matches_lu(ctx, name, mode):
         sv.set_frequencies(p.freqs[freqs], None if p.alpha_w is None else p.alpha_w[:, freqs])
         nb = np.linalg.norm(sv.rhs(0, 7)[:, 0])
         plain = sv.solve(mode=mode, tol=1e-11 * nb, max_krylov=p.n_var)
-        refined = sv.solve(mode=mode, precision='fp64_refined', tol=1e-13 * nb, inner_krylov=p.n_var,
+        refined = sv.solve(mode=mode, precision='fp64_refined', tol=1e-12 * nb, inner_krylov=p.n_var,
                            inner_tol=1e-13, max_outer=10)
     for out, bar in ((plain, 1e-9), (refined, 1e-10)):
         assert (out['status'] == 0).all(), out['status']
