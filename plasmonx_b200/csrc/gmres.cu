@@ -519,7 +519,7 @@ static void gmres_impl(plx_geom *g, const GmresRequest &rq, const double *d_B, d
             for (int i = 0; i <= j; ++i) project(i, i + 1, 0);        // modified Gram-Schmidt
         } else {
             project(0, j + 1, 0);                                     // classical GS ...
-            project(0, j + 1, 1);                                     // ... and re-orthogonalise
+            if (!rq.single_pass) project(0, j + 1, 1);                // ... and re-orthogonalise
         }
         batch_norms(g, na, Wa.p, nrm_part, nrm);
         prof_end(ctx, PROF_ORTHO, 0.0, 0.0);

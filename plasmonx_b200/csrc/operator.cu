@@ -17,57 +17,91 @@ namespace plx {
 namespace {
 
 // ---------------------------------------------------------------------------
-// S^T = X^T T, tiled (R > 16): 64 x 64 output tiles, 4 x 4 per thread, split
-// over K in the SAME chunks as skinny_partial and reduced by skinny_reduce, so
-// every output element is accumulated in the same order whatever the number of
-// columns in the batch: a column's result does not depend on the batch it is in.
+// S^T = X^T T, tiled (R > 16): 64 x 128 output tiles, 8 x 8 per thread (four
+// FMAs per shared-memory load, which keeps the FP64 pipe rather than shared
+// memory the limit), the next k-slab prefetched into registers while the
+// current one is multiplied.  Split over K in the SAME chunks as
+// skinny_partial and reduced by skinny_reduce, and every output element is
+// accumulated by one FMA chain in k order from zero, exactly as
+// skinny_partial does, so a column's result does not depend on the number of
+// columns in the batch.
 // ---------------------------------------------------------------------------
-constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int BM = 64, BN = 128, BK = 8, kTiledThreads = 128;
 
-__global__ void __launch_bounds__(256) tiled_partial(int R, int n, int kchunk,
-                                                     const double *__restrict__ Xt,
-                                                     const double *__restrict__ T,
-                                                     double *__restrict__ part) {
-    __shared__ double As[BK][BM + 1];
-    __shared__ double Bs[BK][BN];
-    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
-    int kbeg = blockIdx.z * kchunk, kend = min(n, kbeg + kchunk);
-    double acc[4][4] = {};
+__global__ void __launch_bounds__(kTiledThreads) tiled_partial(int R, int n, int kchunk,
+                                                               const double *__restrict__ Xt,
+                                                               const double *__restrict__ T,
+                                                               double *__restrict__ part) {
+    __shared__ double As[2][BM][BK + 1];
+    __shared__ double Bs[2][BK][BN];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;          // 16 x 8 threads
+    const int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+    const int kbeg = blockIdx.z * kchunk, kend = min(n, kbeg + kchunk);
+    constexpr int LA = BM * BK / kTiledThreads, LB = BK * BN / kTiledThreads;   // 4, 8
+    double ra[LA], rb[LB];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            const int e = threadIdx.x + q * kTiledThreads, r = e / BK, k = e % BK;
+            const int gr = row0 + r, gk = k0 + k;
+            ra[q] = (gr < R && gk < kend) ? Xt[(int64_t)gr * n + gk] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int e = threadIdx.x + q * kTiledThreads, k = e / BN, c = e % BN;
+            const int gk = k0 + k, gc = col0 + c;
+            rb[q] = (gk < kend && gc < n) ? T[(int64_t)gk * n + gc] : 0.0;
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            const int e = threadIdx.x + q * kTiledThreads;
+            As[buf][e / BK][e % BK] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int e = threadIdx.x + q * kTiledThreads;
+            Bs[buf][e / BN][e % BN] = rb[q];
+        }
+    };
+    double acc[8][8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[u][v] = 0.0;
+    if (kbeg < kend) {
+        load(kbeg);
+        store(0);
+    }
+    __syncthreads();
+    int buf = 0;
     for (int k0 = kbeg; k0 < kend; k0 += BK) {
-        for (int e = threadIdx.x; e < BM * BK; e += 256) {
-            int r = e / BK, k = e % BK;
-            int gr = row0 + r, gk = k0 + k;
-            As[k][r] = (gr < R && gk < kend) ? Xt[(int64_t)gr * n + gk] : 0.0;
-        }
-        for (int e = threadIdx.x; e < BK * BN; e += 256) {
-            int k = e / BN, c = e % BN;
-            int gk = k0 + k, gc = col0 + c;
-            Bs[k][c] = (gk < kend && gc < n) ? T[(int64_t)gk * n + gc] : 0.0;
-        }
-        __syncthreads();
-        int kn = min(BK, kend - k0);
+        const bool more = k0 + BK < kend;
+        if (more) load(k0 + BK);
+        const int kn = min(BK, kend - k0);
         for (int k = 0; k < kn; ++k) {
-            double a[4], b[4];
+            double a[8], b[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                a[u] = As[k][ty * 4 + u];
-                b[u] = Bs[k][tx + 16 * u];
-            }
+            for (int u = 0; u < 8; ++u) a[u] = As[buf][ty * 8 + u][k];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int v = 0; v < 8; ++v) b[v] = Bs[buf][k][tx + 16 * v];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int v = 0; v < 8; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
         }
+        if (more) store(buf ^ 1);
         __syncthreads();
+        buf ^= 1;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        int gr = row0 + ty * 4 + u;
+    for (int u = 0; u < 8; ++u) {
+        const int gr = row0 + ty * 8 + u;
         if (gr >= R) continue;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            int gc = col0 + tx + 16 * v;
+        for (int v = 0; v < 8; ++v) {
+            const int gc = col0 + tx + 16 * v;
             if (gc < n) part[((int64_t)blockIdx.z * R + gr) * n + gc] = acc[u][v];
         }
     }
@@ -550,7 +584,7 @@ void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on
         }
     } else {
         dim3 grid(n_blocks(n, BN), n_blocks(R, BM), ks);
-        tiled_partial<<<grid, 256, 0, st>>>(R, n, kchunk, X, g->d_T.p, part);
+        tiled_partial<<<grid, kTiledThreads, 0, st>>>(R, n, kchunk, X, g->d_T.p, part);
     }
     skinny_reduce<<<n_blocks((int64_t)R * n, 256), 256, 0, st>>>(n, R, ks, part, S);
     ctx->launches += 2;

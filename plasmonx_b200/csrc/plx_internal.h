@@ -220,8 +220,11 @@ struct GmresRequest {
     // right preconditioning by the inverse diagonal of A(w) (inner solves only):
     // the operator becomes A P^-1 and the returned correction P^-1 y
     bool jacobi = false;
-    // inner solves only: Krylov basis stored in FP32
+    // inner solves only: Krylov basis stored in FP32, and classical Gram-Schmidt
+    // without the second pass (the inner tolerance is loose and the refinement's
+    // FP64 residual catches what a less orthogonal basis loses)
     bool basis_fp32 = false;
+    bool single_pass = false;
 };
 struct GmresResult {
     std::vector<int32_t> status, steps;
@@ -243,6 +246,7 @@ struct RefineRequest {
     Contraction inner_contraction = Contraction::TC3;
     Contraction outer_contraction = Contraction::FP64;
     bool jacobi = true;      // diagonal right preconditioning of the inner solves
+    bool single_pass_gs = true;   // tensor-core inner solves: one classical Gram-Schmidt pass
 };
 struct RefineResult {
     std::vector<int32_t> status, inner_steps, outer;
