@@ -131,6 +131,8 @@ struct plx_geom {
     // A0 = blockdiag(K - P, I) T folded once and split like T, so that a
     // tensor-core application of A(w) is one contraction plus the diagonal
     plx::DevArray<uint16_t> d_Ah, d_Al;
+    // k-split partial sums of the tensor-core contraction ([splits][R][n_var])
+    plx::DevArray<double> d_tcpart;
     plx::DevArray<int> d_tc_err;
     // diagonal of blockdiag(Kop, I) T on the charge rows, frequency independent parts:
     // a_i = sum_j K_ij (T_ij - T_ii), b_i,t = sum_{j of type t} K_ji (T_ij - T_ii)

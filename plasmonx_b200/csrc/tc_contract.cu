@@ -131,8 +131,13 @@ template <int BN, int STAGES, int NPROD>
 __global__ void __launch_bounds__(128, 1)
     tc_contract_kernel(const __grid_constant__ CUtensorMap mapTh, const __grid_constant__ CUtensorMap mapTl,
                        const __grid_constant__ CUtensorMap mapXh, const __grid_constant__ CUtensorMap mapXl,
-                       int M, int R, int ktiles, double *__restrict__ S, int ldS, int *__restrict__ err) {
+                       int M, int R, int ktiles, int kper, double *__restrict__ S, int ldS, int64_t split_stride,
+                       int *__restrict__ err) {
     using L = TcSmem<BN, STAGES>;
+    // split over k: this CTA accumulates k-tiles [kt0, kt0 + nk) into its own partial
+    const int kt0 = blockIdx.z * kper;
+    const int nk = min(ktiles, kt0 + kper) - kt0;
+    S += (int64_t)blockIdx.z * split_stride;
     constexpr uint32_t kTmemCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(128, 1)
     if (threadIdx.x == 0) {
         // ---------------- TMA producer ----------------
         int issued = 0;
-        for (int kt = 0; kt < ktiles; ++kt) {
+        for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
             if (kt >= STAGES) {
                 if (!mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1, err, 1) || *abort_flag) {
@@ -184,7 +189,7 @@ __global__ void __launch_bounds__(128, 1)
                 }
             }
             mbar_expect_tx(&full[s], (uint32_t)L::kStage);
-            const int kx = kt * kBK;
+            const int kx = (kt0 + kt) * kBK;
             tma_load_2d(&mapTh, &full[s], stage_ptr(s, 0), kx, m0);
             tma_load_2d(&mapTl, &full[s], stage_ptr(s, 1), kx, m0);
             tma_load_2d(&mapXh, &full[s], stage_ptr(s, 2), kx, n0);
@@ -200,7 +205,7 @@ __global__ void __launch_bounds__(128, 1)
         // ---------------- MMA issuer ----------------
         constexpr uint32_t idesc = umma_idesc_bf16(kBM, BN);
         bool ok = true;
-        for (int kt = 0; kt < ktiles && ok; ++kt) {
+        for (int kt = 0; kt < nk && ok; ++kt) {
             const int s = kt % STAGES;
             if (!mbar_wait(&full[s], (kt / STAGES) & 1, err, 2) || *abort_flag) {
                 *abort_flag = 1;
@@ -364,7 +369,7 @@ CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t l
 
 template <int BN, int NPROD>
 void launch_bn(plx_geom *g, int R, const CUtensorMap &th, const CUtensorMap &tl, const CUtensorMap &xh,
-               const CUtensorMap &xl, int ktiles, double *S, int *err) {
+               const CUtensorMap &xl, int ktiles, int splits, int kper, double *S, int *err) {
     constexpr int ST = tc_stages<BN>();
     using L = TcSmem<BN, ST>;
     auto kern = tc_contract_kernel<BN, ST, NPROD>;
@@ -373,10 +378,47 @@ void launch_bn(plx_geom *g, int R, const CUtensorMap &th, const CUtensorMap &tl,
         PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
         attr = true;
     }
-    dim3 grid((R + BN - 1) / BN, (g->n_var + kBM - 1) / kBM);
-    kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, g->n_var, R, ktiles, S, g->n_var, err);
+    dim3 grid((R + BN - 1) / BN, (g->n_var + kBM - 1) / kBM, splits);
+    kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, g->n_var, R, ktiles, kper, S, g->n_var,
+                                                   (int64_t)R * g->n_var, err);
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
+}
+
+// S = sum_z P[z] over the k-split partials, in split order.
+__global__ void reduce_splits(int64_t count, int splits, const double *__restrict__ P, double *__restrict__ S) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+        double a = P[e];
+        for (int z = 1; z < splits; ++z) a += P[(int64_t)z * count + e];
+        S[e] = a;
+    }
+}
+
+int sm_count(int device) {
+    static int cached_dev = -1, cached = 0;
+    if (device != cached_dev) {
+        PLX_CHECK_CUDA(cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, device));
+        cached_dev = device;
+    }
+    return cached;
+}
+
+// Number of k-splits for `tiles` output tiles: the fewest whose last wave fills
+// at least 90% of the SMs (one CTA per SM), keeping >= 16 k-tiles per split.
+int choose_splits(int tiles, int ktiles, int sms) {
+    int best = 1;
+    double best_eff = 0.0;
+    for (int s = 1; s <= 4; ++s) {
+        if (s > 1 && ktiles / s < 16) break;
+        const int64_t ctas = (int64_t)tiles * s;
+        const double eff = (double)ctas / (double)(((ctas + sms - 1) / sms) * sms);
+        if (eff >= 0.9) return s;
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = s;
+        }
+    }
+    return best;
 }
 
 }  // namespace
@@ -458,16 +500,33 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
     CUtensorMap xl = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
     const int ktiles = (int)(ld / kBK);
     int *err = g->d_tc_err.p;
-#define PLX_TC(BNV)                                                                       \
-    case BNV:                                                                             \
-        if (nprod == 1) launch_bn<BNV, 1>(g, R, th, tl, xh, xl, ktiles, S, err);           \
-        else launch_bn<BNV, 3>(g, R, th, tl, xh, xl, ktiles, S, err);                      \
+    // k-splits against wave quantisation; partials reduced in a fixed order
+    const int tiles = ntile * (int)((n + kBM - 1) / kBM);
+    int splits = choose_splits(tiles, ktiles, sm_count(ctx->device));
+    const int kper = (ktiles + splits - 1) / splits;
+    splits = (ktiles + kper - 1) / kper;
+    double *out = S;
+    if (splits > 1) {
+        const size_t pn = (size_t)splits * R * n;
+        if (g->d_tcpart.n < pn) g->d_tcpart.alloc(ctx, pn);
+        out = g->d_tcpart.p;
+    }
+#define PLX_TC(BNV)                                                                               \
+    case BNV:                                                                                     \
+        if (nprod == 1) launch_bn<BNV, 1>(g, R, th, tl, xh, xl, ktiles, splits, kper, out, err);  \
+        else launch_bn<BNV, 3>(g, R, th, tl, xh, xl, ktiles, splits, kper, out, err);             \
         break;
     switch (bn) {
         PLX_TC(32) PLX_TC(64) PLX_TC(96) PLX_TC(128) PLX_TC(160) PLX_TC(192) PLX_TC(224) PLX_TC(256)
         default: throw Error(PLX_ERR_ARG, "bad column tile");
     }
 #undef PLX_TC
+    if (splits > 1) {
+        const int64_t cnt = (int64_t)R * n;
+        reduce_splits<<<(int)std::min<int64_t>(4096, n_blocks(cnt, 256)), 256, 0, ctx->stream>>>(cnt, splits, out, S);
+        ctx->launches++;
+        PLX_CHECK_CUDA(cudaGetLastError());
+    }
 }
 
 int tc_error(plx_geom *g) {
