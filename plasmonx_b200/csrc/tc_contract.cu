@@ -10,11 +10,14 @@
 // GEMM mapping (all operands K-major, the layout tcgen05 reads natively):
 //   A = T   rows m of T, contiguous along k         (M = n_var)
 //   B = X^T column c of X, contiguous along k        (N = R real columns)
-//   D = TMEM accumulator 128 x BN (FP32), lane = row m, column = c
-// One CTA computes a 128 x BN tile of S; 4 warps: thread 0 issues the TMA
+//   D = TMEM accumulators 128 x BN (FP32), lane = row m, column = c
+// One CTA computes a 256 x BN tile of S as two 128-row accumulators (TMEM
+// columns [0, BN) and [BN, 2 BN)) that share every B tile, which halves the
+// B traffic from L2 per row of T; 4 warps: thread 0 issues the TMA
 // loads, thread 32 issues the MMAs, all 128 threads drain TMEM in the
-// epilogue.  Operand tiles are 64 elements (128 bytes) deep along k and are
-// loaded by TMA with the 128-byte swizzle that the UMMA descriptors describe.
+// epilogue.  Operand tiles are 32 elements (64 bytes) deep along k and are
+// loaded by TMA with the 64-byte swizzle that the UMMA descriptors describe;
+// the small stages allow 4-6 of them in flight.
 // Every wait on an mbarrier is bounded; a CTA that gives up records an error
 // code, waits (bounded) for its outstanding loads, frees its tensor memory and
 // returns.
@@ -29,8 +32,10 @@ namespace plx {
 
 namespace {
 
-constexpr int kBM = 128;          // rows of T per CTA (TMEM lanes)
-constexpr int kBK = 64;           // k per stage (128 bytes of BF16)
+constexpr int kUM = 128;          // rows per tcgen05.mma (TMEM lanes)
+constexpr int kBM = 2 * kUM;      // rows of T per CTA: two accumulators share every B tile
+constexpr int kBK = 32;           // k per stage (64 bytes of BF16: the 64-byte swizzle atom)
+constexpr int kLdAlign = 64;      // k padding of the split operands (zeros)
 constexpr int kUmmaK = 16;        // k per tcgen05.mma (kind::f16)
 constexpr uint32_t kSpinLimit = 1u << 22;   // bounded waits (seconds at most)
 
@@ -75,17 +80,18 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
-// UMMA shared-memory descriptor, K-major operand with the 128-byte swizzle:
-// 8-row x 128-byte swizzle atoms stacked every 1024 bytes (stride byte offset),
-// leading byte offset 16 bytes (unused for this layout), descriptor version 1.
-__device__ __forceinline__ uint64_t umma_desc_sw128(const void *smem) {
+// UMMA shared-memory descriptor, K-major operand with the 64-byte swizzle:
+// 8-row x 64-byte swizzle atoms stacked every 512 bytes (stride byte offset),
+// leading byte offset 16 bytes (unused for this layout), descriptor version 1,
+// layout type 4 (64-byte swizzle) in bits [61,64).
+__device__ __forceinline__ uint64_t umma_desc_sw64(const void *smem) {
     uint64_t addr = smem_u32(smem);
     uint64_t d = 0;
     d |= (addr >> 4) & 0x3FFFull;           // start address, bits [0,14)
     d |= (uint64_t)(16 >> 4) << 16;         // leading byte offset, bits [16,30)
-    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset, bits [32,46)
+    d |= (uint64_t)(512 >> 4) << 32;        // stride byte offset, bits [32,46)
     d |= (uint64_t)1 << 46;                 // version, bits [46,48)
-    d |= (uint64_t)2 << 61;                 // layout: 128-byte swizzle
+    d |= (uint64_t)4 << 61;                 // layout: 64-byte swizzle
     return d;
 }
 
@@ -124,7 +130,7 @@ struct TcSmem {
 
 template <int BN>
 constexpr int tc_stages() {
-    return std::min(4, (200 * 1024) / TcSmem<BN, 1>::kStage);
+    return std::min(6, (200 * 1024) / TcSmem<BN, 1>::kStage);
 }
 
 template <int BN, int STAGES, int NPROD>
@@ -138,7 +144,8 @@ __global__ void __launch_bounds__(128, 1)
     const int kt0 = blockIdx.z * kper;
     const int nk = min(ktiles, kt0 + kper) - kt0;
     S += (int64_t)blockIdx.z * split_stride;
-    constexpr uint32_t kTmemCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    // two accumulators of BN columns each (rows m0.. and m0 + 128..)
+    constexpr uint32_t kTmemCols = 2 * BN <= 64 ? 64 : (2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * L::kStage);
@@ -203,7 +210,8 @@ __global__ void __launch_bounds__(128, 1)
         }
     } else if (threadIdx.x == 32) {
         // ---------------- MMA issuer ----------------
-        constexpr uint32_t idesc = umma_idesc_bf16(kBM, BN);
+        constexpr uint32_t idesc = umma_idesc_bf16(kUM, BN);
+        constexpr uint64_t kHalf = (uint64_t)(kUM * kBK * 2) >> 4;   // second 128 rows of an A tile
         bool ok = true;
         for (int kt = 0; kt < nk && ok; ++kt) {
             const int s = kt % STAGES;
@@ -213,19 +221,24 @@ __global__ void __launch_bounds__(128, 1)
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint64_t dTh = umma_desc_sw128(stage_ptr(s, 0));
-            const uint64_t dTl = umma_desc_sw128(stage_ptr(s, 1));
-            const uint64_t dXh = umma_desc_sw128(stage_ptr(s, 2));
-            const uint64_t dXl = umma_desc_sw128(stage_ptr(s, 3));
+            const uint64_t dTh = umma_desc_sw64(stage_ptr(s, 0));
+            const uint64_t dTl = umma_desc_sw64(stage_ptr(s, 1));
+            const uint64_t dXh = umma_desc_sw64(stage_ptr(s, 2));
+            const uint64_t dXl = umma_desc_sw64(stage_ptr(s, 3));
 #pragma unroll
             for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
                 // advance 16 elements = 32 bytes = 2 descriptor units along k
                 const uint64_t off = (uint64_t)(kk * kUmmaK * 2) >> 4;
                 const uint32_t acc0 = (kt > 0 || kk > 0) ? 1u : 0u;
-                umma_bf16(tmem, dTh + off, dXh + off, idesc, acc0);
-                if (NPROD > 1) {
-                    umma_bf16(tmem, dTh + off, dXl + off, idesc, 1u);
-                    umma_bf16(tmem, dTl + off, dXh + off, idesc, 1u);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t td = tmem + (uint32_t)(h * BN);
+                    const uint64_t ho = h * kHalf;
+                    umma_bf16(td, dTh + ho + off, dXh + off, idesc, acc0);
+                    if (NPROD > 1) {
+                        umma_bf16(td, dTh + ho + off, dXl + off, idesc, 1u);
+                        umma_bf16(td, dTl + ho + off, dXh + off, idesc, 1u);
+                    }
                 }
             }
             umma_commit(&empty[s]);
@@ -240,11 +253,13 @@ __global__ void __launch_bounds__(128, 1)
     if (!have) *abort_flag = 1;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
-        const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        const int row = m0 + h * kUM + warp * 32 + lane;
 #pragma unroll
         for (int c0 = 0; c0 < BN; c0 += 32) {
             uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * BN + c0);
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -264,6 +279,7 @@ __global__ void __launch_bounds__(128, 1)
                 }
             }
         }
+      }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -361,7 +377,7 @@ CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t l
     cuuint32_t box[2] = {(cuuint32_t)kBK, box_outer};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(PLX_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return m;
@@ -427,7 +443,7 @@ void build_t_split(plx_geom *g) {
     if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
     if (g->d_Th.p) return;
     const int64_t n = g->n_var;
-    const int64_t ld = (n + kBK - 1) / kBK * kBK;
+    const int64_t ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
     g->ldk = ld;
     g->d_Th.alloc(g->ctx, (size_t)(n * ld));
     g->d_Tl.alloc(g->ctx, (size_t)(n * ld));
@@ -456,7 +472,7 @@ static void build_a_split(plx_geom *g) {
     if (g->d_Ah.p) return;
     if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
     const int64_t n = g->n_var;
-    const int64_t ld = (n + kBK - 1) / kBK * kBK;
+    const int64_t ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
     g->ldk = ld;
     g->d_Ah.alloc(g->ctx, (size_t)(n * ld));
     g->d_Al.alloc(g->ctx, (size_t)(n * ld));
