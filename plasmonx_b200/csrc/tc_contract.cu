@@ -197,8 +197,9 @@ __global__ void __launch_bounds__(128, 1)
             }
             mbar_expect_tx(&full[s], (uint32_t)L::kStage);
             const int kx = (kt0 + kt) * kBK;
-            tma_load_2d(&mapTh, &full[s], stage_ptr(s, 0), kx, m0);
-            tma_load_2d(&mapTl, &full[s], stage_ptr(s, 1), kx, m0);
+            const int ay = (blockIdx.y * ktiles + kt0 + kt) * kBM;     // tile-ordered A
+            tma_load_2d(&mapTh, &full[s], stage_ptr(s, 0), 0, ay);
+            tma_load_2d(&mapTl, &full[s], stage_ptr(s, 1), 0, ay);
             tma_load_2d(&mapXh, &full[s], stage_ptr(s, 2), kx, n0);
             tma_load_2d(&mapXl, &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
@@ -288,25 +289,53 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// Transposed split for a non-symmetric stored matrix: out[r][c] = in[c][r]
-// (square n x n input), through a shared-memory tile.
-__global__ void split_bf16_t(int n, const double *__restrict__ in, int64_t ld_out, __nv_bfloat16 *__restrict__ hi,
-                             __nv_bfloat16 *__restrict__ lo) {
-    __shared__ float tile[32][33];
-    int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        int r = by + k, c = bx + threadIdx.x;          // read in[r][c]
-        tile[k][threadIdx.x] = (r < n && c < n) ? (float)in[(int64_t)r * n + c] : 0.0f;
+// The A operand (T, A0 or D^T split in BF16 high/low) is stored in the order
+// the kernel reads it: [m-tile of 256 rows][k-slab of 32][256 rows][32 k], so
+// every TMA box (256 x 32) is one contiguous 16 KB block of HBM.  Rows beyond
+// n and k beyond n are zero.
+__device__ __forceinline__ int64_t a_tiled(int64_t r, int64_t k, int64_t ktiles) {
+    return (((r / kBM) * ktiles + k / kBK) * kBM + r % kBM) * kBK + k % kBK;
+}
+
+__device__ __forceinline__ void split_store(double a, int64_t idx, __nv_bfloat16 *__restrict__ hi,
+                                            __nv_bfloat16 *__restrict__ lo) {
+    float x = (float)a;
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi[idx] = h;
+    lo[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+// Row-major n x n FP64 matrix -> tiled BF16 pair; the output is walked in its
+// own (contiguous) order.
+__global__ void split_tiled(int n, int64_t ktiles, int64_t total, const double *__restrict__ in,
+                            __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t kk = e % kBK, rr = (e / kBK) % kBM, tk = e / ((int64_t)kBK * kBM);
+        const int64_t r = (tk / ktiles) * kBM + rr, k = (tk % ktiles) * kBK + kk;
+        const double a = (r < n && k < n) ? in[r * n + k] : 0.0;
+        split_store(a, e, hi, lo);
+    }
+}
+
+// Transposed (BEM: d_T[j][i] = D(i, j)): out(r, k) = in[k][r], through a
+// shared-memory tile of 32 k x 256 r; grid (ktiles, mtiles).
+__global__ void split_tiled_t(int n, int64_t ktiles, const double *__restrict__ in, __nv_bfloat16 *__restrict__ hi,
+                              __nv_bfloat16 *__restrict__ lo) {
+    __shared__ float tile[kBK][kBM + 1];
+    const int64_t k0 = (int64_t)blockIdx.x * kBK, r0 = (int64_t)blockIdx.y * kBM;
+    for (int e = threadIdx.x; e < kBK * kBM; e += blockDim.x) {
+        const int kk = e / kBM, rr = e % kBM;                      // coalesced along r
+        const int64_t k = k0 + kk, r = r0 + rr;
+        tile[kk][rr] = (k < n && r < n) ? (float)in[k * n + r] : 0.0f;
     }
     __syncthreads();
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        int orow = bx + k, ocol = by + threadIdx.x;     // out[orow][ocol] = in[ocol][orow]
-        if (orow < n && ocol < ld_out) {
-            float x = tile[threadIdx.x][k];
-            __nv_bfloat16 h = __float2bfloat16_rn(x);
-            hi[(int64_t)orow * ld_out + ocol] = h;
-            lo[(int64_t)orow * ld_out + ocol] = __float2bfloat16_rn(x - __bfloat162float(h));
-        }
+    const int64_t base = ((int64_t)blockIdx.y * ktiles + blockIdx.x) * kBM * kBK;
+    for (int e = threadIdx.x; e < kBK * kBM; e += blockDim.x) {   // contiguous output block
+        const int rr = e / kBK, kk = e % kBK;
+        float x = tile[kk][rr];
+        __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi[base + e] = h;
+        lo[base + e] = __float2bfloat16_rn(x - __bfloat162float(h));
     }
 }
 
@@ -316,7 +345,7 @@ __global__ void split_bf16_t(int n, const double *__restrict__ in, int64_t ld_ou
 // applied to T itself), for a dipole row A0[r][k] = T[r][k]; zero for k >= n.
 // One block per (row, column chunk); rows vary fastest over the grid, so the
 // blocks running together share their neighbours' rows of T in L2.
-__global__ void fold_split(int N, int n, int64_t ld, const int32_t *__restrict__ rowptr,
+__global__ void fold_split(int N, int n, int64_t ld, int64_t ktiles, const int32_t *__restrict__ rowptr,
                            const int32_t *__restrict__ col, const double *__restrict__ kval,
                            const double *__restrict__ T, __nv_bfloat16 *__restrict__ hi,
                            __nv_bfloat16 *__restrict__ lo) {
@@ -332,10 +361,7 @@ __global__ void fold_split(int N, int n, int64_t ld, const int32_t *__restrict__
             a = trk;
         }
     }
-    float x = (float)a;
-    __nv_bfloat16 h = __float2bfloat16_rn(x);
-    hi[(int64_t)r * ld + k] = h;
-    lo[(int64_t)r * ld + k] = __float2bfloat16_rn(x - __bfloat162float(h));
+    split_store(a, a_tiled(r, k, ktiles), hi, lo);
 }
 
 // FP64 -> (BF16 high, BF16 low) split of a row-major [rows][cols] array into a
@@ -444,21 +470,18 @@ void build_t_split(plx_geom *g) {
     if (g->d_Th.p) return;
     const int64_t n = g->n_var;
     const int64_t ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
+    const int64_t rows = (n + kBM - 1) / kBM * kBM, ktiles = ld / kBK;
     g->ldk = ld;
-    g->d_Th.alloc(g->ctx, (size_t)(n * ld));
-    g->d_Tl.alloc(g->ctx, (size_t)(n * ld));
+    g->d_Th.alloc(g->ctx, (size_t)(rows * ld));
+    g->d_Tl.alloc(g->ctx, (size_t)(rows * ld));
+    auto *hi = reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p);
+    auto *lo = reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p);
     if (g->t_symmetric) {
-        split_bf16<<<2048, 256, 0, g->ctx->stream>>>((int)n, (int)n, n, g->d_T.p, (int)n, ld,
-                                                     reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p),
-                                                     reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p));
+        split_tiled<<<4096, 256, 0, g->ctx->stream>>>((int)n, ktiles, rows * ld, g->d_T.p, hi, lo);
     } else {
-        // stored transposed (BEM): split the transpose; the padded k columns stay zero
-        PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Th.p, 0, (size_t)(n * ld) * 2, g->ctx->stream));
-        PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Tl.p, 0, (size_t)(n * ld) * 2, g->ctx->stream));
-        dim3 grid((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
-        split_bf16_t<<<grid, dim3(32, 8), 0, g->ctx->stream>>>((int)n, g->d_T.p, ld,
-                                                                reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p),
-                                                                reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p));
+        // stored transposed (BEM): split the transpose
+        split_tiled_t<<<dim3((unsigned)ktiles, (unsigned)(rows / kBM)), 256, 0, g->ctx->stream>>>((int)n, ktiles,
+                                                                                                 g->d_T.p, hi, lo);
     }
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
@@ -473,12 +496,16 @@ static void build_a_split(plx_geom *g) {
     if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
     const int64_t n = g->n_var;
     const int64_t ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
+    const int64_t rows = (n + kBM - 1) / kBM * kBM, ktiles = ld / kBK;
     g->ldk = ld;
-    g->d_Ah.alloc(g->ctx, (size_t)(n * ld));
-    g->d_Al.alloc(g->ctx, (size_t)(n * ld));
+    g->d_Ah.alloc(g->ctx, (size_t)(rows * ld));
+    g->d_Al.alloc(g->ctx, (size_t)(rows * ld));
+    // rows n..rows of the last m-tile are read by the kernel: zero them
+    PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Ah.p, 0, (size_t)(rows * ld) * 2, g->ctx->stream));
+    PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Al.p, 0, (size_t)(rows * ld) * 2, g->ctx->stream));
     dim3 grid((unsigned)n, (unsigned)((ld + 255) / 256));
-    fold_split<<<grid, 256, 0, g->ctx->stream>>>(g->n_atoms, (int)n, ld, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
-                                                  g->d_T.p, reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p),
+    fold_split<<<grid, 256, 0, g->ctx->stream>>>(g->n_atoms, (int)n, ld, ktiles, g->d_rowptr.p, g->d_col.p,
+                                                  g->d_kval.p, g->d_T.p, reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p),
                                                   reinterpret_cast<__nv_bfloat16 *>(g->d_Al.p));
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
@@ -510,8 +537,10 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
         R, n, n, X, Rpad, ld, reinterpret_cast<__nv_bfloat16 *>(g->d_Xh.p),
         reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
     ctx->launches++;
-    CUtensorMap th = make_map(folded ? g->d_Ah.p : g->d_Th.p, ld, n, ld, kBM);
-    CUtensorMap tl = make_map(folded ? g->d_Al.p : g->d_Tl.p, ld, n, ld, kBM);
+    // A in tile order: rows of kBK elements, kBM rows per box
+    const uint64_t arows = (uint64_t)((n + kBM - 1) / kBM) * kBM * (uint64_t)(ld / kBK);
+    CUtensorMap th = make_map(folded ? g->d_Ah.p : g->d_Th.p, kBK, arows, kBK, kBM);
+    CUtensorMap tl = make_map(folded ? g->d_Al.p : g->d_Tl.p, kBK, arows, kBK, kBM);
     CUtensorMap xh = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
     CUtensorMap xl = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
     const int ktiles = (int)(ld / kBK);
