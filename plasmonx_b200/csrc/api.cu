@@ -399,8 +399,6 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
             throw Error(PLX_ERR_UNSUPPORTED, "BEM on the fly is not provided (the reference's BEM has no "
                                              "on-the-fly product either); use the on-memory mode");
         const bool refined = desc->precision != PLX_FP64 && desc->mode != PLX_INVERSION;
-        if (refined && otf && desc->precision != PLX_FP64_REFINED)
-            throw Error(PLX_ERR_UNSUPPORTED, "tensor-core refinement needs the stored T (on-memory mode)");
         if (!otf && !g->has_T) throw Error(PLX_ERR_ARG, "this mode needs the stored T (store_t at creation)");
         const int n = g->n_var, F = g->n_freq;
         std::vector<int32_t> pols;

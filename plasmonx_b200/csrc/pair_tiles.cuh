@@ -72,6 +72,33 @@ __device__ __forceinline__ double plx_pair_qq(double dx, double dy, double dz, d
     return erf(r / sqrt(rq_i * rq_i + rq_j * rq_j)) / r;
 }
 
+// One entry T[r][k] of the dense interaction matrix (rows/columns q_i -> i,
+// mu_i,a -> N + 3 i + a), evaluated alone with the formulas of plx_pair_tile /
+// plx_pair_qq: the building block of tiles generated in place (no stored T).
+// pos [4][N] (x, y, z), par [4][N] (r_q, r_mu, eta, a_ij).
+__device__ __forceinline__ double plx_t_element(int N, bool fmu, const double *__restrict__ pos,
+                                                const double *__restrict__ par, int64_t r, int64_t k) {
+    const int i = r < N ? (int)r : (int)((r - N) / 3), a = r < N ? -1 : (int)((r - N) % 3);
+    const int j = k < N ? (int)k : (int)((k - N) / 3), b = k < N ? -1 : (int)((k - N) % 3);
+    if (i == j) return (a < 0 && b < 0) ? par[2 * N + i] : 0.0;
+    const double d[3] = {pos[i] - pos[j], pos[N + i] - pos[N + j], pos[2 * N + i] - pos[2 * N + j]};
+    const double rq_i = par[i], rq_j = par[j];
+    if (!fmu) return plx_pair_qq(d[0], d[1], d[2], rq_i, rq_j);
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double rr = sqrt(r2);
+    const double ir = 1.0 / rr, ir2 = ir * ir, ir3 = ir2 * ir, ir5 = ir3 * ir2;
+    const double rm_i = par[N + i], rm_j = par[N + j];
+    double e;
+    if (a < 0 && b < 0) return erf(rr / sqrt(rq_i * rq_i + rq_j * rq_j)) * ir;
+    if (a < 0) return d[b] * (plx_fdamp(rr, sqrt(rq_i * rq_i + rm_j * rm_j), &e) * ir3);
+    if (b < 0) return -d[a] * (plx_fdamp(rr, sqrt(rq_j * rq_j + rm_i * rm_i), &e) * ir3);
+    const double Rmm = sqrt(rm_i * rm_i + rm_j * rm_j);
+    const double fD1 = plx_fdamp(rr, Rmm, &e);
+    const double fD2 = (4.0 / (PLX_SQRT_PI * Rmm * Rmm * Rmm)) * e;
+    const double c = -3.0 * ir5 * fD1 + fD2 * ir2;
+    return c * d[a] * d[b] + (a == b ? ir3 * fD1 : 0.0);
+}
+
 // Drude/Fermi conductance K_ij = (1 - 1/(1 + exp(-d (r/(s r0) - 1)))) A_i / r
 // (construct_K_minus_P_matrix and fermi_function, matrix_module.f90:393-426,
 // 694-715), evaluated in the same order as the reference so that pairs whose

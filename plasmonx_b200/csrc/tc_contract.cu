@@ -26,6 +26,7 @@
 
 #include <algorithm>
 
+#include "pair_tiles.cuh"
 #include "plx_internal.h"
 
 namespace plx {
@@ -339,6 +340,20 @@ __global__ void split_tiled_t(int n, int64_t ktiles, const double *__restrict__ 
     }
 }
 
+// No stored T (on-the-fly geometries): the split generated from the pair
+// formulas, one block per TMA box (256 rows x 32 k, contiguous output).
+__global__ void split_tiled_gen(int N, int n, int fmu, int64_t ktiles, const double *__restrict__ pos,
+                                const double *__restrict__ par, __nv_bfloat16 *__restrict__ hi,
+                                __nv_bfloat16 *__restrict__ lo) {
+    const int64_t k0 = (int64_t)blockIdx.x * kBK, r0 = (int64_t)blockIdx.y * kBM;
+    const int64_t base = ((int64_t)blockIdx.y * ktiles + blockIdx.x) * kBM * kBK;
+    for (int e = threadIdx.x; e < kBK * kBM; e += blockDim.x) {
+        const int64_t r = r0 + e / kBK, k = k0 + e % kBK;
+        const double a = (r < n && k < n) ? plx_t_element(N, fmu != 0, pos, par, r, k) : 0.0;
+        split_store(a, base + e, hi, lo);
+    }
+}
+
 // Folded operator rows, split like T: for a charge row i < N
 //   A0[i][k] = sum_e K_e (T[j_e][k] - T[i][k])      (CSR order, FP64)
 // (the charge rows of (K - P) T, update_y_q of matrix_module.f90:1011-1098
@@ -466,8 +481,8 @@ int choose_splits(int tiles, int ktiles, int sms) {
 }  // namespace
 
 void build_t_split(plx_geom *g) {
-    if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
     if (g->d_Th.p) return;
+    if (!g->has_T && is_bem(g)) throw Error(PLX_ERR_ARG, "BEM geometry without its Green-function matrix");
     const int64_t n = g->n_var;
     const int64_t ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
     const int64_t rows = (n + kBM - 1) / kBM * kBM, ktiles = ld / kBK;
@@ -476,7 +491,11 @@ void build_t_split(plx_geom *g) {
     g->d_Tl.alloc(g->ctx, (size_t)(rows * ld));
     auto *hi = reinterpret_cast<__nv_bfloat16 *>(g->d_Th.p);
     auto *lo = reinterpret_cast<__nv_bfloat16 *>(g->d_Tl.p);
-    if (g->t_symmetric) {
+    if (!g->has_T) {
+        // on-the-fly geometry: the split is generated from the pair formulas
+        split_tiled_gen<<<dim3((unsigned)ktiles, (unsigned)(rows / kBM)), 256, 0, g->ctx->stream>>>(
+            g->n_atoms, (int)n, g->model == PLX_WFQFMU, ktiles, g->d_pos.p, g->d_par.p, hi, lo);
+    } else if (g->t_symmetric) {
         split_tiled<<<4096, 256, 0, g->ctx->stream>>>((int)n, ktiles, rows * ld, g->d_T.p, hi, lo);
     } else {
         // stored transposed (BEM): split the transpose

@@ -69,3 +69,40 @@ def test_refined_solve_matches_lu(ctx, precision, bar):
     assert (out['status'] == 0).all(), out['status']
     sig, sref = out['results'][:, 9], ref['results'][:, 9]
     assert np.max(np.abs(sig - sref) / np.abs(sref)) < bar
+
+
+def _bowtie(edge=24.0, thickness=10.0, n_freq=4):
+    p0 = configs.agau_bowtie(edge=edge, thickness=thickness, gap=6.0, n_freq=n_freq, method='iterative on the fly',
+                             tolerance=1e-9, polarization='x')
+    text = p0.to_keyword_text()
+    return Problem.from_keyword_text(text), model.System.from_keywords(keywords.read_keyword_text(text))
+
+
+def test_generated_split_matches_stored_t(ctx):
+    """Without a stored T (on-the-fly geometry) the tensor-core operand is generated
+    from the pair formulas; its contraction agrees with the FP64 product of the
+    stored T like the stored split does (relative 5e-5)."""
+    p, _ = _ag(radius=10.0, n_freq=1)
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((9, p.n_var))
+    with Solver(p, ctx=ctx, store_t=True) as sv:
+        ref = sv.contract(X, 'fp64')
+    with Solver(p, ctx=ctx, store_t=False) as sv:
+        s3 = sv.contract(X, 'bf16x3')
+    assert np.max(np.linalg.norm(s3 - ref, axis=1) / np.linalg.norm(ref, axis=1)) < 5e-5
+
+
+@pytest.mark.parametrize('case', ['ag_sphere', 'agau_bowtie'])
+def test_mixed_on_the_fly_matches_lu(ctx, case):
+    """Matrix-free mode with the mixed form: tensor-core inner solves on the generated
+    split, FP64 residuals from the on-the-fly product; sigma_abs within 1e-6 of LU
+    (one atom type and the two-type Ag-Au bow-tie, whose conductance rows depend on w)."""
+    p, s = _ag(radius=10.0, n_freq=4) if case == 'ag_sphere' else _bowtie()
+    ref = osolve.solve(s, method='inversion')
+    with Solver(p, ctx=ctx, store_t=False) as sv:
+        b = sv.rhs(0, 1)
+        out = sv.solve(mode='iterative on the fly', precision='mixed_bf16x3', pol_mask=1,
+                       tol=1e-12 * np.linalg.norm(b[:, 0]))
+    assert (out['status'] == 0).all(), out['status']
+    sig, sref = out['results'][:, 9], ref['results'][:, 9]
+    assert np.max(np.abs(sig - sref) / np.abs(sref)) < 1e-6
