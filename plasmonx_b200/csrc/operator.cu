@@ -108,6 +108,66 @@ __global__ void __launch_bounds__(kTiledThreads) tiled_partial(int R, int n, int
 }
 
 // ---------------------------------------------------------------------------
+// S^T = X^T T with T generated in place (matrix-free, R > 16): the tiled
+// product above with its T slab computed from the pair formulas
+// (plx_t_element) instead of loaded, so every element of T is evaluated once
+// per 64-column row tile of X^T and a batch of many columns costs about one
+// dense FP64 product.  Same K chunks and per-element FMA order as the stored
+// kernels.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTiledThreads) otf_tiled_partial(int R, int n, int kchunk, int N, int fmu,
+                                                                   const double *__restrict__ pos,
+                                                                   const double *__restrict__ par,
+                                                                   const double *__restrict__ Xt,
+                                                                   double *__restrict__ part) {
+    __shared__ double As[BM][BK + 1];
+    __shared__ double Bs[BK][BN];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int row0 = blockIdx.y * BM, col0 = blockIdx.x * BN;
+    const int kbeg = blockIdx.z * kchunk, kend = min(n, kbeg + kchunk);
+    double acc[8][8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[u][v] = 0.0;
+    for (int k0 = kbeg; k0 < kend; k0 += BK) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < BM * BK; e += kTiledThreads) {
+            const int r = e / BK, k = e % BK, gr = row0 + r, gk = k0 + k;
+            As[r][k] = (gr < R && gk < kend) ? Xt[(int64_t)gr * n + gk] : 0.0;
+        }
+#pragma unroll 1
+        for (int e = threadIdx.x; e < BK * BN; e += kTiledThreads) {
+            const int k = e / BN, c = e % BN, gk = k0 + k, gc = col0 + c;
+            Bs[k][c] = (gk < kend && gc < n) ? plx_t_element(N, fmu != 0, pos, par, gk, gc) : 0.0;
+        }
+        __syncthreads();
+        const int kn = min(BK, kend - k0);
+        for (int k = 0; k < kn; ++k) {
+            double a[8], b[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] = As[ty * 8 + u][k];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) b[v] = Bs[k][tx + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int v = 0; v < 8; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int gr = row0 + ty * 8 + u;
+        if (gr >= R) continue;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            const int gc = col0 + tx + 16 * v;
+            if (gc < n) part[((int64_t)blockIdx.z * R + gr) * n + gc] = acc[u][v];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // S = T X generated on the fly (matrix-free), CB columns per launch.
 // One thread per target atom; source atoms staged in shared memory.
 // ---------------------------------------------------------------------------
@@ -547,6 +607,20 @@ void contract_t_impl(plx_geom *g, int count, const double *X, double *S, bool on
     cudaStream_t st = ctx->stream;
     const int n = g->n_var;
     const int R = 2 * count;
+    if (on_the_fly && R > 16) {
+        // many columns: tiled product with T generated per slab
+        int ks, kchunk;
+        skinny_split(n, ks, kchunk);
+        size_t need = (size_t)ks * R * n;
+        if (g->d_part.n < need) g->d_part.alloc(ctx, need);
+        dim3 grid(n_blocks(n, BN), n_blocks(R, BM), ks);
+        otf_tiled_partial<<<grid, kTiledThreads, 0, st>>>(R, n, kchunk, g->n_atoms, g->model == PLX_WFQFMU,
+                                                          g->d_pos.p, g->d_par.p, X, g->d_part.p);
+        skinny_reduce<<<n_blocks((int64_t)R * n, 256), 256, 0, st>>>(n, R, ks, g->d_part.p, S);
+        ctx->launches += 2;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        return;
+    }
     if (on_the_fly) {
         const bool fmu = g->model == PLX_WFQFMU;
         for (int c0 = 0; c0 < count; c0 += 4) {

@@ -106,3 +106,17 @@ def test_mixed_on_the_fly_matches_lu(ctx, case):
     assert (out['status'] == 0).all(), out['status']
     sig, sref = out['results'][:, 9], ref['results'][:, 9]
     assert np.max(np.abs(sig - sref) / np.abs(sref)) < 1e-6
+
+
+@pytest.mark.parametrize('count', [3, 40])
+def test_on_the_fly_fp64_contraction_matches_stored(ctx, count):
+    """The matrix-free FP64 product (pair kernel for few columns, tiled product with
+    T generated per slab for many) against the stored T: relative 1e-12."""
+    p, _ = _ag(radius=10.0, n_freq=1)
+    rng = np.random.default_rng(count)
+    X = rng.standard_normal((count, p.n_var))
+    with Solver(p, ctx=ctx, store_t=True) as sv:
+        ref = sv.contract(X, 'fp64')
+    with Solver(p, ctx=ctx, store_t=False) as sv:
+        otf = sv.contract(X, 'fp64_otf')
+    assert np.max(np.linalg.norm(otf - ref, axis=1) / np.linalg.norm(ref, axis=1)) < 1e-12
