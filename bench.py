@@ -27,6 +27,13 @@ Python API with host buffers: geometry upload and build, frequency tables,
 solve, results back to the host.  Under torchrun every rank solves its own
 replica of the spectrum (weak scaling; no collective on the data path).
 
+Serving leg (`serving` in the line): a seeded Poisson stream of spectrum
+requests (wFQ Na spheres, wFQFMu Ag/Au spheres and rods, BEM spheres and
+rods; `--serving-scale small` keeps them at 500-4k atoms or tesserae and
+20-100 frequencies) through plasmonx_b200.serving (admission by HBM
+footprint, resident geometries, batching, two concurrent workers), reported as
+p50/p99 request latency and freq-solves/s.
+
 `--impl reference` times the reference's algorithm on the host CPU: the
 threaded C restatement of its on-the-fly product (oracle/pairs.c) over a
 bounded sample of matrix-vector products of the same geometry, turned into
@@ -311,6 +318,10 @@ def main():
     ap.add_argument('--accuracy-freqs', type=int, default=5)
     ap.add_argument('--radius', type=float, default=None, help='smaller sphere (profiling runs only)')
     ap.add_argument('--n-freq', type=int, default=None, help='fewer frequencies (profiling runs only)')
+    ap.add_argument('--serving-requests', type=int, default=24, help='requests in the serving leg (0: skip)')
+    ap.add_argument('--serving-rate', type=float, default=20.0, help='Poisson arrival rate, requests/s')
+    ap.add_argument('--serving-scale', default='small', choices=['small', 'full'])
+    ap.add_argument('--serving-workers', type=int, default=2)
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
@@ -421,6 +432,20 @@ def main():
                 'note': 'achieved counts one product (algorithmic); the tensor pipe executes %d' % nprod}
     roof['frac'] = roof['achieved'] / roof['peak']
 
+    # serving leg: a seeded Poisson mix of spectrum requests through the request loop
+    serving = None
+    if args.serving_requests > 0 and args.impl == 'ours':
+        from plasmonx_b200.serving import Server, request_pool, run_mix
+        pool = request_pool(n_requests=args.serving_requests, rate=args.serving_rate, seed=7 + rank,
+                            scale=args.serving_scale, precision=args.precision)
+        with Server(device=local, workers=args.serving_workers) as srv:
+            serving = run_mix(srv, pool)
+        serving.update({'rate_per_s': args.serving_rate, 'scale': args.serving_scale,
+                        'workers': args.serving_workers, 'precision': args.precision,
+                        'modes': sorted({str(r.mode) for r in pool}),
+                        'mean_batch_requests': float(np.mean([r.batch_size for r in pool])),
+                        'p99_ms_max_over_ranks': allmax(pg, serving['p99_ms'], local)})
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         sps = float(np.mean(np.concatenate(steps_hist))) if steps_hist else args.steps_per_solve
@@ -448,7 +473,8 @@ def main():
                 'accuracy': acc, 'fp64_plain_gmres': fp64,
                 'speedup_vs_fp64_plain': None if fp64 is None else value / fp64['value'],
                 'arnoldi_steps': {'mean': float(np.mean(np.concatenate(steps_hist))),
-                                  'max': int(np.max(np.concatenate(steps_hist)))}}
+                                  'max': int(np.max(np.concatenate(steps_hist)))},
+                'serving': serving}
         print(json.dumps(line), flush=True)
     solver.close()
     ctx.close()

@@ -69,6 +69,25 @@ def ag_sphere(radius=35.0, n_freq=201, seed=1, jitter=0.0, lo=3.0, hi=4.5, **kw)
     return build('wfqfmu', pts, ['Ag'], np.zeros(len(pts), np.int32), ev_grid(lo, hi, n_freq), **kw)
 
 
+LATTICE = {'Na': ('bcc', 4.225), 'Ag': ('fcc', 4.086), 'Au': ('fcc', 4.08)}
+WINDOW = {'Na': (2.0, 4.0), 'Ag': (3.0, 4.5), 'Au': (2.0, 3.0)}
+
+
+def particle(metal, shape='sphere', radius=20.0, length=None, n_freq=61, seed=1, jitter=0.0, **kw):
+    """A single-metal sphere or rod (cylinder with hemispherical caps along z) of the
+    metal's lattice, in its frequency window: wFQ for Na, wFQFMu for Ag and Au."""
+    kind, a = LATTICE[metal]
+    if shape == 'sphere':
+        pts = G.sphere(kind, a, radius, jitter, seed)
+    elif shape == 'rod':
+        pts = G.rod(kind, a, length if length is not None else 4.0 * radius, radius, jitter, seed)
+    else:
+        raise ValueError(shape)
+    lo, hi = WINDOW[metal]
+    model = 'wfq' if metal == 'Na' else 'wfqfmu'
+    return build(model, pts, [metal], np.zeros(len(pts), np.int32), ev_grid(lo, hi, n_freq), **kw)
+
+
 def agau_bowtie(edge=80.0, thickness=20.0, gap=10.0, n_freq=201, seed=1, jitter=0.0, **kw):
     """wFQFMu Ag-Au bow-tie: two fcc (a = 4.08 A) prisms tip to tip along x, 2.0-4.5 eV."""
     pts, sp = G.bowtie(4.08, edge, thickness, gap, jitter, seed)

@@ -38,6 +38,21 @@ def sphere(kind, a, radius, jitter=0.0, seed=0):
     return pts
 
 
+def rod(kind, a, length, radius, jitter=0.0, seed=0):
+    """Lattice sites inside a cylinder of the given radius along z with hemispherical
+    caps, total length `length` (Angstrom), ordered by (x, y, z), plus uniform jitter."""
+    half = max(length / 2.0 - radius, 0.0)
+    pts = _lattice(kind, a, length / 2.0 + a)
+    z = np.clip(pts[:, 2], -half, half)
+    d2 = pts[:, 0] ** 2 + pts[:, 1] ** 2 + (pts[:, 2] - z) ** 2
+    pts = pts[d2 <= radius * radius + 1e-9]
+    pts = pts[np.lexsort((pts[:, 2], pts[:, 1], pts[:, 0]))]
+    if jitter:
+        rng = np.random.default_rng(seed)
+        pts = pts + rng.uniform(-jitter, jitter, size=pts.shape)
+    return pts
+
+
 def prism(a, edge, thickness, kind='fcc'):
     """Equilateral triangular prism in the xy plane, one tip at the origin pointing to -x,
     the opposite side at x = edge * sqrt(3)/2, thickness along z centred on 0."""

@@ -1,0 +1,136 @@
+"""Scheduling of the serving loop (admission by footprint, resident geometries,
+batching of requests that share a geometry, concurrent workers), exercised with
+a stand-in solver on the CPU; the GPU test of the same loop is test_gpu_serving.py."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from plasmonx_b200 import configs
+from plasmonx_b200.serving import Server, ServeRequest, footprint, request_pool, run_mix
+
+
+class FakeContext:
+    def __init__(self, dev):
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+class FakeSolver:
+    """Returns results[:, 0] = the frequencies it was given; sleeps to simulate work."""
+    log = []
+    lock = threading.Lock()
+
+    def __init__(self, problem, ctx, store_t, delay=0.05):
+        self.problem, self.store_t, self.delay = problem, store_t, delay
+        self.closed = False
+        with FakeSolver.lock:
+            FakeSolver.log.append(('build', id(problem), store_t))
+
+    def set_frequencies(self, freqs, alpha_w=None):
+        self.freqs = np.asarray(freqs)
+
+    def solve(self, mode=None, precision=None, pol_mask=None, tol=None):
+        t0 = time.perf_counter()
+        time.sleep(self.delay)
+        F = len(self.freqs)
+        res = np.zeros((F, 20))
+        res[:, 0] = self.freqs
+        with FakeSolver.lock:
+            FakeSolver.log.append(('solve', id(self.problem), mode, F, t0, time.perf_counter()))
+        return {'results': res, 'polar': np.zeros((F, 3, 3), complex), 'status': np.zeros(F, np.int32),
+                'steps': np.zeros((F, 3), np.int32)}
+
+    def close(self):
+        self.closed = True
+
+
+def _server(budget, workers=2):
+    FakeSolver.log = []
+    return Server(hbm_budget=budget, workers=workers, solver_factory=FakeSolver, context_factory=FakeContext)
+
+
+def _na(radius=12.0, nf=5):
+    p = configs.particle('Na', 'sphere', radius, n_freq=nf, method='iterative', tolerance=1e-9, polarization='x')
+    return p
+
+
+def _req(i, p, freqs=None, arrival=0.0):
+    if freqs is not None:
+        import copy
+        q = copy.copy(p)
+        q.freqs = np.asarray(freqs)
+        q.geometry_key = getattr(p, 'geometry_key', id(p))
+        p = q
+    return ServeRequest(i, p, arrival=arrival, precision='mixed_bf16x3', pol_mask=1, tol=1.0)
+
+
+def test_requests_on_one_geometry_are_batched_and_sliced():
+    p = _na()
+    p.geometry_key = 'na'
+    with _server(1 << 40, workers=1) as srv:
+        first = srv.submit(_req(0, p, [1.0, 2.0]))
+        time.sleep(0.01)                          # the first batch is running
+        later = [srv.submit(_req(k, p, [10.0 * k, 10.0 * k + 1, 10.0 * k + 2])) for k in (1, 2, 3)]
+        for r in [first] + later:
+            assert r.done.wait(5)
+    assert first.batch_size == 1
+    assert all(r.batch_size == 3 for r in later)        # merged while the worker was busy
+    for r in later:
+        np.testing.assert_array_equal(r.result['results'][:, 0], r.problem.freqs)
+    builds = [e for e in FakeSolver.log if e[0] == 'build']
+    assert len(builds) == 1                               # the geometry stayed resident
+
+
+def test_admission_picks_matrix_free_when_t_does_not_fit_and_rejects_too_large():
+    p = configs.particle('Ag', 'sphere', 12.0, n_freq=4, method='iterative', tolerance=1e-9)
+    geo_mem, bat = footprint(p, 'iterative', 'mixed_bf16x3', 4)
+    geo_otf, _ = footprint(p, 'iterative on the fly', 'mixed_bf16x3', 4)
+    budget = geo_otf + bat + (geo_mem - geo_otf) // 2
+    with _server(budget) as srv:
+        r = srv.submit(ServeRequest(0, p, precision='mixed_bf16x3', pol_mask=1, tol=1.0))
+        assert r.done.wait(5)
+        assert r.error is None and r.mode == 'iterative on the fly'
+    with _server(geo_otf // 2) as srv:
+        r = srv.submit(ServeRequest(1, p, precision='mixed_bf16x3', pol_mask=1, tol=1.0))
+        assert r.done.wait(5)
+        assert isinstance(r.error, MemoryError)
+
+
+def test_idle_geometry_is_evicted_for_a_new_one():
+    a, b = _na(12.0), _na(14.0)
+    geo, bat = footprint(b, 'iterative', 'mixed_bf16x3', 5)
+    with _server(geo + bat + geo // 2, workers=1) as srv:
+        ra = srv.submit(_req(0, a))
+        assert ra.done.wait(5)
+        rb = srv.submit(_req(1, b))
+        assert rb.done.wait(5)
+        assert rb.error is None
+        assert srv.committed <= srv.budget
+    assert [e[1] for e in FakeSolver.log if e[0] == 'build'] == [id(a), id(b)]
+
+
+def test_two_workers_overlap_different_geometries():
+    a, b = _na(12.0), _na(13.0)
+    with _server(1 << 40, workers=2) as srv:
+        ra, rb = srv.submit(_req(0, a)), srv.submit(_req(1, b))
+        assert ra.done.wait(5) and rb.done.wait(5)
+    solves = [e for e in FakeSolver.log if e[0] == 'solve']
+    assert len(solves) == 2
+    (s0, e0), (s1, e1) = [(x[4], x[5]) for x in solves]
+    assert max(s0, s1) < min(e0, e1)                       # the two solves ran at the same time
+    assert ra.worker != rb.worker
+
+
+def test_mix_statistics_and_pool_is_seeded():
+    pool1 = request_pool(n_requests=6, rate=200.0, seed=3)
+    pool2 = request_pool(n_requests=6, rate=200.0, seed=3)
+    assert [r.n_freq for r in pool1] == [r.n_freq for r in pool2]
+    assert [r.arrival for r in pool1] == [r.arrival for r in pool2]
+    with _server(1 << 44, workers=2) as srv:
+        st = run_mix(srv, pool1)
+    assert st['requests'] == 6 and st['errors'] == 0
+    assert st['p50_ms'] <= st['p99_ms'] and st['throughput'] > 0
