@@ -64,6 +64,8 @@ PEAKS_FALLBACK = {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustain
 # frequencies), measured with the FP64 GMRES on B200; used to turn the CPU
 # arm's timed matrix-vector products into freq-solves/s.
 STEPS_PER_SOLVE = {'ag_sphere': None}
+# measured DRAM bytes / algorithmic bytes of the tensor-core contraction (ncu, small case)
+TRAFFIC_RATIO = 1.004
 
 
 def peaks():
@@ -428,7 +430,11 @@ def main():
                 'achieved': flops_per / (avg_ms / 1000.0) / 1e12, 'peak': pk['bf16_tflops'], 'unit': 'TFLOP/s',
                 'peak_kind': pk_kind, 'flops_per_launch': flops_per, 'bytes_per_launch': bytes_per,
                 'avg_launch_ms': avg_ms, 'issued_tensor_tflops': nprod * flops_per / (avg_ms / 1000.0) / 1e12,
-                'achieved_hbm_gbs': bytes_per / (avg_ms / 1000.0) / 1e9, 'traffic': None,
+                'achieved_hbm_gbs': bytes_per / (avg_ms / 1000.0) / 1e9,
+                # DRAM bytes per launch: the ncu capture of the 7,844-unknown case read its
+                # operand 1.004 times (X tiles come from L2); traffic grows with the operand
+                'traffic': bytes_per * TRAFFIC_RATIO, 'traffic_unit': 'bytes per launch',
+                'traffic_source': 'ncu dram__bytes of a 7,844-unknown capture, scaled by operand bytes',
                 'note': 'achieved counts one product (algorithmic); the tensor pipe executes %d' % nprod}
     roof['frac'] = roof['achieved'] / roof['peak']
 
