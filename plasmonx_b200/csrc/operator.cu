@@ -406,7 +406,7 @@ __global__ void dipole_rows(int N, int nt, int nv, int count, const int32_t *__r
 // Rows after a contraction with the folded A0 = blockdiag(K - P, I) T (one atom
 // type): only the diagonal D(w) is left, y = s + D(w) x, with -z(w) on the
 // charge rows and sum_t f_t,i / alpha_t(w) on the dipole rows.
-__global__ void folded_rows(int N, int nt, int nv, int count, const int32_t *__restrict__ freq,
+__global__ void folded_rows(int N, int nt, int nv, int64_t ldS, int count, const int32_t *__restrict__ freq,
                             const int32_t *__restrict__ type, const Cplx *__restrict__ dq,
                             const double *__restrict__ frac, const Cplx *__restrict__ inv_alpha,
                             const double *__restrict__ S, const double *__restrict__ X,
@@ -427,10 +427,39 @@ __global__ void folded_rows(int N, int nt, int nv, int count, const int32_t *__r
             d.im += fr * a.im;
         }
     }
-    const int64_t base = (int64_t)c * 2 * nv;
+    const int64_t base = (int64_t)c * 2 * nv, sb = (int64_t)c * 2 * ldS;
     const double xr = X[base + r], xi = X[base + nv + r];
-    Y[base + r] = S[base + r] + d.re * xr - d.im * xi;
-    Y[base + nv + r] = S[base + nv + r] + d.re * xi + d.im * xr;
+    Y[base + r] = S[sb + r] + d.re * xr - d.im * xi;
+    Y[base + nv + r] = S[sb + ldS + r] + d.re * xi + d.im * xr;
+}
+
+// Alloy correction after the folded contraction: for every interface row i,
+//   y_i += sum_{j of another type} 1/2 (w_tj/w_ti(w) - 1) K_ji (s_j - s_i),
+// s = T x of the interface atoms (rows n + position in J of the output).
+// One thread per (interface row, column).
+__global__ void iface_rows(int nx, int count, int nt, int nv, int64_t ldS, const int32_t *__restrict__ freq,
+                           const int32_t *__restrict__ type, const int32_t *__restrict__ xrow,
+                           const int32_t *__restrict__ xipos, const int32_t *__restrict__ xrowptr,
+                           const int32_t *__restrict__ xcol, const int32_t *__restrict__ xtj,
+                           const double *__restrict__ xkt, const Cplx *__restrict__ wratio,
+                           const double *__restrict__ S, double *__restrict__ Y) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (t >= nx || c >= count) return;
+    const int i = xrow[t], f = freq[c], ti = type[i];
+    const double *sr = S + (int64_t)c * 2 * ldS + nv, *si = sr + ldS;
+    const double s_re = sr[xipos[t]], s_im = si[xipos[t]];
+    double yre = 0.0, yim = 0.0;
+    for (int e = xrowptr[t]; e < xrowptr[t + 1]; ++e) {
+        const int p = xcol[e];
+        const Cplx w = wratio[ti + nt * xtj[e] + (int64_t)nt * nt * f];
+        const double cre = 0.5 * (w.re - 1.0) * xkt[e], cim = 0.5 * w.im * xkt[e];
+        const double dre = sr[p] - s_re, dim = si[p] - s_im;
+        yre += cre * dre - cim * dim;
+        yim += cre * dim + cim * dre;
+    }
+    Y[(int64_t)c * 2 * nv + i] += yre;
+    Y[(int64_t)c * 2 * nv + nv + i] += yim;
 }
 
 // Static potential V_i (field along pol) for the right-hand side.
@@ -692,15 +721,29 @@ void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, d
         // matrix and a diagonal pass (no conductance rows per application)
         plx_ctx *ctx = g->ctx;
         const double nn = (double)g->n_var;
+        const int64_t M = tc_fold_rows(g);
+        double *S = work;
+        if (M > g->n_var) {
+            // alloys: the output carries the interface rows after the n operator rows
+            const size_t need = (size_t)b.count * 2 * M;
+            if (g->d_fold_work.n < need) g->d_fold_work.alloc(ctx, need);
+            S = g->d_fold_work.p;
+        }
         prof_begin(ctx);
-        tc_contract(g, b.count, X, work, how == Contraction::TC3 ? 3 : 1, true);
+        tc_contract(g, b.count, X, S, how == Contraction::TC3 ? 3 : 1, true);
         prof_end(ctx, PROF_TC, 2.0 * nn * nn * 2.0 * b.count,
-                 (how == Contraction::TC3 ? 4.0 : 2.0) * nn * (double)g->ldk + 2.0 * 8.0 * nn * 2.0 * b.count);
+                 (how == Contraction::TC3 ? 4.0 : 2.0) * (double)M * (double)g->ldk + 2.0 * 8.0 * nn * 2.0 * b.count);
         prof_begin(ctx);
         folded_rows<<<dim3(n_blocks(g->n_var, 256), b.count), 256, 0, ctx->stream>>>(
-            g->n_atoms, g->n_types, g->n_var, b.count, b.d_freq, g->d_type.p, g->d_dq.p, g->d_frac.p,
-            g->d_inv_alpha.p, work, X, Y);
+            g->n_atoms, g->n_types, g->n_var, M, b.count, b.d_freq, g->d_type.p, g->d_dq.p, g->d_frac.p,
+            g->d_inv_alpha.p, S, X, Y);
         ctx->launches++;
+        if (g->n_xrows > 0) {
+            iface_rows<<<dim3(n_blocks(g->n_xrows, 128), b.count), 128, 0, ctx->stream>>>(
+                g->n_xrows, b.count, g->n_types, g->n_var, M, b.d_freq, g->d_type.p, g->d_xrow.p, g->d_xipos.p,
+                g->d_xrowptr.p, g->d_xcol.p, g->d_xtj.p, g->d_xkt.p, g->d_wratio.p, S, Y);
+            ctx->launches++;
+        }
         PLX_CHECK_CUDA(cudaGetLastError());
         prof_end(ctx, PROF_ROWS, 0.0, 0.0);
         return;

@@ -131,6 +131,19 @@ struct plx_geom {
     // A0 = blockdiag(K - P, I) T folded once and split like T, so that a
     // tensor-core application of A(w) is one contraction plus the diagonal
     plx::DevArray<uint16_t> d_Ah, d_Al;
+    // rows of the folded operand: n, plus for alloys the T charge rows of the
+    // interface atoms J (atoms with a neighbour of the other type, and those
+    // neighbours), whose products feed the w-dependent correction
+    //   y_i += sum_{j of other type} 1/2 (w_tj/w_ti - 1) K_ji (s_j - s_i)
+    // over the interface rows I (CSR over I, columns as positions in J)
+    int64_t fold_rows = 0;
+    int n_iface = 0, n_xrows = 0;
+    plx::DevArray<int32_t> d_iface_atom;          // [|J|]
+    plx::DevArray<int32_t> d_xrow, d_xipos;       // [|I|]: row atom, its position in J
+    plx::DevArray<int32_t> d_xrowptr;             // [|I| + 1]
+    plx::DevArray<int32_t> d_xcol, d_xtj;         // position of j in J, type of j
+    plx::DevArray<double> d_xkt;                  // K_ji
+    plx::DevArray<double> d_fold_work;            // [R][fold_rows] output of the folded contraction
     // k-split partial sums of the tensor-core contraction ([splits][R][n_var])
     plx::DevArray<double> d_tcpart;
     plx::DevArray<int> d_tc_err;
@@ -184,10 +197,12 @@ void diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv);
 // (nprod 3: Th Xh + Th Xl + Tl Xh; nprod 1: Th Xh).  X, S: [count][2][n] FP64.
 void build_t_split(plx_geom *g);
 void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded = false);
-// true when apply_operator contracts with the folded A0 on the tensor cores
-inline bool tc_folds_operator(const plx_geom *g) {
-    return (g->model == PLX_WFQ || g->model == PLX_WFQFMU) && g->n_types == 1 && g->has_T;
-}
+// true when apply_operator contracts with the folded A0 on the tensor cores:
+// every atomistic geometry (T stored or generated; alloys with the interface
+// correction)
+inline bool tc_folds_operator(const plx_geom *g) { return g->model == PLX_WFQ || g->model == PLX_WFQFMU; }
+// builds the folded operand if needed; returns its number of rows
+int64_t tc_fold_rows(plx_geom *g);
 int tc_error(plx_geom *g);   // non-zero when a tensor-core CTA gave up waiting
 
 // inversion.cu

@@ -123,7 +123,9 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
         in.jacobi = rq.jacobi;
         // a tensor-core inner solve is accurate to ~1e-6 at best: an FP32 basis costs nothing in accuracy
         in.basis_fp32 = rq.inner_contraction == Contraction::TC3 || rq.inner_contraction == Contraction::TC1;
-        in.single_pass = in.basis_fp32 && rq.single_pass_gs;
+        // one Gram-Schmidt pass keeps an FP32 basis orthogonal enough up to 64 vectors
+        // (measured); longer inner solves re-orthogonalise
+        in.single_pass = in.basis_fp32 && rq.single_pass_gs && rq.inner_m <= 64;
         for (int k = 0; k < na; ++k) {
             int c = act[k];
             fa[k] = rq.freq[c];

@@ -354,26 +354,43 @@ __global__ void split_tiled_gen(int N, int n, int fmu, int64_t ktiles, const dou
     }
 }
 
-// Folded operator rows, split like T: for a charge row i < N
-//   A0[i][k] = sum_e K_e (T[j_e][k] - T[i][k])      (CSR order, FP64)
-// (the charge rows of (K - P) T, update_y_q of matrix_module.f90:1011-1098
-// applied to T itself), for a dipole row A0[r][k] = T[r][k]; zero for k >= n.
-// One block per (row, column chunk); rows vary fastest over the grid, so the
-// blocks running together share their neighbours' rows of T in L2.
-__global__ void fold_split(int N, int n, int64_t ld, int64_t ktiles, const int32_t *__restrict__ rowptr,
-                           const int32_t *__restrict__ col, const double *__restrict__ kval,
-                           const double *__restrict__ T, __nv_bfloat16 *__restrict__ hi,
-                           __nv_bfloat16 *__restrict__ lo) {
+// Folded operator rows, split like T.  For a charge row i < N
+//   A0[i][k] = sum_e c_e (T[j_e][k] - T[i][k])      (CSR order, FP64)
+// with c_e = K_ij for one atom type (the charge rows of (K - P) T,
+// update_y_q of matrix_module.f90:1011-1098, applied to T itself) and
+// c_e = 1/2 (K_ij + K_ji) for alloys (the w-independent part of
+// 1/2 (K + (w_j/w_i) K^T)); for a dipole row A0[r][k] = T[r][k]; the rows
+// appended after n are the charge rows of T of the interface atoms.  T comes
+// from the stored matrix or, without one, from the pair formulas.  One block
+// per (row, column chunk); rows vary fastest over the grid, so the blocks
+// running together share their neighbours' rows of T in L2.
+__device__ __forceinline__ double t_value(const double *__restrict__ T, int N, int n, int fmu,
+                                          const double *__restrict__ pos, const double *__restrict__ par, int64_t r,
+                                          int64_t k) {
+    return T ? T[r * n + k] : plx_t_element(N, fmu != 0, pos, par, r, k);
+}
+
+__global__ void fold_split(int N, int n, int64_t ld, int64_t ktiles, int hetero, int fmu,
+                           const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                           const double *__restrict__ kval, const double *__restrict__ ktval,
+                           const double *__restrict__ T, const double *__restrict__ pos,
+                           const double *__restrict__ par, const int32_t *__restrict__ iface_atom,
+                           __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
     const int r = blockIdx.x;
     const int64_t k = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
     if (k >= ld) return;
     double a = 0.0;
     if (k < n) {
-        const double trk = T[(int64_t)r * n + k];
         if (r < N) {
-            for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) a = fma(kval[e], T[(int64_t)col[e] * n + k] - trk, a);
+            const double trk = t_value(T, N, n, fmu, pos, par, r, k);
+            for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+                const double c = hetero ? 0.5 * (kval[e] + ktval[e]) : kval[e];
+                a = fma(c, t_value(T, N, n, fmu, pos, par, col[e], k) - trk, a);
+            }
+        } else if (r < n) {
+            a = t_value(T, N, n, fmu, pos, par, r, k);
         } else {
-            a = trk;
+            a = t_value(T, N, n, fmu, pos, par, iface_atom[r - n], k);
         }
     }
     split_store(a, a_tiled(r, k, ktiles), hi, lo);
@@ -425,7 +442,7 @@ CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t l
 }
 
 template <int BN, int NPROD>
-void launch_bn(plx_geom *g, int R, const CUtensorMap &th, const CUtensorMap &tl, const CUtensorMap &xh,
+void launch_bn(plx_geom *g, int M, int R, const CUtensorMap &th, const CUtensorMap &tl, const CUtensorMap &xh,
                const CUtensorMap &xl, int ktiles, int splits, int kper, double *S, int *err) {
     constexpr int ST = tc_stages<BN>();
     using L = TcSmem<BN, ST>;
@@ -435,9 +452,8 @@ void launch_bn(plx_geom *g, int R, const CUtensorMap &th, const CUtensorMap &tl,
         PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
         attr = true;
     }
-    dim3 grid((R + BN - 1) / BN, (g->n_var + kBM - 1) / kBM, splits);
-    kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, g->n_var, R, ktiles, kper, S, g->n_var,
-                                                   (int64_t)R * g->n_var, err);
+    dim3 grid((R + BN - 1) / BN, (M + kBM - 1) / kBM, splits);
+    kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, M, R, ktiles, kper, S, M, (int64_t)R * M, err);
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
 }
@@ -510,28 +526,99 @@ void build_t_split(plx_geom *g) {
     }
 }
 
+// Interface of an alloy: rows I with neighbours of another type, the atoms J
+// whose T charge rows the correction needs (I and those neighbours), and the
+// cross-type entries of I as a CSR over positions in J.
+static void build_interface(plx_geom *g) {
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int N = g->n_atoms;
+    std::vector<int32_t> rowptr(N + 1), type(N);
+    std::vector<int32_t> col((size_t)g->nnz);
+    std::vector<double> kt((size_t)g->nnz);
+    PLX_CHECK_CUDA(cudaMemcpyAsync(rowptr.data(), g->d_rowptr.p, (N + 1) * 4, cudaMemcpyDeviceToHost, st));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(type.data(), g->d_type.p, N * 4, cudaMemcpyDeviceToHost, st));
+    if (g->nnz) {
+        PLX_CHECK_CUDA(cudaMemcpyAsync(col.data(), g->d_col.p, g->nnz * 4, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(kt.data(), g->d_ktval.p, g->nnz * 8, cudaMemcpyDeviceToHost, st));
+    }
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+    std::vector<int32_t> pos(N, -1), J, rows, ptr(1, 0), xcol, xtj;
+    std::vector<double> xkt;
+    auto place = [&](int a) {
+        if (pos[a] < 0) {
+            pos[a] = (int32_t)J.size();
+            J.push_back(a);
+        }
+    };
+    for (int i = 0; i < N; ++i) {
+        bool any = false;
+        for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+            if (type[col[e]] != type[i]) any = true;
+        if (!any) continue;
+        place(i);
+        rows.push_back(i);
+        for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+            const int j = col[e];
+            if (type[j] == type[i]) continue;
+            place(j);
+            xcol.push_back(j);          // atom index for now
+            xtj.push_back(type[j]);
+            xkt.push_back(kt[e]);
+        }
+        ptr.push_back((int32_t)xcol.size());
+    }
+    for (auto &c : xcol) c = pos[c];
+    std::vector<int32_t> ipos(rows.size());
+    for (size_t t = 0; t < rows.size(); ++t) ipos[t] = pos[rows[t]];
+    g->n_iface = (int)J.size();
+    g->n_xrows = (int)rows.size();
+    auto up_i = [&](DevArray<int32_t> &d, const std::vector<int32_t> &h) {
+        d.alloc(ctx, std::max<size_t>(h.size(), 1));
+        if (!h.empty()) PLX_CHECK_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st));
+    };
+    up_i(g->d_iface_atom, J);
+    up_i(g->d_xrow, rows);
+    up_i(g->d_xipos, ipos);
+    up_i(g->d_xrowptr, ptr);
+    up_i(g->d_xcol, xcol);
+    up_i(g->d_xtj, xtj);
+    g->d_xkt.alloc(ctx, std::max<size_t>(xkt.size(), 1));
+    if (!xkt.empty()) PLX_CHECK_CUDA(cudaMemcpyAsync(g->d_xkt.p, xkt.data(), xkt.size() * 8, cudaMemcpyHostToDevice, st));
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+}
+
 static void build_a_split(plx_geom *g) {
     if (g->d_Ah.p) return;
-    if (!g->has_T) throw Error(PLX_ERR_ARG, "the mixed-precision solve needs the stored T");
+    const bool hetero = g->n_types > 1;
+    if (hetero) build_interface(g);
     const int64_t n = g->n_var;
+    const int64_t M = n + (hetero ? g->n_iface : 0);
     const int64_t ld = (n + kLdAlign - 1) / kLdAlign * kLdAlign;
-    const int64_t rows = (n + kBM - 1) / kBM * kBM, ktiles = ld / kBK;
+    const int64_t rows = (M + kBM - 1) / kBM * kBM, ktiles = ld / kBK;
     g->ldk = ld;
+    g->fold_rows = M;
     g->d_Ah.alloc(g->ctx, (size_t)(rows * ld));
     g->d_Al.alloc(g->ctx, (size_t)(rows * ld));
-    // rows n..rows of the last m-tile are read by the kernel: zero them
+    // rows M..rows of the last m-tile are read by the kernel: zero them
     PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Ah.p, 0, (size_t)(rows * ld) * 2, g->ctx->stream));
     PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Al.p, 0, (size_t)(rows * ld) * 2, g->ctx->stream));
-    dim3 grid((unsigned)n, (unsigned)((ld + 255) / 256));
-    fold_split<<<grid, 256, 0, g->ctx->stream>>>(g->n_atoms, (int)n, ld, ktiles, g->d_rowptr.p, g->d_col.p,
-                                                  g->d_kval.p, g->d_T.p, reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p),
-                                                  reinterpret_cast<__nv_bfloat16 *>(g->d_Al.p));
+    dim3 grid((unsigned)M, (unsigned)((ld + 255) / 256));
+    fold_split<<<grid, 256, 0, g->ctx->stream>>>(
+        g->n_atoms, (int)n, ld, ktiles, hetero, g->model == PLX_WFQFMU, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
+        g->d_ktval.p, g->has_T ? g->d_T.p : nullptr, g->d_pos.p, g->d_par.p, g->d_iface_atom.p,
+        reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p), reinterpret_cast<__nv_bfloat16 *>(g->d_Al.p));
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
     if (!g->d_tc_err.p) {
         g->d_tc_err.alloc(g->ctx, 1);
         PLX_CHECK_CUDA(cudaMemsetAsync(g->d_tc_err.p, 0, sizeof(int), g->ctx->stream));
     }
+}
+
+int64_t tc_fold_rows(plx_geom *g) {
+    build_a_split(g);
+    return g->fold_rows;
 }
 
 void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded) {
@@ -541,6 +628,8 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
         build_t_split(g);
     plx_ctx *ctx = g->ctx;
     const int n = g->n_var;
+    // output rows: n, or the folded operand's rows (n plus interface rows); S is [R][M]
+    const int M = folded ? (int)g->fold_rows : n;
     const int R = 2 * count;
     const int64_t ld = g->ldk;
     // column tiles: as few as possible, each a multiple of 32 columns (<= 256)
@@ -557,7 +646,7 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
         reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
     ctx->launches++;
     // A in tile order: rows of kBK elements, kBM rows per box
-    const uint64_t arows = (uint64_t)((n + kBM - 1) / kBM) * kBM * (uint64_t)(ld / kBK);
+    const uint64_t arows = (uint64_t)((M + kBM - 1) / kBM) * kBM * (uint64_t)(ld / kBK);
     CUtensorMap th = make_map(folded ? g->d_Ah.p : g->d_Th.p, kBK, arows, kBK, kBM);
     CUtensorMap tl = make_map(folded ? g->d_Al.p : g->d_Tl.p, kBK, arows, kBK, kBM);
     CUtensorMap xh = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
@@ -565,20 +654,20 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
     const int ktiles = (int)(ld / kBK);
     int *err = g->d_tc_err.p;
     // k-splits against wave quantisation; partials reduced in a fixed order
-    const int tiles = ntile * (int)((n + kBM - 1) / kBM);
+    const int tiles = ntile * (int)((M + kBM - 1) / kBM);
     int splits = choose_splits(tiles, ktiles, sm_count(ctx->device));
     const int kper = (ktiles + splits - 1) / splits;
     splits = (ktiles + kper - 1) / kper;
     double *out = S;
     if (splits > 1) {
-        const size_t pn = (size_t)splits * R * n;
+        const size_t pn = (size_t)splits * R * M;
         if (g->d_tcpart.n < pn) g->d_tcpart.alloc(ctx, pn);
         out = g->d_tcpart.p;
     }
 #define PLX_TC(BNV)                                                                               \
     case BNV:                                                                                     \
-        if (nprod == 1) launch_bn<BNV, 1>(g, R, th, tl, xh, xl, ktiles, splits, kper, out, err);  \
-        else launch_bn<BNV, 3>(g, R, th, tl, xh, xl, ktiles, splits, kper, out, err);             \
+        if (nprod == 1) launch_bn<BNV, 1>(g, M, R, th, tl, xh, xl, ktiles, splits, kper, out, err);  \
+        else launch_bn<BNV, 3>(g, M, R, th, tl, xh, xl, ktiles, splits, kper, out, err);             \
         break;
     switch (bn) {
         PLX_TC(32) PLX_TC(64) PLX_TC(96) PLX_TC(128) PLX_TC(160) PLX_TC(192) PLX_TC(224) PLX_TC(256)
@@ -586,7 +675,7 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
     }
 #undef PLX_TC
     if (splits > 1) {
-        const int64_t cnt = (int64_t)R * n;
+        const int64_t cnt = (int64_t)R * M;
         reduce_splits<<<(int)std::min<int64_t>(4096, n_blocks(cnt, 256)), 256, 0, ctx->stream>>>(cnt, splits, out, S);
         ctx->launches++;
         PLX_CHECK_CUDA(cudaGetLastError());

@@ -120,3 +120,16 @@ def test_on_the_fly_fp64_contraction_matches_stored(ctx, count):
     with Solver(p, ctx=ctx, store_t=False) as sv:
         otf = sv.contract(X, 'fp64_otf')
     assert np.max(np.linalg.norm(otf - ref, axis=1) / np.linalg.norm(ref, axis=1)) < 1e-12
+
+
+def test_mixed_alloy_on_memory_matches_lu(ctx):
+    """Stored-T alloy: the folded operand carries 1/2 (K + K^T) and the interface rows,
+    the w-dependent remainder is the interface correction; sigma_abs within 1e-6 of LU."""
+    p, s = _bowtie()
+    ref = osolve.solve(s, method='inversion')
+    with Solver(p, ctx=ctx, store_t=True) as sv:
+        b = sv.rhs(0, 1)
+        out = sv.solve(mode='iterative', precision='mixed_bf16x3', pol_mask=1, tol=1e-12 * np.linalg.norm(b[:, 0]))
+    assert (out['status'] == 0).all(), out['status']
+    sig, sref = out['results'][:, 9], ref['results'][:, 9]
+    assert np.max(np.abs(sig - sref) / np.abs(sref)) < 1e-6
