@@ -346,17 +346,6 @@ __global__ void gather_x(int n, const int32_t *__restrict__ act, const double *_
         dst[r] = src[r];
 }
 
-// Y[idx[k]] = X[k]: the inverse of gather_x.
-__global__ void scatter_cols(int n, const int32_t *__restrict__ idx, const double *__restrict__ X,
-                             double *__restrict__ Y) {
-    int k = blockIdx.y;
-    const double *src = X + (int64_t)k * 2 * n;
-    double *dst = Y + (int64_t)idx[k] * 2 * n;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n;
-         r += (int64_t)gridDim.x * blockDim.x)
-        dst[r] = src[r];
-}
-
 // Y[k] *= P[idx[k]] elementwise (complex), or in place on the column itself
 // when by_col (Y indexed by idx[k]).
 __global__ void scale_cols(int n, const int32_t *__restrict__ idx, const double *__restrict__ P,
@@ -453,8 +442,6 @@ static void gmres_impl(plx_geom *g, const GmresRequest &rq, const double *d_B, d
     std::vector<double2 *> h_hcols(m, nullptr);
     PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, st));
     DevArray<double> Pinv;
-    DevArray<int32_t> reo_pos, reo_cols;     // selective re-orthogonalisation (inner, long basis)
-    DevArray<double> reo_w;
     const bool jac = rq.jacobi && rq.inner;
     if (jac) {
         DevArray<int32_t> d_fall;
@@ -519,49 +506,17 @@ static void gmres_impl(plx_geom *g, const GmresRequest &rq, const double *d_B, d
         PLX_CHECK_CUDA(cudaMemsetAsync(hcols[j].p, 0, (size_t)C * hstride * 16, st));
         size_t need = (size_t)na * ndot * (j + 1);
         if (part.n < need) part.alloc(ctx, std::max(need, part.n * 2));
-        auto project_on = [&](int i0, int i1, int accumulate, int cnt, const int32_t *cols, double *W) {
+        auto project = [&](int i0, int i1, int accumulate) {
             int ni = i1 - i0;
-            dots_partial<VT><<<dim3(ndot, cnt), kThreads, 0, st>>>(n, i0, i1, cols, d_slabs.p, W, part.p);
-            dots_finish<<<dim3(n_blocks(ni, 128), cnt), 128, 0, st>>>(ndot, ni, i0, cols, part.p, hbuf.p,
-                                                                       hcols[j].p, hstride, accumulate);
-            ctx->launches += 2 + combine_chunked(st, n, i0, ni, cnt, cols, d_slabs.p, hbuf.p, -1.0, W, 0);
+            dots_partial<VT><<<dim3(ndot, na), kThreads, 0, st>>>(n, i0, i1, d_act.p, d_slabs.p, Wa.p, part.p);
+            dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st>>>(ndot, ni, i0, d_act.p, part.p,
+                                                                      hbuf.p, hcols[j].p, hstride,
+                                                                      accumulate);
+            ctx->launches += 2 + combine_chunked(st, n, i0, ni, na, d_act.p, d_slabs.p, hbuf.p, -1.0, Wa.p, 0);
         };
-        auto project = [&](int i0, int i1, int accumulate) { project_on(i0, i1, accumulate, na, d_act.p, Wa.p); };
         prof_begin(ctx);
         if (j + 1 < 25 && !rq.inner) {
             for (int i = 0; i <= j; ++i) project(i, i + 1, 0);        // modified Gram-Schmidt
-        } else if (rq.inner && !rq.single_pass) {
-            // inner solves with a long basis: classical GS, then a second pass only for the
-            // columns whose norm fell below 1/sqrt(2) of its value ("twice is enough")
-            batch_norms(g, na, Wa.p, nrm_part, nrm);
-            std::vector<double> n0(na), n1(na);
-            PLX_CHECK_CUDA(cudaMemcpyAsync(n0.data(), nrm.p, na * 8, cudaMemcpyDeviceToHost, st));
-            project(0, j + 1, 0);
-            batch_norms(g, na, Wa.p, nrm_part, nrm);
-            PLX_CHECK_CUDA(cudaMemcpyAsync(n1.data(), nrm.p, na * 8, cudaMemcpyDeviceToHost, st));
-            PLX_CHECK_CUDA(cudaStreamSynchronize(st));
-            std::vector<int32_t> pos, cols;
-            for (int k = 0; k < na; ++k)
-                if (!(n1[k] >= 0.7071067811865476 * n0[k])) {
-                    pos.push_back(k);
-                    cols.push_back(act[k]);
-                }
-            const int nr = (int)pos.size();
-            if (nr == na) {
-                project(0, j + 1, 1);
-            } else if (nr > 0) {
-                if (reo_pos.n < (size_t)na) {
-                    reo_pos.alloc(ctx, na);
-                    reo_cols.alloc(ctx, na);
-                    reo_w.alloc(ctx, (size_t)na * 2 * n);
-                }
-                PLX_CHECK_CUDA(cudaMemcpyAsync(reo_pos.p, pos.data(), nr * 4, cudaMemcpyHostToDevice, st));
-                PLX_CHECK_CUDA(cudaMemcpyAsync(reo_cols.p, cols.data(), nr * 4, cudaMemcpyHostToDevice, st));
-                gather_x<<<dim3(grid_rows(2LL * n), nr), 256, 0, st>>>(n, reo_pos.p, Wa.p, reo_w.p);
-                project_on(0, j + 1, 1, nr, reo_cols.p, reo_w.p);
-                scatter_cols<<<dim3(grid_rows(2LL * n), nr), 256, 0, st>>>(n, reo_pos.p, reo_w.p, Wa.p);
-                ctx->launches += 2;
-            }
         } else {
             project(0, j + 1, 0);                                     // classical GS ...
             if (!rq.single_pass) project(0, j + 1, 1);                // ... and re-orthogonalise
