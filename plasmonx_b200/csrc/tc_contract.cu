@@ -364,33 +364,44 @@ __global__ void split_tiled_gen(int N, int n, int fmu, int64_t ktiles, const dou
 // from the stored matrix or, without one, from the pair formulas.  One block
 // per (row, column chunk); rows vary fastest over the grid, so the blocks
 // running together share their neighbours' rows of T in L2.
-__device__ __forceinline__ double t_value(const double *__restrict__ T, int N, int n, int fmu,
+// T rows [t_row0, ...) held in T (stored matrix: t_row0 = 0; a generated
+// window of charge rows otherwise), or generated from the pair formulas.
+__device__ __forceinline__ double t_value(const double *__restrict__ T, int64_t t_row0, int N, int n, int fmu,
                                           const double *__restrict__ pos, const double *__restrict__ par, int64_t r,
                                           int64_t k) {
-    return T ? T[r * n + k] : plx_t_element(N, fmu != 0, pos, par, r, k);
+    return T ? T[(r - t_row0) * n + k] : plx_t_element(N, fmu != 0, pos, par, r, k);
 }
 
-__global__ void fold_split(int N, int n, int64_t ld, int64_t ktiles, int hetero, int fmu,
+// Charge rows [a0, a0 + gridDim.x) of T generated into a window buffer.
+__global__ void t_rows_gen(int N, int n, int fmu, int64_t a0, const double *__restrict__ pos,
+                           const double *__restrict__ par, double *__restrict__ Tw) {
+    const int64_t a = a0 + blockIdx.x;
+    const int64_t k = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+    if (k < n) Tw[(int64_t)blockIdx.x * n + k] = plx_t_element(N, fmu != 0, pos, par, a, k);
+}
+
+__global__ void fold_split(int N, int n, int64_t ld, int64_t ktiles, int hetero, int fmu, int64_t r_begin,
+                           int64_t t_row0,
                            const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                            const double *__restrict__ kval, const double *__restrict__ ktval,
                            const double *__restrict__ T, const double *__restrict__ pos,
                            const double *__restrict__ par, const int32_t *__restrict__ iface_atom,
                            __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
-    const int r = blockIdx.x;
+    const int64_t r = r_begin + blockIdx.x;
     const int64_t k = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
     if (k >= ld) return;
     double a = 0.0;
     if (k < n) {
         if (r < N) {
-            const double trk = t_value(T, N, n, fmu, pos, par, r, k);
+            const double trk = t_value(T, t_row0, N, n, fmu, pos, par, r, k);
             for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) {
                 const double c = hetero ? 0.5 * (kval[e] + ktval[e]) : kval[e];
-                a = fma(c, t_value(T, N, n, fmu, pos, par, col[e], k) - trk, a);
+                a = fma(c, t_value(T, t_row0, N, n, fmu, pos, par, col[e], k) - trk, a);
             }
         } else if (r < n) {
-            a = t_value(T, N, n, fmu, pos, par, r, k);
+            a = t_value(T, t_row0, N, n, fmu, pos, par, r, k);
         } else {
-            a = t_value(T, N, n, fmu, pos, par, iface_atom[r - n], k);
+            a = t_value(T, t_row0, N, n, fmu, pos, par, iface_atom[r - n], k);
         }
     }
     split_store(a, a_tiled(r, k, ktiles), hi, lo);
@@ -603,12 +614,70 @@ static void build_a_split(plx_geom *g) {
     // rows M..rows of the last m-tile are read by the kernel: zero them
     PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Ah.p, 0, (size_t)(rows * ld) * 2, g->ctx->stream));
     PLX_CHECK_CUDA(cudaMemsetAsync(g->d_Al.p, 0, (size_t)(rows * ld) * 2, g->ctx->stream));
-    dim3 grid((unsigned)M, (unsigned)((ld + 255) / 256));
-    fold_split<<<grid, 256, 0, g->ctx->stream>>>(
-        g->n_atoms, (int)n, ld, ktiles, hetero, g->model == PLX_WFQFMU, g->d_rowptr.p, g->d_col.p, g->d_kval.p,
-        g->d_ktval.p, g->has_T ? g->d_T.p : nullptr, g->d_pos.p, g->d_par.p, g->d_iface_atom.p,
-        reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p), reinterpret_cast<__nv_bfloat16 *>(g->d_Al.p));
-    g->ctx->launches++;
+    const int fmu = g->model == PLX_WFQFMU, N = g->n_atoms;
+    auto *hi = reinterpret_cast<__nv_bfloat16 *>(g->d_Ah.p);
+    auto *lo = reinterpret_cast<__nv_bfloat16 *>(g->d_Al.p);
+    const unsigned kchunks = (unsigned)((ld + 255) / 256);
+    cudaStream_t st = g->ctx->stream;
+    if (g->has_T) {
+        fold_split<<<dim3((unsigned)M, kchunks), 256, 0, st>>>(
+            N, (int)n, ld, ktiles, hetero, fmu, 0, 0, g->d_rowptr.p, g->d_col.p, g->d_kval.p, g->d_ktval.p, g->d_T.p,
+            g->d_pos.p, g->d_par.p, g->d_iface_atom.p, hi, lo);
+        g->ctx->launches++;
+    } else {
+        // matrix-free: dipole and interface rows generated element by element; the
+        // charge rows folded chunk by chunk from a window of generated T rows that
+        // covers the chunk's conductance neighbours (atoms are ordered in space, so
+        // a window is the chunk plus the neighbours' reach)
+        if (M > N) {
+            fold_split<<<dim3((unsigned)(M - N), kchunks), 256, 0, st>>>(
+                N, (int)n, ld, ktiles, hetero, fmu, N, 0, g->d_rowptr.p, g->d_col.p, g->d_kval.p, g->d_ktval.p,
+                nullptr, g->d_pos.p, g->d_par.p, g->d_iface_atom.p, hi, lo);
+            g->ctx->launches++;
+        }
+        std::vector<int32_t> rowptr(N + 1), col((size_t)g->nnz);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(rowptr.data(), g->d_rowptr.p, (N + 1) * 4, cudaMemcpyDeviceToHost, st));
+        if (g->nnz) PLX_CHECK_CUDA(cudaMemcpyAsync(col.data(), g->d_col.p, g->nnz * 4, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        const int64_t max_rows = std::max<int64_t>(64, (int64_t)(6.0e9 / (8.0 * (double)n)));   // <= ~6 GB window
+        DevArray<double> Tw;
+        Tw.alloc(g->ctx, (size_t)(max_rows * n));
+        int64_t r0 = 0;
+        while (r0 < N) {
+            // grow the chunk while its window fits
+            int64_t r1 = r0, lo_w = r0, hi_w = r0;
+            while (r1 < N) {
+                int64_t l = std::min<int64_t>(lo_w, r1), h = std::max<int64_t>(hi_w, r1);
+                for (int e = rowptr[r1]; e < rowptr[r1 + 1]; ++e) {
+                    l = std::min<int64_t>(l, col[e]);
+                    h = std::max<int64_t>(h, col[e]);
+                }
+                if (h - l + 1 > max_rows) break;
+                lo_w = l;
+                hi_w = h;
+                ++r1;
+            }
+            if (r1 == r0) {
+                // a single row reaching farther than the window: generate its T values in place
+                fold_split<<<dim3(1, kchunks), 256, 0, st>>>(N, (int)n, ld, ktiles, hetero, fmu, r0, 0, g->d_rowptr.p,
+                                                             g->d_col.p, g->d_kval.p, g->d_ktval.p, nullptr, g->d_pos.p,
+                                                             g->d_par.p, g->d_iface_atom.p, hi, lo);
+                g->ctx->launches++;
+                r0 = r0 + 1;
+                continue;
+            }
+            const int64_t W = hi_w - lo_w + 1;
+            t_rows_gen<<<dim3((unsigned)W, (unsigned)((n + 255) / 256)), 256, 0, st>>>(N, (int)n, fmu, lo_w, g->d_pos.p,
+                                                                                       g->d_par.p, Tw.p);
+            fold_split<<<dim3((unsigned)(r1 - r0), kchunks), 256, 0, st>>>(
+                N, (int)n, ld, ktiles, hetero, fmu, r0, lo_w, g->d_rowptr.p, g->d_col.p, g->d_kval.p, g->d_ktval.p,
+                Tw.p, g->d_pos.p, g->d_par.p, g->d_iface_atom.p, hi, lo);
+            g->ctx->launches += 2;
+            PLX_CHECK_CUDA(cudaGetLastError());
+            r0 = r1;
+        }
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+    }
     PLX_CHECK_CUDA(cudaGetLastError());
     if (!g->d_tc_err.p) {
         g->d_tc_err.alloc(g->ctx, 1);
