@@ -15,7 +15,9 @@ script
   3. parses the reference log ``tests/<name>/reference/<name>.log`` and stores
      the printed numbers in ``<name>/expected.json``: the final per-frequency
      results block (20 values), the charge / dipole tables, the GMRES residual
-     traces and, when printed, the full dynamic matrix.
+     traces, when printed the full dynamic matrix, the maxima analysis and the
+     frequencies recovered from backup files;
+  4. copies the test's backup files (``bk/*.plasmonX.bk``, restart tests).
 Nothing at run time of the tests reads the reference tree; only these files.
 """
 import json
@@ -49,6 +51,8 @@ TESTS = [
     'bem_ief_accurate_inversion',
     'bem_dpcm_accurate_inversion',
     'bem_dpcm_accurate_iterative_on_memory',
+    'wfq_sodium_restart',
+    'wfqfmu_ag_restart',
 ]
 
 NUM = r'[-+]?\d*\.\d+(?:[EeDd][-+]?\d+)?'
@@ -110,6 +114,14 @@ def parse_log(text):
             vals = [float(v) for v in re.findall(r'\s+\d+\s+(' + NUM + r')\n', pm.group(2))]
             traces.append({'freq_ev': freq_ev, 'pol': pm.group(1), 'residuals': vals})
     out['gmres'] = traces
+    # maxima analysis (print_maxima) and frequencies recovered from backups
+    m = re.search(r'Maxima Analysis: NumExFreq =\s+(\d+)\n\n.*?\n((?:\s+\d+\s+' + NUM + r'\s+' + NUM + r'\n)+)',
+                  text)
+    if m:
+        out['maxima'] = {'n_freq': int(m.group(1)),
+                         'rows': [[float(v) for v in re.findall(NUM, l)] for l in m.group(2).splitlines()]}
+    out['recovered_ev'] = [float(v) for v in re.findall(r'Recovering from backup frequency:\s+(' + NUM + r') eV',
+                                                        text)]
     # full dynamic matrix print (verbose 3, inversion)
     for part in ('Real', 'IMag'):
         key = 'matrix_' + part.lower()
@@ -197,6 +209,11 @@ def one(name, ref):
                     src = os.path.join(tdir, fn)
                     with open(os.path.join(odir, os.path.basename(fn)), 'w') as f:
                         f.write(csv_subset(src, fev))
+        bkdir = os.path.join(tdir, 'bk')
+        if os.path.isdir(bkdir):
+            os.makedirs(os.path.join(odir, 'bk'), exist_ok=True)
+            for fn in os.listdir(bkdir):
+                shutil.copy(os.path.join(bkdir, fn), os.path.join(odir, 'bk', fn))
         with open(os.path.join(tdir, 'reference', name + '.log')) as f:
             parsed = parse_log(f.read())
         with open(os.path.join(tdir, 'test')) as f:
