@@ -163,6 +163,16 @@ void plx_geometry_destroy(plx_geom *geom);
  * plx_set_frequencies then takes eps(w) (complex, one per frequency) in alpha_w.
  * The reference has no on-the-fly BEM product; PLX_GMRES_OTF is refused. */
 plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *desc, plx_geom **out);
+/* Induced field and plasmon density at points: the analysis step of the
+ * reference (calculate_induced_field_at_point_{wfq,wfqfmu} and
+ * calculate_density_at_point_{wfq,wfqfmu}, src/wfq/wfq_module.f90:590-650,
+ * src/wfq/wfqfmu_module.f90:975-1040).  x: one solution (complex, n_var,
+ * reference ordering) for polarisation i_pol (0 x, 1 y, 2 z), whose external
+ * field E0 is included in the field; points: 3 x n_points, bohr,
+ * column-major; field_out: 3 x n_points complex, density_out: n_points
+ * complex (either may be NULL).  Atomistic models only. */
+plx_status plx_field_at_points(plx_geom *geom, int32_t i_pol, const double *x, int32_t n_points,
+                               const double *points, double *field_out, double *density_out);
 /* Number of unknowns n_var (N for wFQ, 4N for wFQFMu, n_tess for BEM). */
 int64_t plx_geometry_n_var(const plx_geom *geom);
 /* Stored non-zeros of K (both triangles). */

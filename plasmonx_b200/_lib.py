@@ -21,7 +21,7 @@ EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes
            'plx_geometry_create', 'plx_bem_create', 'plx_geometry_destroy', 'plx_geometry_n_var', 'plx_geometry_k_nnz',
            'plx_set_frequencies', 'plx_matvec', 'plx_rhs', 'plx_gmres_solver', 'plx_complex_inversion',
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
-           'plx_profile_read', 'plx_contract', 'plx_contract_noalloc']
+           'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points']
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -93,6 +93,7 @@ def load():
     lib.plx_last_solve_launches.argtypes = [vp]
     lib.plx_contract.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int32]
     lib.plx_contract_noalloc.argtypes = [vp, C.c_int32, C.c_void_p, C.c_void_p]
+    lib.plx_field_at_points.argtypes = [vp, C.c_int32, _dp, C.c_int32, _dp, _dp, _dp]
     lib.plx_profile_enable.argtypes = [vp, C.c_int32]
     lib.plx_profile_read.argtypes = [vp, C.c_int32, _dp, C.POINTER(C.c_int64), _dp, _dp]
     _lib = lib

@@ -310,6 +310,35 @@ plx_status plx_matvec(plx_geom *g, int32_t i_freq, int32_t on_the_fly, const dou
     });
 }
 
+plx_status plx_field_at_points(plx_geom *g, int32_t i_pol, const double *x, int32_t n_points, const double *points,
+                               double *field_out, double *density_out) {
+    if (!g || !x || !points || n_points < 0) return PLX_ERR_ARG;
+    return guarded(g->ctx, [&] {
+        set_device(g->ctx);
+        if (is_bem(g)) throw Error(PLX_ERR_UNSUPPORTED, "field at points: atomistic models only");
+        if (i_pol < 0 || i_pol > 2) throw Error(PLX_ERR_ARG, "polarisation index must be 0, 1 or 2");
+        if (n_points == 0) return;
+        cudaStream_t st = g->ctx->stream;
+        DevArray<double> X, P, Fd, D;
+        X.alloc(g->ctx, 2 * (size_t)g->n_var);
+        P.alloc(g->ctx, 3 * (size_t)n_points);
+        Fd.alloc(g->ctx, 6 * (size_t)n_points);
+        D.alloc(g->ctx, 2 * (size_t)n_points);
+        // x stays interleaved complex; points to [3][P]
+        std::vector<double> pts(3 * (size_t)n_points);
+        for (int64_t i = 0; i < n_points; ++i)
+            for (int k = 0; k < 3; ++k) pts[(size_t)k * n_points + i] = points[3 * i + k];
+        PLX_CHECK_CUDA(cudaMemcpyAsync(X.p, x, 2 * (size_t)g->n_var * 8, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(P.p, pts.data(), pts.size() * 8, cudaMemcpyHostToDevice, st));
+        field_at_points(g, i_pol, X.p, n_points, P.p, Fd.p, D.p);
+        if (field_out)
+            PLX_CHECK_CUDA(cudaMemcpyAsync(field_out, Fd.p, 6 * (size_t)n_points * 8, cudaMemcpyDeviceToHost, st));
+        if (density_out)
+            PLX_CHECK_CUDA(cudaMemcpyAsync(density_out, D.p, 2 * (size_t)n_points * 8, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
 plx_status plx_rhs(plx_geom *g, int32_t i_freq, int32_t pol_mask, double *b) {
     if (!g || !b) return PLX_ERR_ARG;
     return guarded(g->ctx, [&] {

@@ -271,6 +271,11 @@ struct RefineResult {
 };
 void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, double *d_X, RefineResult &res);
 
+// analysis.cu: induced field (3 complex per point) and density (1 complex per
+// point) of one solution x (complex interleaved, n_var) at P points [3][P] bohr
+void field_at_points(plx_geom *g, int pol, const double *d_x, int P, const double *d_pts, double *d_field,
+                     double *d_dens);
+
 // observables.cu
 void polar_batch(plx_geom *g, int count, const int32_t *d_pol, const double *X,
                  Cplx *d_polar /* [count][3] : alpha(a, pol_c) */);

@@ -155,6 +155,18 @@ class Solver:
         self.ctx.check(self.lib.plx_complex_inversion(self.g, i_freq, ptr(buf.view(np.float64))))
         return buf.T.copy()
 
+    def field_at_points(self, i_pol, x, points):
+        """Induced field (P, 3) and density (P,) of solution x (n_var complex, polarisation
+        i_pol) at points (P, 3) in bohr; the external field E0 along i_pol is included."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        P = pts.shape[0]
+        field = np.zeros((P, 3), dtype=np.complex128)
+        dens = np.zeros(P, dtype=np.complex128)
+        self.ctx.check(self.lib.plx_field_at_points(self.g, int(i_pol), ptr(x.view(np.float64)), P, ptr(pts),
+                                                    ptr(field.view(np.float64)), ptr(dens.view(np.float64))))
+        return field, dens
+
     # ---- the spectrum -------------------------------------------------------
     def contract(self, X, how='fp64'):
         """S = T X for real columns X (count x n_var)."""
