@@ -407,13 +407,11 @@ static void gmres_impl(plx_geom *g, const GmresRequest &rq, const double *d_B, d
     const int nchunk = n_blocks(n, kRows);
     const int ndot = n_blocks(n, kDotRows);
     if ((size_t)(m + 1) * sizeof(double2) > 200 * 1024) throw Error(PLX_ERR_ARG, "GMRES dimension above 12800");
-    static bool tri_attr = false;
-    if (!tri_attr) {
+    once_per_device(reinterpret_cast<const void *>(tri_solve), ctx->device, [] {
         PLX_CHECK_CUDA(cudaFuncSetAttribute(tri_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-        tri_attr = true;
-    }
+    });
     const int hstride = m + 1;   // rows of an H column (0..m)
     DevArray<int32_t> d_act, d_freq_act, d_cols;
     d_act.alloc(ctx, C);

@@ -3,7 +3,10 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
+#include <set>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/plasmonx_b200.h"
@@ -286,6 +289,19 @@ void polar_batch(plx_geom *g, int count, const int32_t *d_pol, const double *X,
 enum ProfCat { PROF_TC = 0, PROF_FP64 = 1, PROF_ORTHO = 2, PROF_ROWS = 3, PROF_LSQ = 4 };
 void prof_begin(plx_ctx *ctx);
 void prof_end(plx_ctx *ctx, int cat, double flops, double bytes);
+
+// Runs fn once per (key, device) in the process; thread-safe.  Kernel attributes
+// (cudaFuncSetAttribute) belong to the device that is current, and several host
+// threads (one context each) may reach the same launch site.
+template <typename F>
+void once_per_device(const void *key, int device, F fn) {
+    static std::mutex m;
+    static std::set<std::pair<const void *, int>> done;
+    std::lock_guard<std::mutex> lk(m);
+    if (done.count({key, device})) return;
+    fn();
+    done.insert({key, device});
+}
 
 inline int n_blocks(int64_t work, int per_block) {
     int64_t b = (work + per_block - 1) / per_block;

@@ -426,19 +426,19 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
+    // initialised once, thread-safely (function-local static)
+    static const EncodeTiledFn fn = [] {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         PLX_CHECK_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
         if (!p || q != cudaDriverEntryPointSuccess) throw Error(PLX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
     return fn;
 }
 
 // 2-D BF16 tensor [outer][inner] with leading dimension ld (elements), boxes of
-// (64 inner x box_outer), 128-byte swizzle, zero fill out of bounds.
+// (kBK inner x box_outer), 64-byte swizzle, zero fill out of bounds.
 CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t ld, uint32_t box_outer) {
     CUtensorMap m;
     cuuint64_t dims[2] = {inner, outer};
@@ -458,11 +458,9 @@ void launch_bn(plx_geom *g, int M, int R, const CUtensorMap &th, const CUtensorM
     constexpr int ST = tc_stages<BN>();
     using L = TcSmem<BN, ST>;
     auto kern = tc_contract_kernel<BN, ST, NPROD>;
-    static bool attr = false;
-    if (!attr) {
+    once_per_device(reinterpret_cast<const void *>(kern), g->ctx->device, [&] {
         PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
-        attr = true;
-    }
+    });
     dim3 grid((R + BN - 1) / BN, (M + kBM - 1) / kBM, splits);
     kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, M, R, ktiles, kper, S, M, (int64_t)R * M, err);
     g->ctx->launches++;
@@ -479,12 +477,9 @@ __global__ void reduce_splits(int64_t count, int splits, const double *__restric
 }
 
 int sm_count(int device) {
-    static int cached_dev = -1, cached = 0;
-    if (device != cached_dev) {
-        PLX_CHECK_CUDA(cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, device));
-        cached_dev = device;
-    }
-    return cached;
+    int v = 0;
+    PLX_CHECK_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
+    return v > 0 ? v : 1;
 }
 
 // Number of k-splits for `tiles` output tiles: the fewest whose last wave fills
