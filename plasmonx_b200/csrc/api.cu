@@ -450,7 +450,18 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
                 fb = 1;
             } else {
                 uint64_t avail = ctx->budget > ctx->in_use ? ctx->budget - ctx->in_use : 0;
-                uint64_t per_col = (uint64_t)16 * n * (std::min(m, 64) + 8);
+                // device bytes per complex column: the plain form keeps an FP64 Krylov
+                // basis that grows with its (unrestarted) steps, counted up to 512;
+                // the refined forms a basis of the inner dimension (FP32 for the mixed
+                // forms) plus a dozen FP64 work vectors
+                uint64_t per_col;
+                if (!refined) {
+                    per_col = (uint64_t)16 * n * (std::min(m, 512) + 8);
+                } else {
+                    const int im = desc->inner_krylov > 0 ? std::min(desc->inner_krylov, n) : std::min(64, n);
+                    const uint64_t vb = desc->precision == PLX_FP64_REFINED ? 16 : 8;
+                    per_col = vb * n * (uint64_t)(im + 1) + (uint64_t)16 * n * 12;
+                }
                 fb = (int)std::max<uint64_t>(1, std::min<uint64_t>(avail / 2 / per_col / np, 256 / np));
             }
         }
