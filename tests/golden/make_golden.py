@@ -18,6 +18,9 @@ script
      traces, when printed the full dynamic matrix, the maxima analysis and the
      frequencies recovered from backup files;
   4. copies the test's backup files (``bk/*.plasmonX.bk``, restart tests).
+With ``--analysis`` it instead stores, for three analysis tests of the
+reference, the inputs of the field / density step and a sample of the cube
+file the reference wrote (``<name>/analysis.json``).
 Nothing at run time of the tests reads the reference tree; only these files.
 """
 import json
@@ -224,7 +227,64 @@ def one(name, ref):
               len(parsed['gmres']), 'traces', 'matrix' if 'matrix_real' in parsed else '')
 
 
+# analysis step (post-processing) of the reference: test name -> (cube file
+# suffix, quantity, polarisation index of the .freq block, frequency label)
+ANALYSIS = {
+    'analysis_field_3d_x_wfq_sodium': ('-Ex-1.5800000000.cube', 'field', 0, '1.5800000000'),
+    'analysis_field_3d_x_y_z_wfqfmu_ag': ('-Ez-3.0000000000.cube', 'field', 2, '3.0000000000'),
+    'analysis_density_3d_x_wfq_sodium': ('-Ex-1.5800000000-densityRe.cube', 'density_re', 0, '1.5800000000'),
+}
+
+
+def one_analysis(name, ref, stride=5):
+    """Inputs (geometry, widths, the solution of one polarisation) and a strided
+    sample of the reference's output cube for one analysis test."""
+    import tarfile
+    suffix, what, pol, flabel = ANALYSIS[name]
+    tdir = os.path.join(ref, 'tests', name)
+    with tempfile.TemporaryDirectory() as work:
+        with tarfile.open(os.path.join(tdir, name + '.tar.gz')) as tf:
+            tf.extractall(work)
+        with open(os.path.join(work, name + '.info')) as f:
+            info = f.read().splitlines()
+        with open(os.path.join(work, '%s-%s.freq' % (name, flabel))) as f:
+            freq = f.read().splitlines()
+    n_atoms = int(info[0].split(':')[1])
+    model = info[5].split(':')[1].strip()
+    e0 = float(info[7].split(':')[1])
+    g0 = info.index('Input Geometry (angstrom)') + 1
+    coords = [[float(v) for v in l.split()[2:5]] for l in info[g0:g0 + n_atoms]]
+    zs = [int(float(l.split()[0])) for l in info[g0:g0 + n_atoms]]
+    p0 = next(i for i, l in enumerate(info) if l.startswith('Parameters:'))
+    par = [float(v) for v in info[p0 + 2].split()[1:]]
+    rq = par[2] if model == 'wfq' else par[3]
+    rmu = par[4] if model == 'wfqfmu' else 0.0
+    heads = [i for i, l in enumerate(freq) if l.startswith('complex')]
+    rows = freq[heads[pol] + 1:(heads[pol + 1] if pol + 1 < len(heads) else len(freq))]
+    x = [[float(l.split()[1]), float(l.split()[2])] for l in rows if l.strip()]
+    with open(os.path.join(tdir, 'reference', 'post_process_' + name, name + suffix)) as f:
+        cube = f.read().splitlines()
+    dims = [int(cube[3 + k].split()[0]) for k in range(3)]
+    vals = [float(v) for l in cube[6 + n_atoms:] for v in l.split()]
+    assert len(vals) == dims[0] * dims[1] * dims[2]
+    idx = list(range(0, len(vals), stride))
+    out = {'name': name, 'model': model, 'e0': e0, 'coords_ang': coords, 'z': zs, 'rq': rq, 'rmu': rmu,
+           'pol': pol, 'quantity': what, 'x': x, 'n': dims, 'offset_ang': 10.0,
+           'cube_origin_bohr': [float(v) for v in cube[2].split()[1:4]],
+           'cube_step_bohr': [float(cube[3 + k].split()[1 + k]) for k in range(3)],
+           'sample_index': idx, 'sample_value': [vals[i] for i in idx]}
+    odir = os.path.join(HERE, name)
+    os.makedirs(odir, exist_ok=True)
+    with open(os.path.join(odir, 'analysis.json'), 'w') as f:
+        json.dump(out, f)
+    print(name, n_atoms, 'atoms', len(x), 'unknowns', len(idx), 'cube samples')
+
+
 if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[1] == '--analysis':
+        for nm in ANALYSIS:
+            one_analysis(nm, sys.argv[2])
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--one':
         one(sys.argv[2], sys.argv[3])
     else:

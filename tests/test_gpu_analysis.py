@@ -37,3 +37,21 @@ class _ctx:
 
     def __exit__(self, *a):
         self.c.close()
+
+
+@pytest.mark.parametrize('name', ['analysis_field_3d_x_wfq_sodium', 'analysis_field_3d_x_y_z_wfqfmu_ag',
+                                  'analysis_density_3d_x_wfq_sodium'])
+def test_field_and_density_reproduce_reference_cubes(name):
+    """The kernel against the cube files of the reference's analysis tests (E14.6)."""
+    from tests.test_analysis_golden import load_case, quantity
+    a, coords, pts, x, _, _ = load_case(name)
+    metal = {11: 'Na', 47: 'Ag', 79: 'Au'}[a['z'][0]]
+    p = configs.build(a['model'], np.array(a['coords_ang']), [metal], np.zeros(len(coords), np.int32),
+                      np.array([0.1]), e0=a['e0'])
+    assert np.isclose(p.r_q[0], a['rq']) and (a['model'] == 'wfq' or np.isclose(p.r_mu[0], a['rmu']))
+    with _ctx() as ctx:
+        with Solver(p, ctx=ctx) as sv:
+            E, rho = sv.field_at_points(a['pol'], x, pts)
+    v = quantity(a, E, rho)
+    ref = np.array(a['sample_value'])
+    assert np.all(np.abs(v - ref) <= 5.01e-6 * np.abs(ref) + 1e-30)
