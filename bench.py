@@ -1,7 +1,7 @@
 """Benchmark of the per-frequency response solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config ag_sphere|na_sphere|bowtie|bem_sphere|bem_rod]
+                    [--config ag_sphere|na_sphere|bowtie|bem_sphere|bem_rod|fq_water|fqfmu_water]
                     [--precision fp64|mixed_bf16x3] [--n-tess 2000] [--bem-variant dpcm|iefpcm]
 
 Workload (default): the wFQFMu silver sphere -- fcc a = 4.086 A cut to a 35 A
@@ -38,6 +38,13 @@ p50/p99 request latency and freq-solves/s.
 threaded C restatement of its on-the-fly product (oracle/pairs.c) over a
 bounded sample of matrix-vector products of the same geometry, turned into
 freq-solves/s with the Arnoldi step count per frequency-solve.
+
+Static workloads (--config fq_water / fqfmu_water): the static FQ / FQFMu solve
+(ground state: charges and energy) of a seeded cluster of --waters rigid water
+molecules (default 3000 FQ, 9,000 atoms and 12,000 unknowns; FQFMu 1000,
+13,000 unknowns) with the reference test's water parameters.  One step = one
+solve: the static matrix built on the device, its dense LU, the energy.  The
+CPU arm times the oracle's NumPy restatement (threaded LAPACK LU).
 
 BEM workloads (--config bem_sphere / bem_rod): a 10 nm sphere or a 40 x 10 nm
 prolate rod meshed into --n-tess tesserae (20 nu^2; 2000, 8000, 20480) with a
@@ -273,9 +280,116 @@ def cpu_sample(prob, n_mv, n_threads, steps_per_solve):
     return 1.0 / (dt * steps_per_solve), dt, op.n_threads
 
 
+STATIC_METRIC = 'static solves/s (ground state: charges and energy, FP64)'
+
+
+def static_problem(args):
+    from plasmonx_b200.static import water_cluster
+    ff = 'fq' if args.config == 'fq_water' else 'fqfmu'
+    n_mol = args.waters or (3000 if ff == 'fq' else 1000)
+    return water_cluster(n_mol, ff, what='energy', seed=11)
+
+
+def static_desc(prob):
+    return {'workload': '%s water cluster, %d molecules, %s kernel, ground state'
+                        % (prob.forcefield.upper(), prob.n_mol, prob.kernel),
+            'n_atoms': int(prob.n_atoms), 'n_var': int(prob.n_var),
+            'l2': 'inputs larger than L2 (static matrix %.2f GB)' % (8.0 * prob.n_var ** 2 / 1e9)}
+
+
+def static_cpu(prob):
+    """One solve of the oracle's restatement (threaded LAPACK) -> (solves/s, seconds)."""
+    from oracle import static as ost
+    o = ost.Static(prob.forcefield, prob.kernel, prob.coord, prob.atom_types, prob.apm, prob.chi, prob.eta,
+                   prob.alpha, prob.r_q, prob.r_mu, prob.rhs_form, prob.e0)
+    t0 = time.perf_counter()
+    o.solve('energy')
+    dt = time.perf_counter() - t0
+    return 1.0 / dt, dt
+
+
+def run_static(args):
+    rank, world, local, pg = dist_setup()
+    from plasmonx_b200.solver import Context
+    from plasmonx_b200.static import StaticSolver
+    prob = static_problem(args)
+    ctx = Context(local)
+    solver = StaticSolver(prob, ctx=ctx)
+    for _ in range(args.warmup):
+        solver.solve()
+    barrier(pg, local)
+    ctx.profile(True)
+    with Clocks(local) as clk:
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            out = solver.solve()
+        barrier(pg, local)
+        wall = time.perf_counter() - t0
+    asm, fac = ctx.profile_read(5), ctx.profile_read(6)
+    ctx.profile(False)
+    dev_ms = asm['ms'] + fac['ms']
+    value, solves, total_ms = job_throughput(pg, local, args.steps, dev_ms)
+    # end to end through the public API: host geometry in, variables and energy out
+    e2e = []
+    for _ in range(max(1, args.e2e_steps)):
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        o2 = StaticSolver(prob, ctx=ctx).solve()
+        barrier(pg, local)
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = allmax(pg, float(np.mean(e2e)), local)
+    h2d = prob.coord.nbytes + prob.atom_types.nbytes + prob.apm.nbytes + 5 * prob.chi.nbytes
+    pk, pk_kind = peaks()
+    asm_ms = asm['ms'] / max(1, asm['launches'])
+    asm_bytes = asm['bytes'] / max(1, asm['launches'])
+    fac_ms = fac['ms'] / max(1, fac['launches'])
+    roof = {'kernel': 'static_matrix_kernel (matrix and right-hand side build)', 'bound': 'hbm',
+            'achieved': asm_bytes / (asm_ms / 1000.0) / 1e9, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+            'peak_kind': pk_kind, 'bytes_per_launch': asm_bytes, 'avg_launch_ms': asm_ms, 'traffic': None,
+            'note': 'the dense LU (cuSOLVER dgetrf/dgetrs, a library) takes the rest of the step: %.2f ms, '
+                    '%.1f FP64 TFLOP/s' % (fac_ms, fac['flops'] / max(1, fac['launches']) / (fac_ms / 1e3) / 1e12)}
+    roof['frac'] = roof['achieved'] / roof['peak']
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, dt = static_cpu(prob)
+        cpu = {'value': v, 'unit': 'solves/s', 'cores': os.cpu_count(), 'kind': 'port',
+               'sample': 'one full solve of the NumPy restatement (threaded LAPACK LU), %.2f s' % dt}
+    if rank == 0:
+        line = {'metric': STATIC_METRIC, 'value': value, 'unit': 'solves/s', 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic (seeded water cluster, reference test parameters)', 'config': static_desc(prob),
+                'e2e': {'value': 1.0 / e2e_s, 'unit': 'solves/s', 'h2d_bytes_per_step': int(h2d),
+                        'd2h_bytes_per_step': int(prob.n_var * 8 + 8)},
+                'gpu_launches': 2 * args.steps, 'gpu_launches_note': 'library kernels; cuSOLVER launches not counted',
+                'roofline': roof, 'cpu_baseline': cpu, 'clocks': clk.summary(), 'wall_s_timed': wall,
+                'device_ms_breakdown': {'static_assembly': asm['ms'], 'static_factor': fac['ms']},
+                'energy': out['energy'], 'energy_e2e': o2['energy']}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def run_reference(args):
     rank, world, local, pg = dist_setup()
     if rank != 0:
+        return
+    if args.config in ('fq_water', 'fqfmu_water'):
+        prob = static_problem(args)
+        for _ in range(args.warmup):
+            static_cpu(prob)
+        vals = [static_cpu(prob)[0] for _ in range(args.steps)]
+        v = float(np.mean(vals))
+        line = {'metric': STATIC_METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': 1000.0 / v, 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded water cluster)',
+                'config': static_desc(prob), 'impl': 'reference',
+                'cpu_baseline': {'value': v, 'unit': 'solves/s', 'cores': os.cpu_count(), 'kind': 'port',
+                                 'sample': 'one full solve of the NumPy restatement per step'},
+                'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+        print(json.dumps(line), flush=True)
         return
     prob = make_problem(args.config, n_tess=args.n_tess, bem_variant=args.bem_variant)
     sps = args.steps_per_solve
@@ -306,7 +420,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', default='ag_sphere',
-                    choices=['ag_sphere', 'na_sphere', 'bowtie', 'bem_sphere', 'bem_rod'])
+                    choices=['ag_sphere', 'na_sphere', 'bowtie', 'bem_sphere', 'bem_rod', 'fq_water', 'fqfmu_water'])
+    ap.add_argument('--waters', type=int, default=0, help='water molecules of fq_water / fqfmu_water')
     ap.add_argument('--n-tess', type=int, default=2000, help='BEM tesserae (20 nu^2)')
     ap.add_argument('--bowtie-edge', type=float, default=80.0, help='prism edge (A): 80 gives 5,850 atoms, 180 ~30k')
     ap.add_argument('--bem-variant', default='dpcm', choices=['dpcm', 'iefpcm'])
@@ -332,6 +447,8 @@ def main():
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
+    if args.config in ('fq_water', 'fqfmu_water'):
+        return run_static(args)
 
     rank, world, local, pg = dist_setup()
     from plasmonx_b200.solver import Context, Solver

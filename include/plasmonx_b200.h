@@ -253,6 +253,78 @@ plx_status plx_contract(plx_geom *geom, int32_t count, const double *X, double *
  * the context's stream and returns when S is written. */
 plx_status plx_contract_noalloc(plx_geom *geom, int32_t count, const double *d_X, double *d_S);
 
+/* ---- static FQ / FQFMu ---------------------------------------------------- */
+
+/* The static force fields whose types the w-models extend
+ * (src/forcefield/fq_module.f90, src/forcefield/fqfmu_module.f90): charges
+ * (and, for FQFMu, dipoles) under electronegativity equalisation with one
+ * charge constraint per molecule, for the ground state or a static field. */
+typedef enum {
+    PLX_STATIC_FQ = 0,          /* n_var = n_atoms + n_mol */
+    PLX_STATIC_FQFMU = 1        /* n_var = 4 n_atoms + n_mol: charges, constraints, dipoles */
+} plx_static_forcefield;
+
+typedef enum {                  /* T_qq kernel (construct_static_t_qq, matrix_module.f90:58-115) */
+    PLX_KERNEL_COULOMB = 0,     /* 1/r, eta on the diagonal */
+    PLX_KERNEL_OHNO = 1,        /* eta_ij / sqrt(1 + eta_ij^2 r^2), eta_ij the mean hardness */
+    PLX_KERNEL_GAUSSIAN = 2     /* erf(r / sqrt(r_qi^2 + r_qj^2)) / r, eta on the diagonal */
+} plx_charge_kernel;
+
+typedef enum {
+    PLX_GROUND_STATE = 0,       /* solve_ground_state (algorithm_module.f90:91-115): rhs -chi */
+    PLX_STATIC_FIELD = 1        /* solve_static_field (algorithm_module.f90:120-145): 3 rhs */
+} plx_static_what;
+
+/* Geometry and parameters of a static problem (target_ after input).  Molecules
+ * are runs of consecutive atoms (create_n_atoms_per_molecule,
+ * src/input_output/input_module.f90:1007-1030); the constraint rows follow the
+ * reference's indexing (add_lagrangian_blocks, matrix_module.f90:351-382), exact
+ * for molecules of equal size; a geometry whose indexed rows would run past the
+ * atoms is refused with PLX_ERR_ARG. */
+typedef struct {
+    int32_t forcefield;         /* plx_static_forcefield */
+    int32_t kernel;             /* plx_charge_kernel */
+    int32_t n_atoms;
+    int32_t n_types;
+    int32_t n_mol;
+    int32_t rhs_potential;      /* static field: 0 V = -E0 r ("field"), 1 V = -E0 |r - r_min| */
+    const double *coord;        /* 3 x n_atoms, bohr */
+    const int32_t *atom_type;   /* n_atoms, 0-based */
+    const int32_t *atoms_per_molecule;  /* n_mol */
+    const double *chi;          /* electronegativity, per type */
+    const double *eta;          /* chemical hardness, per type */
+    const double *alpha;        /* polarizability (FQFMu), per type; may be NULL for FQ */
+    const double *r_q;          /* Gaussian charge width (Gaussian kernel, FQFMu) */
+    const double *r_mu;         /* Gaussian dipole width (FQFMu) */
+    double e0;                  /* field intensity (a.u.) */
+} plx_static_desc;
+
+/* n_var of a static problem, or -1 for an invalid description. */
+int64_t plx_static_n_var(const plx_static_desc *desc);
+
+/* Builds the static matrix and right-hand side on the device and solves them
+ * (construct_static_matrix, construct_ground_state_rhs /
+ * construct_static_field_rhs and real_inversion, algorithm_module.f90:91-145,
+ * :469-504).  Outputs (each may be NULL):
+ *   variables  n_var x n_rhs column-major, n_rhs = 1 (ground state) or 3
+ *              (static field x, y, z): target_%variables
+ *   energy     ground state: -1/2 x.b (calculate_energy_fq, fq_module.f90:374)
+ *   polar      static field, FQ: the 3 x 3 static polarizability, column-major
+ *              (calculate_static_polar_fq, fq_module.f90:396-595).  FQFMu
+ *              returns PLX_ERR_UNSUPPORTED, as the reference stops there. */
+plx_status plx_static_solve(plx_ctx *ctx, const plx_static_desc *desc, int32_t what, double *variables,
+                            double *energy, double *polar);
+
+/* rotate_principal_axis (src/target/target_module.f90:684-835), host only:
+ * moves the centre of mass (standard atomic masses by atomic number) to the
+ * origin and rotates coord (3 x n_atoms, in place) onto the eigenvectors of the
+ * inertia tensor, in ascending order of the eigenvalues.  Each eigenvector's
+ * sign (left to the implementation by LAPACK) makes its last nonzero component
+ * positive.  eigenvalues (3) and axes (3 x 3 column-major, the eigenvectors)
+ * may be NULL.  An atomic number without a mass returns PLX_ERR_ARG. */
+plx_status plx_principal_axes(int32_t n_atoms, const int32_t *atomic_number, double *coord, double *eigenvalues,
+                              double *axes);
+
 /* Device time (ms, CUDA events on the library's stream) of the last plx_solve,
  * and the number of kernels it launched. */
 double plx_last_solve_ms(const plx_geom *geom);
@@ -264,10 +336,12 @@ int64_t plx_last_solve_launches(const plx_geom *geom);
  * with CUDA events on its stream and accumulates their device time per
  * category: 0 tensor-core T contraction, 1 FP64 T contraction, 2 Arnoldi
  * orthogonalisation, 3 conductance and diagonal rows of the operator,
- * 4 least squares and solution updates.  For the contractions it also
- * accumulates, per launch, the algorithmic flops (2 n_var^2 x real columns)
- * and bytes (the stored T once at its storage precision, the input and output
- * columns).  Enabling resets the counters. */
+ * 4 least squares and solution updates, 5 static matrix and right-hand-side
+ * build (plx_static_solve), 6 static dense LU factorisations and solves.  For
+ * the contractions it also accumulates, per launch, the algorithmic flops
+ * (2 n_var^2 x real columns) and bytes (the stored T once at its storage
+ * precision, the input and output columns); for 5 the bytes written, for 6 the
+ * LU flops (2/3 n^3 + 2 n^2 n_rhs).  Enabling resets the counters. */
 plx_status plx_profile_enable(plx_ctx *ctx, int32_t on);
 /* Reads one category: accumulated time (ms), sections, flops and bytes. */
 plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,

@@ -21,7 +21,11 @@ EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes
            'plx_geometry_create', 'plx_bem_create', 'plx_geometry_destroy', 'plx_geometry_n_var', 'plx_geometry_k_nnz',
            'plx_set_frequencies', 'plx_matvec', 'plx_rhs', 'plx_gmres_solver', 'plx_complex_inversion',
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
-           'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points']
+           'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points',
+           'plx_static_n_var', 'plx_static_solve', 'plx_principal_axes']
+STATIC_FF = {'fq': 0, 'fqfmu': 1}
+KERNEL = {'coulomb': 0, 'ohno': 1, 'gaussian': 2}
+STATIC_WHAT = {'energy': 0, 'static': 1}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -39,6 +43,13 @@ class BemDesc(C.Structure):
     _fields_ = [('variant', C.c_int32), ('n_tess', C.c_int32), ('accurate', C.c_int32), ('triangles', _dp),
                 ('normal_factor', C.c_double), ('sphere_radius', C.c_double), ('eps_solvent', C.c_double),
                 ('e0', C.c_double)]
+
+
+class StaticDesc(C.Structure):
+    _fields_ = [('forcefield', C.c_int32), ('kernel', C.c_int32), ('n_atoms', C.c_int32), ('n_types', C.c_int32),
+                ('n_mol', C.c_int32), ('rhs_potential', C.c_int32), ('coord', _dp), ('atom_type', _ip),
+                ('atoms_per_molecule', _ip), ('chi', _dp), ('eta', _dp), ('alpha', _dp), ('r_q', _dp),
+                ('r_mu', _dp), ('e0', C.c_double)]
 
 
 class SolveDesc(C.Structure):
@@ -94,6 +105,10 @@ def load():
     lib.plx_contract.argtypes = [vp, C.c_int32, _dp, _dp, C.c_int32]
     lib.plx_contract_noalloc.argtypes = [vp, C.c_int32, C.c_void_p, C.c_void_p]
     lib.plx_field_at_points.argtypes = [vp, C.c_int32, _dp, C.c_int32, _dp, _dp, _dp]
+    lib.plx_static_n_var.restype = C.c_int64
+    lib.plx_static_n_var.argtypes = [C.POINTER(StaticDesc)]
+    lib.plx_static_solve.argtypes = [vp, C.POINTER(StaticDesc), C.c_int32, _dp, _dp, _dp]
+    lib.plx_principal_axes.argtypes = [C.c_int32, _ip, _dp, _dp, _dp]
     lib.plx_profile_enable.argtypes = [vp, C.c_int32]
     lib.plx_profile_read.argtypes = [vp, C.c_int32, _dp, C.POINTER(C.c_int64), _dp, _dp]
     _lib = lib

@@ -339,6 +339,22 @@ plx_status plx_field_at_points(plx_geom *g, int32_t i_pol, const double *x, int3
     });
 }
 
+int64_t plx_static_n_var(const plx_static_desc *desc) { return static_n_var(desc); }
+
+plx_status plx_static_solve(plx_ctx *ctx, const plx_static_desc *desc, int32_t what, double *variables,
+                            double *energy, double *polar) {
+    if (!ctx || !desc) return PLX_ERR_ARG;
+    return guarded(ctx, [&] {
+        set_device(ctx);
+        static_solve(ctx, desc, what, variables, energy, polar);
+    });
+}
+
+plx_status plx_principal_axes(int32_t n_atoms, const int32_t *atomic_number, double *coord, double *eigenvalues,
+                              double *axes) {
+    return guarded(nullptr, [&] { principal_axes(n_atoms, atomic_number, coord, eigenvalues, axes); });
+}
+
 plx_status plx_rhs(plx_geom *g, int32_t i_freq, int32_t pol_mask, double *b) {
     if (!g || !b) return PLX_ERR_ARG;
     return guarded(g->ctx, [&] {
@@ -627,7 +643,7 @@ plx_status plx_profile_enable(plx_ctx *ctx, int32_t on) {
 
 plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,
                             double *bytes) {
-    if (!ctx || category < 0 || category > 4) return PLX_ERR_ARG;
+    if (!ctx || category < 0 || category > 6) return PLX_ERR_ARG;
     return guarded(ctx, [&] {
         set_device(ctx);
         PLX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -134,6 +134,10 @@ struct BlasHandle {
     cublasHandle_t h = nullptr;
 };
 
+}  // namespace
+
+// One cuSOLVER / cuBLAS handle per host thread, bound to the context's stream
+// at every use (contexts are used by one thread at a time).
 cusolverDnHandle_t solver_handle(plx_ctx *ctx) {
     static thread_local SolverHandle sh;
     if (!sh.h) {
@@ -144,15 +148,18 @@ cusolverDnHandle_t solver_handle(plx_ctx *ctx) {
     return sh.h;
 }
 
-}  // namespace
-
-void bem_dgemm(plx_geom *g, const double *A, const double *B, double *C) {
+cublasHandle_t blas_handle(plx_ctx *ctx) {
     static thread_local BlasHandle bh;
     if (!bh.h && cublasCreate(&bh.h) != CUBLAS_STATUS_SUCCESS) throw Error(PLX_ERR_CUDA, "cublasCreate failed");
-    cublasSetStream(bh.h, g->ctx->stream);
+    cublasSetStream(bh.h, ctx->stream);
+    return bh.h;
+}
+
+void bem_dgemm(plx_geom *g, const double *A, const double *B, double *C) {
+    cublasHandle_t h = blas_handle(g->ctx);
     const int n = g->n_var;
     const double one = 1.0, zero = 0.0;
-    if (cublasDgemm(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, A, n, B, n, &zero, C, n) != CUBLAS_STATUS_SUCCESS)
+    if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, A, n, B, n, &zero, C, n) != CUBLAS_STATUS_SUCCESS)
         throw Error(PLX_ERR_CUDA, "cublasDgemm failed");
 }
 

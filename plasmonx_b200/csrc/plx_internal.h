@@ -279,6 +279,12 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
 void field_at_points(plx_geom *g, int pol, const double *d_x, int P, const double *d_pts, double *d_field,
                      double *d_dens);
 
+// static_fq.cu: static FQ / FQFMu solves and the principal-axis rotation
+int64_t static_n_var(const plx_static_desc *d);
+void static_solve(plx_ctx *ctx, const plx_static_desc *d, int what, double *variables, double *energy,
+                  double *polar);
+void principal_axes(int n, const int32_t *z, double *coord, double *eigenvalues, double *axes);
+
 // observables.cu
 void polar_batch(plx_geom *g, int count, const int32_t *d_pol, const double *X,
                  Cplx *d_polar /* [count][3] : alpha(a, pol_c) */);

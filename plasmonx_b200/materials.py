@@ -39,6 +39,18 @@ def atomic_number(name):
     return z
 
 
+# atom names the reference also accepts (assign_atomic_number,
+# src/target/target_module.f90:315-400)
+NAME_ALIASES = {'hw': 1, 'h-hw': 1, 'ow': 8, 'o-ow': 8}
+
+
+def atom_name_number(name):
+    """Atomic number of an atom name as the reference assigns it: element symbols and
+    the water names (HW, H-HW, OW, O-OW), case-insensitive; 0 when not recognised."""
+    key = name.strip().lower()
+    return ELEMENTS.get(key, NAME_ALIASES.get(key, 0))
+
+
 def nearest_distance(zi, zj):
     """Nearest-neighbour distance of an element pair (target_module.f90:472-518)."""
     if {zi, zj} <= {1, 8}:

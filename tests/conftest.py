@@ -16,12 +16,13 @@ def pytest_configure(config):
 
 
 def golden_dirs(kind=None):
-    """Fixture directories; kind 'atomistic' (wFQ/wFQFMu) or 'bem' filters them."""
+    """Fixture directories of one kind: 'atomistic' (wFQ / wFQFMu spectra), 'bem'
+    or 'static' (static FQ / FQFMu); None lists them all."""
     out = []
     for d in sorted(os.listdir(GOLDEN)):
         if not os.path.isfile(os.path.join(GOLDEN, d, 'expected.json')):
             continue
-        is_bem = d.startswith('bem_')
-        if kind is None or (kind == 'bem') == is_bem:
+        k = 'bem' if d.startswith('bem_') else ('static' if d.startswith('fq') else 'atomistic')
+        if kind is None or kind == k:
             out.append(d)
     return out

@@ -20,7 +20,10 @@ script
   4. copies the test's backup files (``bk/*.plasmonX.bk``, restart tests).
 With ``--analysis`` it instead stores, for three analysis tests of the
 reference, the inputs of the field / density step and a sample of the cube
-file the reference wrote (``<name>/analysis.json``).
+file the reference wrote (``<name>/analysis.json``).  With ``--static`` it
+stores, for the five static FQ / FQFMu tests, the keyword file and the numbers
+their logs print (static matrix, right-hand side, charges, dipoles, energy,
+J^-1, the polarizability tensor, the rotated geometry) in ``expected.json``.
 Nothing at run time of the tests reads the reference tree; only these files.
 """
 import json
@@ -280,7 +283,102 @@ def one_analysis(name, ref, stride=5):
     print(name, n_atoms, 'atoms', len(x), 'unknowns', len(idx), 'cube samples')
 
 
+STATIC = ['fq_energy', 'fq_polarizability', 'fq_principal_axis_energy', 'fqfmu_energy', 'fqfmu_rq_rmu_energy']
+
+
+def parse_matrix(text, title):
+    """Entries {"r,c": value} of a matrix printed by print_matrix under `title`."""
+    i = text.find(title)
+    if i < 0:
+        return None
+    lines = text[i:].splitlines()[2:]
+    entries, cols, seen = {}, None, False
+    for line in lines:
+        if line.startswith(' ---'):
+            if seen:
+                break
+            continue
+        toks = line.split()
+        if not toks:
+            continue
+        if all(re.fullmatch(r'\d+', t) for t in toks):
+            cols = [int(t) for t in toks]
+            continue
+        if cols and re.fullmatch(r'\d+', toks[0]):
+            seen = True
+            for c, v in zip(cols, toks[1:]):
+                entries['%s,%d' % (toks[0], c)] = float(v.replace('D', 'E'))
+    return entries
+
+
+def parse_table(text, title, width):
+    """Rows [index, values...] of a charges / dipoles / RHS table."""
+    i = text.find(title)
+    if i < 0:
+        return None
+    rows = []
+    for line in text[i:].splitlines()[1:]:
+        if line.startswith(' ---') or line.startswith(' ChErr'):
+            break
+        toks = line.split()
+        if len(toks) == width + 1 and re.fullmatch(r'\d+', toks[0]):
+            rows.append([float(v.replace('D', 'E')) for v in toks[1:]])
+    return rows
+
+
+def one_static(name, ref):
+    tdir = os.path.join(ref, 'tests', name)
+    yamls = [f for f in os.listdir(tdir) if f.endswith('.yaml')]
+    with tempfile.TemporaryDirectory() as work:
+        kw = run_front_end(ref, tdir, yamls[0], work)
+    odir = os.path.join(HERE, name)
+    os.makedirs(odir, exist_ok=True)
+    with open(os.path.join(odir, 'input.kw'), 'w') as f:
+        f.write(kw)
+    with open(os.path.join(tdir, 'reference', name + '.log')) as f:
+        text = f.read()
+    static = 'static response' in kw
+    width = 3 if static else 1
+    out = {'what': 'static' if static else 'energy'}
+    for key, title in (('matrix', ' FQ Matrix\n'), ('matrix', ' FQFMu Matrix\n'), ('j_inverse', ' JMatrix-1\n'),
+                       ('j_1_1', ' J_1_1 in calculate_static_polar\n'), ('polar', ' polarizability tensor (a.u.)\n')):
+        m = parse_matrix(text, title)
+        if m is not None:
+            out[key] = m
+    for key, title in (('rhs', ' RHS \n'), ('charges', ' Charges \n'), ('dipoles', ' Dipoles \n')):
+        t = parse_table(text, title, width)
+        if t is not None:
+            out[key] = t
+    m = re.search(r'ChErr\s+((?:' + NUM + r'\s+)+)', text)
+    if m:
+        out['charge_err'] = [float(v.replace('D', 'E')) for v in m.group(1).split()]
+    m = re.search(r'Energy =\s+(' + NUM + ')', text)
+    if m:
+        out['energy'] = float(m.group(1))
+    m = re.search(r'Polar Iso  =\s+(' + NUM + ')', text)
+    if m:
+        out['polar_iso'] = float(m.group(1))
+    i = text.find('Rotated Geometry (Ang)')
+    if i >= 0:
+        out['rotated'] = [[float(v) for v in l.split()[2:5]] for l in text[i:].splitlines()[5:]
+                          if re.match(r'^\s+\d+\s+\S+\s+' + NUM, l)]
+    with open(os.path.join(tdir, 'test')) as f:
+        out['runtest_filter'] = filters(f.read())
+    with open(os.path.join(odir, 'expected.json'), 'w') as f:
+        json.dump(out, f, indent=0)
+    print(name, sorted(out))
+
+
 if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[1] == '--static':
+        import subprocess
+        for nm in STATIC:
+            subprocess.run([sys.executable, os.path.abspath(__file__), '--one-static', nm, sys.argv[2]],
+                           check=True, stderr=subprocess.DEVNULL)
+        sys.exit(0)
+    if len(sys.argv) > 3 and sys.argv[1] == '--one-static':
+        one_static(sys.argv[2], sys.argv[3])
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--analysis':
         for nm in ANALYSIS:
             one_analysis(nm, sys.argv[2])
