@@ -308,9 +308,9 @@ int64_t plx_static_n_var(const plx_static_desc *desc);
  * :469-504).  Outputs (each may be NULL):
  *   variables  n_var x n_rhs column-major, n_rhs = 1 (ground state) or 3
  *              (static field x, y, z): target_%variables
- *   energy     ground state: -1/2 x.b (calculate_energy_fq, fq_module.f90:374)
+ *   energy     ground state: -1/2 x.b (calculate_energy_fq, fq_module.f90:358-374)
  *   polar      static field, FQ: the 3 x 3 static polarizability, column-major
- *              (calculate_static_polar_fq, fq_module.f90:396-595).  FQFMu
+ *              (calculate_static_polar_fq, fq_module.f90:379-595).  FQFMu
  *              returns PLX_ERR_UNSUPPORTED, as the reference stops there. */
 plx_status plx_static_solve(plx_ctx *ctx, const plx_static_desc *desc, int32_t what, double *variables,
                             double *energy, double *polar);

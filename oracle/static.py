@@ -9,17 +9,17 @@ Follows the reference's static and ground-state path:
   * charge-constraint rows and columns add_lagrangian_blocks
                                       src/matrix/matrix_module.f90:351-382
   * matrix layout: FQ [T_qq L; L^T 0] (construct_static_matrix_fq,
-    src/forcefield/fq_module.f90:179-208); FQFMu [T_qq L T_qmu; L^T 0 0;
+    src/forcefield/fq_module.f90:179-207); FQFMu [T_qq L T_qmu; L^T 0 0;
     T_qmu^T 0 T_mumu] (construct_static_matrix_fqfmu,
-    src/forcefield/fqfmu_module.f90:76-126)
-  * right-hand sides: ground state -chi per atom (fq_module.f90:213-240);
+    src/forcefield/fqfmu_module.f90:81-132)
+  * right-hand sides: ground state -chi per atom (fq_module.f90:212-242);
     static field construct_static_field_rhs_q / _mu
-                                      src/rhs/rhs_module.f90:43-130
+                                      src/rhs/rhs_module.f90:43-127
   * solve: dsysv on the upper triangle (real_inversion,
     src/solvers/algorithm_module.f90:469-504); the energy -1/2 x.b
-    (calculate_energy_fq, fq_module.f90:374-391); the static polarizability
+    (calculate_energy_fq, fq_module.f90:358-374); the static polarizability
     R^T J^-1 R - (1^T J^-1 R)^T (1^T J^-1 1)^-1 (1^T J^-1 R) with J the charge
-    block (calculate_static_polar_fq, fq_module.f90:396-595)
+    block (calculate_static_polar_fq, fq_module.f90:379-595)
   * molecules: n_atoms_per_molecule from runs of equal molecule index
     (create_n_atoms_per_molecule, src/input_output/input_module.f90:1007-1030)
   * principal axes: centre of mass, inertia tensor, eigenvectors in ascending
@@ -35,7 +35,7 @@ from scipy.special import erf
 TO_BOHR = 1.8897261254578281
 
 # atom names the reference maps to atomic numbers (assign_atomic_number,
-# src/target/target_module.f90:315-400); unknown names map to 0
+# src/target/target_module.f90:315-378); unknown names map to 0
 ATOM_NAMES = {'h': 1, 'hw': 1, 'h-hw': 1, 'he': 2, 'li': 3, 'be': 4, 'b': 5, 'c': 6, 'n': 7, 'o': 8,
               'ow': 8, 'o-ow': 8, 'f': 9, 'ne': 10, 'na': 11, 'mg': 12, 'al': 13, 'si': 14, 'p': 15,
               's': 16, 'cl': 17, 'ar': 18, 'ag': 47, 'cu': 29, 'au': 79}
@@ -164,7 +164,7 @@ class Static:
         return b
 
     def rhs_static_field(self):
-        """construct_static_field_rhs_q / _mu (rhs_module.f90:43-130)."""
+        """construct_static_field_rhs_q / _mu (rhs_module.f90:43-127)."""
         b = np.zeros((self.n_var, 3))
         c = self.coord
         if self.rhs_form == 'potential':

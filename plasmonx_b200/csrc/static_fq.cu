@@ -7,21 +7,21 @@
 //     charge-constraint row and column per molecule (add_lagrangian_blocks,
 //     :351-382) and, for FQFMu, T_qmu, its transpose and T_mumu with 1/alpha on
 //     the diagonal blocks (:120-345); layout of construct_static_matrix_fq
-//     (src/forcefield/fq_module.f90:179-208) and construct_static_matrix_fqfmu
-//     (src/forcefield/fqfmu_module.f90:76-126);
+//     (src/forcefield/fq_module.f90:179-207) and construct_static_matrix_fqfmu
+//     (src/forcefield/fqfmu_module.f90:81-132);
 //   * right-hand sides: -chi per atom for the ground state
-//     (construct_ground_state_rhs_fq, fq_module.f90:213-240), or the three
+//     (construct_ground_state_rhs_fq, fq_module.f90:212-242), or the three
 //     static-field columns (construct_static_field_rhs_q / _mu,
-//     src/rhs/rhs_module.f90:43-130);
+//     src/rhs/rhs_module.f90:43-127);
 //   * the solve: the reference factors with dsysv (Bunch-Kaufman on the upper
 //     triangle, real_inversion, src/solvers/algorithm_module.f90:469-504); the
 //     matrix built here is exactly symmetric, and the library factors it with
 //     cuSOLVER's pivoted LU (dgetrf / dgetrs), the same solution to rounding;
-//   * the ground-state energy -1/2 x.b (calculate_energy_fq, fq_module.f90:374)
+//   * the ground-state energy -1/2 x.b (calculate_energy_fq, fq_module.f90:358-374)
 //     and the FQ static polarizability
 //     R^T J^-1 R - (L^T J^-1 R)^T (L^T J^-1 L)^-1 (L^T J^-1 R), J the charge
 //     block and L the constraint columns (calculate_static_polar_fq,
-//     fq_module.f90:396-595; the reference forms J^-1 and (L^T J^-1 L)^-1
+//     fq_module.f90:379-595; the reference forms J^-1 and (L^T J^-1 L)^-1
 //     explicitly, here both are applied through their LU factors).
 // The principal-axis rotation (rotate_principal_axis,
 // src/target/target_module.f90:684-835) runs on the host: it is O(N) with a
@@ -143,7 +143,7 @@ __global__ void static_matrix_kernel(StaticDims s, const double *__restrict__ po
 // atom's type.  Static field: -E0 r_k ("field") or -E0 |r_k - min r_k|
 // ("potential") for the charges; for the dipoles of FQFMu the reference writes
 // E0 on the k-th component of column k when E0 is zero (|E0| <= 1e-14) and 1
-// otherwise (rhs_module.f90:100-128).
+// otherwise (rhs_module.f90:96-127).
 __global__ void static_rhs_kernel(StaticDims s, int field, int potential, double e0, double x0, double y0, double z0,
                                   const double *__restrict__ pos, const int32_t *__restrict__ type,
                                   const double *__restrict__ par, double *__restrict__ B) {

@@ -195,12 +195,12 @@ class StaticSolver:
 
 
 def energy_line(e):
-    """The reference's log line (calculate_energy_fq, fq_module.f90:386)."""
+    """The reference's log line (calculate_energy_fq, fq_module.f90:358-374)."""
     return ' Energy = %s a.u.' % fortran_f(e, 14, 8)
 
 
 def polar_iso_line(v):
-    """The reference's log line (calculate_static_polar_fq, fq_module.f90:585)."""
+    """The reference's log line (calculate_static_polar_fq, fq_module.f90:379-595)."""
     return ' Polar Iso  = %s a.u.' % fortran_f(v, 19, 10)
 
 
