@@ -297,6 +297,10 @@ typedef struct {
     const double *r_q;          /* Gaussian charge width (Gaussian kernel, FQFMu) */
     const double *r_mu;         /* Gaussian dipole width (FQFMu) */
     double e0;                  /* field intensity (a.u.) */
+    int32_t factorization;      /* 0 automatic: the charge constraints eliminated on a
+                                   null-space basis and the rest factored by Cholesky,
+                                   LU of the full system where that does not apply;
+                                   1 LU of the full system (the reference's form) */
 } plx_static_desc;
 
 /* n_var of a static problem, or -1 for an invalid description. */

@@ -49,7 +49,7 @@ class StaticDesc(C.Structure):
     _fields_ = [('forcefield', C.c_int32), ('kernel', C.c_int32), ('n_atoms', C.c_int32), ('n_types', C.c_int32),
                 ('n_mol', C.c_int32), ('rhs_potential', C.c_int32), ('coord', _dp), ('atom_type', _ip),
                 ('atoms_per_molecule', _ip), ('chi', _dp), ('eta', _dp), ('alpha', _dp), ('r_q', _dp),
-                ('r_mu', _dp), ('e0', C.c_double)]
+                ('r_mu', _dp), ('e0', C.c_double), ('factorization', C.c_int32)]
 
 
 class SolveDesc(C.Structure):

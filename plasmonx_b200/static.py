@@ -29,6 +29,9 @@ from .outputs import fortran_f
 from .solver import Context
 
 
+FACTORIZATION = {'auto': 0, 'lu': 1}
+
+
 def atoms_per_molecule(mol_index):
     """Number of atoms of each molecule: a molecule starts where the index changes."""
     mol_index = [int(v) for v in mol_index]
@@ -64,7 +67,7 @@ class StaticProblem:
 
     def __init__(self, forcefield, kernel, coord_ang, type_names, atom_types, mol_index, chi, eta, alpha=None,
                  r_q=None, r_mu=None, what='energy', rhs_form='field', e0=0.0, principal_axes=False,
-                 atom_names=None, method='inversion'):
+                 atom_names=None, method='inversion', factorization='auto'):
         self.forcefield = forcefield.lower()
         self.kernel = kernel.lower()
         if self.forcefield not in _lib.STATIC_FF:
@@ -75,6 +78,11 @@ class StaticProblem:
             raise ValueError("what must be 'energy' (ground state) or 'static' (static field)")
         self.what = what
         self.method = method
+        if factorization not in FACTORIZATION:
+            raise ValueError("factorization must be 'auto' or 'lu'")
+        # 'auto': charge constraints eliminated, Cholesky of the rest (LU where that
+        # does not apply); 'lu': LU of the full system, the reference's form
+        self.factorization = factorization
         self.type_names = list(type_names)
         nt = len(self.type_names)
         self.atom_types = np.ascontiguousarray(atom_types, dtype=np.int32)
@@ -114,6 +122,7 @@ class StaticProblem:
         d.chi, d.eta, d.alpha = _lib.ptr(self.chi), _lib.ptr(self.eta), _lib.ptr(self.alpha)
         d.r_q, d.r_mu = _lib.ptr(self.r_q), _lib.ptr(self.r_mu)
         d.e0 = self.e0
+        d.factorization = FACTORIZATION[self.factorization]
         return d
 
     @classmethod
@@ -212,7 +221,7 @@ WATER_FQFMU = {'O-OW': dict(chi=0.290842985, eta=0.582518114, alpha=2.218798372)
 
 
 def water_cluster(n_mol, forcefield='fq', kernel=None, what='energy', rhs_form='field', e0=0.0, seed=0,
-                  spacing=3.1, principal_axes=False):
+                  spacing=3.1, principal_axes=False, factorization='auto'):
     """A seeded synthetic water cluster: n_mol rigid waters (O-H 0.9572 A, H-O-H
     104.52 deg) with random orientations on a jittered cubic lattice of `spacing`
     Angstrom, one molecule index per water, typed O-OW / H-HW.  Gaussian widths
@@ -241,4 +250,4 @@ def water_cluster(n_mol, forcefield='fq', kernel=None, what='energy', rhs_form='
     types = [1, 0, 0] * n_mol
     return StaticProblem(forcefield, kernel, np.concatenate(coords), names, types, mol,
                          [params[n]['chi'] for n in names], eta, alpha, r_q, r_mu, what=what, rhs_form=rhs_form,
-                         e0=e0, principal_axes=principal_axes)
+                         e0=e0, principal_axes=principal_axes, factorization=factorization)

@@ -2,11 +2,13 @@
 
 The oracle (oracle/static.py) is pinned to the reference's five static logs
 (test_static_golden.py).  Here the device path -- matrix and right-hand sides
-built by the library's kernels, cuSOLVER LU, the energy and the FQ static
+built by the library's kernels, the charge constraints eliminated and the rest
+factored by Cholesky (or the full system by LU), the energy and the FQ static
 polarizability -- is compared with it:
   * the reference's five inputs: energy, charges, dipoles and polarizability
     relative 1e-11 to the oracle, and the logs' printed numbers at their printed
-    precision;
+    precision -- with the default factorisation (charge constraints eliminated,
+    Cholesky) and with LU of the full system (the reference's form);
   * seeded water clusters over the three charge kernels, both force fields,
     ground state and static field ('field' and 'potential' right-hand sides):
     variables relative 1e-10 (norm-wise), energy and polarizability 1e-11;
@@ -49,9 +51,11 @@ def _oracle(p):
                       p.rhs_form, p.e0)
 
 
+@pytest.mark.parametrize('factorization', ['auto', 'lu'])
 @pytest.mark.parametrize('name', CASES)
-def test_golden_static_matches_oracle_and_log(ctx, name):
+def test_golden_static_matches_oracle_and_log(ctx, name, factorization):
     p = StaticProblem.from_keyword_file(os.path.join(GOLDEN, name, 'input.kw'))
+    p.factorization = factorization
     with open(os.path.join(GOLDEN, name, 'expected.json')) as f:
         exp = json.load(f)
     out = StaticSolver(p, ctx=ctx).solve()
@@ -79,9 +83,10 @@ SYNTH = [(ff, kernel, what, form, e0)
          for what, form, e0 in (('energy', 'field', 0.0), ('static', 'field', 1e-3), ('static', 'potential', 2e-3))]
 
 
+@pytest.mark.parametrize('factorization', ['auto', 'lu'])
 @pytest.mark.parametrize('ff,kernel,what,form,e0', SYNTH, ids=lambda v: str(v))
-def test_water_clusters_match_oracle(ctx, ff, kernel, what, form, e0):
-    p = water_cluster(40, ff, kernel, what=what, rhs_form=form, e0=e0, seed=7)
+def test_water_clusters_match_oracle(ctx, ff, kernel, what, form, e0, factorization):
+    p = water_cluster(40, ff, kernel, what=what, rhs_form=form, e0=e0, seed=7, factorization=factorization)
     out = StaticSolver(p, ctx=ctx).solve()
     ref = _oracle(p).solve(what)
     assert _rel(out['variables'], ref['variables']) < 1e-10
@@ -89,6 +94,44 @@ def test_water_clusters_match_oracle(ctx, ff, kernel, what, form, e0):
         assert abs(out['energy'] - ref['energy']) <= 1e-11 * abs(ref['energy'])
     elif ff == 'fq':
         assert _rel(out['polar'], ref['polar']) < 1e-11
+
+
+@pytest.mark.parametrize('ff,what', [('fq', 'energy'), ('fq', 'static'), ('fqfmu', 'energy')])
+def test_elimination_is_the_default_path(ctx, ff, what):
+    """With positive definite blocks (Ohno, Gaussian) the default factors the
+    reduced system by Cholesky: the profiled flops are those of a reduced
+    Cholesky, not of the full LU, and the answers agree with the LU form."""
+    p = water_cluster(40, ff, what=what, e0=1e-3, seed=7)
+    ctx.profile(True)
+    auto = StaticSolver(p, ctx=ctx).solve()
+    fl = ctx.profile_read(6)['flops']
+    ctx.profile(False)
+    n, m = p.n_atoms, p.n_mol
+    nr = (n if ff == 'fq' else 4 * n) - m
+    ncols = (1 if what == 'energy' else 3) + (3 if (ff == 'fq' and what == 'static') else 0)
+    assert abs(fl - (nr ** 3 / 3.0 + 2.0 * nr * nr * ncols)) <= 1e-9 * fl
+    p.factorization = 'lu'
+    lu = StaticSolver(p, ctx=ctx).solve()
+    assert _rel(auto['variables'], lu['variables']) < 1e-11
+    if what == 'energy':
+        assert abs(auto['energy'] - lu['energy']) <= 1e-12 * abs(lu['energy'])
+    if 'polar' in lu:
+        assert _rel(auto['polar'], lu['polar']) < 1e-11
+
+
+@pytest.mark.parametrize('apm', [[2, 4], [3, 1, 2]])
+def test_ragged_molecules_follow_the_reference_rows(ctx, apm):
+    """Molecule sizes that differ: the constraint rows are the reference's
+    (disjoint for [2, 4]: eliminated; overlapping for [3, 1, 2]: LU)."""
+    for what in ('energy', 'static'):
+        p = water_cluster(2, 'fq', what=what, e0=1e-3, seed=5)
+        p.apm = np.array(apm, dtype=np.int32)
+        p.n_mol = len(apm)
+        out = StaticSolver(p, ctx=ctx).solve()
+        ref = _oracle(p).solve(what)
+        assert _rel(out['variables'], ref['variables']) < 1e-11
+        if what == 'static':
+            assert _rel(out['polar'], ref['polar']) < 1e-11
 
 
 def test_medium_fqfmu_cluster_matches_oracle(ctx):
