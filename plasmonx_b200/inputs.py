@@ -64,7 +64,7 @@ def read_keywords(text):
         n = int(float(kw.get('number of atoms', 0)))
         for line in lines[g0 + 1:g0 + 1 + n]:
             p = line.split()
-            geom.append((p[0], float(p[-3]), float(p[-2]), float(p[-1])))
+            geom.append((p[0], float(p[-3]), float(p[-2]), float(p[-1]), int(p[1]) if len(p) > 4 else 1))
     return kw, types, params, inter, geom
 
 
@@ -108,7 +108,8 @@ class Problem:
     def __init__(self, model, coord_ang, type_names, atom_types, eta, r_q, r_mu, tau, sigma0, scaling,
                  a_ij, fermi_d, fermi_s, freqs, e0=1e-4, alpha_w=None, rhs_form='field',
                  polarization='all', method='inversion', tolerance=1e-9, gmres_dim=1000, n_iter=1000,
-                 fermi_energy=None, atom_names=None, permittivity=None):
+                 fermi_energy=None, atom_names=None, permittivity=None, kernel='gaussian', chi=None, alpha=None,
+                 mol_index=None, principal_axes=False):
         self.raw = dict(tau=list(map(float, tau)), sigma0=list(map(float, sigma0)),
                         scaling=list(map(float, scaling)), permittivity=permittivity,
                         fermi_energy=None if fermi_energy is None else list(map(float, fermi_energy)))
@@ -147,6 +148,24 @@ class Problem:
                              for b in range(nt)] for a in range(nt)])
         self.neighbours, self.n_neighbours = neighbour_counts(self.coord_ang, self.atom_types, self.znum, nt)
         self.coord = self.coord_ang * M.TO_BOHR
+        # carried for the .info file: charge kernel, the static force field the
+        # w-model extends, chi / alpha per type, molecule index per atom
+        self.kernel = kernel
+        self.forcefield = 'fq' if self.model == 'wfq' else 'fqfmu'
+        self.chi = np.zeros(nt) if chi is None else np.asarray(chi, dtype=np.float64)
+        self.alpha = np.zeros(nt) if alpha is None else np.asarray(alpha, dtype=np.float64)
+        self.mol_index = (np.ones(self.n_atoms, dtype=np.int64) if mol_index is None
+                          else np.asarray(mol_index, dtype=np.int64))
+        from .static import atoms_per_molecule, rotate_principal_axes
+        self.apm = atoms_per_molecule(self.mol_index)
+        self.n_mol = len(self.apm)
+        # rotate_principal_axis runs after the input (and its neighbour counts),
+        # before any solve (src/plasmonX.f90:37-38)
+        self.principal_axes = bool(principal_axes)
+        self.inertia = None
+        if self.principal_axes:
+            self.coord, w, v = rotate_principal_axes(self.coord, self.znum)
+            self.inertia = {'eigenvalues': w, 'axes': v}
         self.freqs = np.asarray(freqs, dtype=np.float64)
         self.e0 = float(e0)
         self.rhs_form = rhs_form
@@ -250,7 +269,7 @@ class Problem:
                 elif fn != 'none':
                     alpha_w[t] = M.read_table(fn if os.path.isabs(fn) else os.path.join(base_dir, fn), freqs)
         atom_names = [g[0] for g in geom]
-        return cls(model, np.array([g[1:] for g in geom]), names, [idx[n] for n in atom_names],
+        return cls(model, np.array([g[1:4] for g in geom]), names, [idx[n] for n in atom_names],
                    get(types, 'eta'), get(types, 'rq'), get(types, 'rmu'), get(plist, 'tau'),
                    get(plist, 'sigma0'), get(plist, 'scaling sigma0-tau'), get(plist, 'a_ij'), fd, fs,
                    freqs, e0=float(kw.get('field field intensity', 1e-4)), alpha_w=alpha_w,
@@ -259,7 +278,10 @@ class Problem:
                    tolerance=float(kw.get('algorithm tolerance', 0.0)),
                    gmres_dim=int(float(kw.get('algorithm gmres dimension', 1000))),
                    n_iter=int(float(kw.get('algorithm number of iterations', 1000))),
-                   fermi_energy=get(plist, 'fermi energy'), atom_names=atom_names)
+                   fermi_energy=get(plist, 'fermi energy'), atom_names=atom_names,
+                   kernel=kw.get('forcefield kernel', 'gaussian').strip().lower(), chi=get(types, 'chi'),
+                   alpha=get(types, 'alpha'), mol_index=[g[4] for g in geom],
+                   principal_axes=kw.get('control principal axes', 'False').strip().lower() == 'true')
 
     @classmethod
     def from_keyword_file(cls, path):

@@ -20,7 +20,9 @@ script
   4. copies the test's backup files (``bk/*.plasmonX.bk``, restart tests).
 With ``--analysis`` it instead stores, for three analysis tests of the
 reference, the inputs of the field / density step and a sample of the cube
-file the reference wrote (``<name>/analysis.json``).  With ``--static`` it
+file the reference wrote (``<name>/analysis.json``).  With ``--info`` it copies three
+``.info`` files and one ``.freq`` file out of the reference's analysis-test
+tarballs into ``info/`` (the files its analysis tool reads).  With ``--static`` it
 stores, for the five static FQ / FQFMu tests, the keyword file and the numbers
 their logs print (static matrix, right-hand side, charges, dipoles, energy,
 J^-1, the polarizability tensor, the rotated geometry) in ``expected.json``.
@@ -369,7 +371,28 @@ def one_static(name, ref):
     print(name, sorted(out))
 
 
+INFO = {'analysis_field_3d_x_wfq_sodium': ['analysis_field_3d_x_wfq_sodium.info'],
+        'analysis_field_3d_x_y_z_wfqfmu_ag': ['analysis_field_3d_x_y_z_wfqfmu_ag.info',
+                                              'analysis_field_3d_x_y_z_wfqfmu_ag-3.0000000000.freq'],
+        'analysis_pqr_bem': ['analysis_pqr_bem.info']}
+
+
+def copy_info(ref):
+    import tarfile
+    odir = os.path.join(HERE, 'info')
+    os.makedirs(odir, exist_ok=True)
+    for name, members in INFO.items():
+        with tarfile.open(os.path.join(ref, 'tests', name, name + '.tar.gz')) as tf:
+            for m in members:
+                with open(os.path.join(odir, m), 'wb') as f:
+                    f.write(tf.extractfile(m).read())
+                print('info/' + m)
+
+
 if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[1] == '--info':
+        copy_info(sys.argv[2])
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--static':
         import subprocess
         for nm in STATIC:

@@ -93,3 +93,27 @@ def test_fortran_edit_descriptors():
     assert O.fortran_e(0.0, 14, 6) == '  0.000000E+00'
     assert O.fortran_e(10.671, 12, 5) == ' 0.10671E+02'
     assert O.fortran_f(2.0, 7, 5) == '2.00000'
+
+
+def test_spectrum_packed_with_its_info(tmp_path):
+    """save_info: the run's .info is written first and packed at the end with the CSV
+    and the .freq files into <stem>.tar.gz (make_targz); what the analysis step reads
+    comes back out of the archive."""
+    import tarfile
+    name = 'wfq_sodium_inversion'
+    d, exp, p = _load(name)
+    stem = str(tmp_path / name)
+    sv = OracleSolver(p, os.path.join(d, 'input.kw'))
+    out = O.solve_spectrum(sv, stem, save_freq=True, save_info=True)
+    with tarfile.open(out['paths']['tar']) as tf:
+        names = sorted(tf.getnames())
+        info = O.read_info(tf.extractfile(name + '.info').read().decode())
+        fname = os.path.basename(O.freq_path(stem, p.freqs[0]))
+        _, ev, blocks = O.read_freq(tf.extractfile(fname).read().decode())
+    assert name + '.info' in names and name + '.csv' in names
+    assert len([n for n in names if n.endswith('.freq')]) == len(p.freqs)
+    assert info['terminated'] and info['model'] == 'wfq' and info['n_atoms'] == p.n_atoms
+    np.testing.assert_allclose(info['coord_ang'], p.coord_ang, rtol=1e-15, atol=1e-14)
+    np.testing.assert_allclose(info['freqs_ev'], p.freqs * O.M.AU_TO_EV, rtol=1e-15)
+    assert ev == pytest.approx(O.freq_ev(p.freqs[0]), rel=1e-15)
+    assert not glob.glob(stem + '*.freq') and not os.path.exists(stem + '.info')
