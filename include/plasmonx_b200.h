@@ -173,6 +173,18 @@ plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *desc, plx_geom **out
  * complex (either may be NULL).  Atomistic models only. */
 plx_status plx_field_at_points(plx_geom *geom, int32_t i_pol, const double *x, int32_t n_points,
                                const double *points, double *field_out, double *density_out);
+/* get_neighbours (src/target/target_module.f90:417-464) on the device: per atom
+ * the number of atoms within the nearest-neighbour distance r0 of the pair
+ * (counting the atom itself) and the per-type counts the wFQFMu dipole diagonal
+ * divides by it.  coord_ang: 3 x n_atoms in ANGSTROM -- the reference tests
+ * sqrt(dx^2 + dy^2 + dz^2) * ToBohr <= r0 on the input coordinates, and the
+ * same expression is evaluated here without fused operations; atom_type
+ * 0-based; type_z the atomic number of each type; r0: n_types x n_types, bohr.
+ * Out: neighbours_out n_types x n_atoms (the `neighbours` array of
+ * plx_geometry_desc), n_neighbours_out n_atoms.  At most 16 atom types. */
+plx_status plx_neighbour_counts(plx_ctx *ctx, int32_t n_atoms, int32_t n_types, const double *coord_ang,
+                                const int32_t *atom_type, const int32_t *type_z, const double *r0,
+                                int32_t *neighbours_out, int32_t *n_neighbours_out);
 /* Number of unknowns n_var (N for wFQ, 4N for wFQFMu, n_tess for BEM). */
 int64_t plx_geometry_n_var(const plx_geom *geom);
 /* Stored non-zeros of K (both triangles). */

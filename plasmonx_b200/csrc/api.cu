@@ -339,6 +339,16 @@ plx_status plx_field_at_points(plx_geom *g, int32_t i_pol, const double *x, int3
     });
 }
 
+plx_status plx_neighbour_counts(plx_ctx *ctx, int32_t n_atoms, int32_t n_types, const double *coord_ang,
+                                const int32_t *atom_type, const int32_t *type_z, const double *r0,
+                                int32_t *neighbours_out, int32_t *n_neighbours_out) {
+    if (!ctx) return PLX_ERR_ARG;
+    return guarded(ctx, [&] {
+        set_device(ctx);
+        neighbour_counts(ctx, n_atoms, n_types, coord_ang, atom_type, type_z, r0, neighbours_out, n_neighbours_out);
+    });
+}
+
 int64_t plx_static_n_var(const plx_static_desc *desc) { return static_n_var(desc); }
 
 plx_status plx_static_solve(plx_ctx *ctx, const plx_static_desc *desc, int32_t what, double *variables,

@@ -279,6 +279,10 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
 void field_at_points(plx_geom *g, int pol, const double *d_x, int P, const double *d_pts, double *d_field,
                      double *d_dens);
 
+// neighbours.cu: neighbour counts per atom (cell list on the device)
+void neighbour_counts(plx_ctx *ctx, int n, int nt, const double *coord_ang, const int32_t *atom_type,
+                      const int32_t *type_z, const double *r0, int32_t *nb_out, int32_t *n_nb_out);
+
 // static_fq.cu: static FQ / FQFMu solves and the principal-axis rotation
 int64_t static_n_var(const plx_static_desc *d);
 void static_solve(plx_ctx *ctx, const plx_static_desc *d, int what, double *variables, double *energy,

@@ -11,7 +11,8 @@ derived quantities the reference computes at input time:
     factor (assign_model_parameters_wfq, src/wfq/wfq_module.f90:96-127);
   * neighbour counts per atom type (get_neighbours,
     src/target/target_module.f90:417-464), evaluated on the Angstrom
-    coordinates times ToBohr exactly as the reference does;
+    coordinates times ToBohr exactly as the reference does (here on the host,
+    on demand; the solver counts on the device, plx_neighbour_counts);
   * coordinates scaled to bohr (input_module.f90:238);
   * the GMRES tolerance multiplied by sqrt(n_var) (input_module.f90:250-251);
   * alpha_t(w) per atom type from the Etchegoin fits or a CSV table
@@ -146,7 +147,7 @@ class Problem:
         self.tau, self.sigma0, self.density = tau, sigma0, dens
         self.r0 = np.array([[M.nearest_distance(int(self._type_z(a)), int(self._type_z(b)))
                              for b in range(nt)] for a in range(nt)])
-        self.neighbours, self.n_neighbours = neighbour_counts(self.coord_ang, self.atom_types, self.znum, nt)
+        self._nb = None
         self.coord = self.coord_ang * M.TO_BOHR
         # carried for the .info file: charge kernel, the static force field the
         # w-model extends, chi / alpha per type, molecule index per atom
@@ -182,6 +183,25 @@ class Problem:
             self.alpha_w = np.ascontiguousarray(alpha_w, dtype=np.complex128).reshape(nt, len(self.freqs))
         else:
             self.alpha_w = None
+
+    def _counts(self):
+        if self._nb is None:
+            self._nb = neighbour_counts(self.coord_ang, self.atom_types, self.znum, len(self.type_names))
+        return self._nb
+
+    @property
+    def neighbours(self):
+        """Per-type neighbour counts (n_types x N), on the host; the solver counts on the
+        device (plx_neighbour_counts) with the same test."""
+        return self._counts()[0]
+
+    @property
+    def n_neighbours(self):
+        return self._counts()[1]
+
+    @property
+    def type_z(self):
+        return np.array([self._type_z(t) for t in range(len(self.type_names))], dtype=np.int32)
 
     def _type_z(self, t):
         hit = np.nonzero(self.atom_types == t)[0]

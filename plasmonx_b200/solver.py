@@ -82,17 +82,26 @@ class Solver:
         if store_t is None:
             store_t = prob.method != 'iterative on the fly'
         nt = len(prob.type_names)
+        # neighbour counts on the device, from the input Angstrom coordinates
+        r0 = np.asfortranarray(prob.r0).ravel(order='F')
+        atom_type = np.ascontiguousarray(prob.atom_types, dtype=np.int32)
+        nb = np.zeros((prob.n_atoms, nt), dtype=np.int32)                       # (N,nt) row-major == nt x N
+        nnb = np.zeros(prob.n_atoms, dtype=np.int32)
+        ang = np.ascontiguousarray(prob.coord_ang, dtype=np.float64)
+        tz = prob.type_z
+        self.ctx.check(self.lib.plx_neighbour_counts(self.ctx.h, prob.n_atoms, nt, ptr(ang), ptr(atom_type, _lib._ip),
+                                                     ptr(tz, _lib._ip), ptr(r0), ptr(nb, _lib._ip),
+                                                     ptr(nnb, _lib._ip)))
+        self.neighbours, self.n_neighbours = nb.T, nnb
         self._keep = dict(
             coord=np.ascontiguousarray(prob.coord, dtype=np.float64),            # (N,3) row-major == 3xN col-major
-            atom_type=np.ascontiguousarray(prob.atom_types, dtype=np.int32),
-            neighbours=np.ascontiguousarray(prob.neighbours.T, dtype=np.int32),   # (N,nt) row-major == nt x N
-            n_neighbours=np.ascontiguousarray(prob.n_neighbours, dtype=np.int32),
+            atom_type=atom_type, neighbours=nb, n_neighbours=nnb,
             eta=np.ascontiguousarray(prob.eta), r_q=np.ascontiguousarray(prob.r_q),
             r_mu=np.ascontiguousarray(prob.r_mu), tau=np.ascontiguousarray(prob.tau),
             density=np.ascontiguousarray(prob.density), a_ij=np.ascontiguousarray(prob.a_ij),
             fermi_d=np.asfortranarray(prob.fermi_d).ravel(order='F'),
             fermi_s=np.asfortranarray(prob.fermi_s).ravel(order='F'),
-            r0=np.asfortranarray(prob.r0).ravel(order='F'))
+            r0=r0)
         k = self._keep
         d = _lib.GeometryDesc(
             _lib.MODEL[prob.model], prob.n_atoms, nt, 1 if prob.rhs_form == 'potential' else 0,
