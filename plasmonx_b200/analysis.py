@@ -1,0 +1,232 @@
+"""Field and density on grids: the analysis step of the reference on the device.
+
+The reference's analysis program (src/plasmonX_analysis) reads a run's
+``.tar.gz`` (the ``.info`` description and the ``.freq`` solutions), builds a
+grid around the particle and writes |E|/E0 or the plasmon density on it:
+  * grids: create_cubic_grid / create_plane_grid (grid_module.f90:64-154) --
+    the atoms' bounding box (Angstrom) widened by ``offset`` on every side,
+    or bounds given by the user, with n points per axis and
+    step = (max - min) / (n - 1); a plane keeps its third coordinate fixed;
+  * values: calculate_field_3d / calculate_density_3d (grid_module.f90:200-301)
+    and their plane versions (:310-453), evaluated here for all points at once
+    by plx_field_at_points (csrc/analysis.cu); |E| is the norm of the complex
+    field over its six real components, divided by E0;
+  * files: the cube file (write_cube_file, plot_module.f90:496-562: origin and
+    steps in bohr, atoms as atomic number, 0.0 and bohr coordinates, values
+    E14.6 six per line with z fastest) and the maximum's log lines
+    (print_quantity_analysis_3d, plot_module.f90:620-669: the first maximum
+    in Fortran order, x fastest).
+Grid arrays here are indexed [i, j, k] = [x, y, z].
+"""
+import os
+import tarfile
+
+import numpy as np
+
+from . import materials as M
+from . import outputs as O
+
+
+class Grid:
+    """A regular grid: bounds (Angstrom), points per axis (0 for the fixed axis of a plane)."""
+
+    def __init__(self, lo, hi, n):
+        self.lo = np.asarray(lo, dtype=np.float64)
+        self.hi = np.asarray(hi, dtype=np.float64)
+        self.n = [int(v) for v in n]
+        self.step = np.array([(self.hi[k] - self.lo[k]) / (self.n[k] - 1) if self.n[k] > 1 else 0.0
+                              for k in range(3)])
+
+    def axes(self):
+        return [self.lo[k] + np.arange(max(self.n[k], 1)) * self.step[k] for k in range(3)]
+
+    def points_ang(self):
+        """(nx * ny * nz, 3) points, x fastest (the reference's loop order)."""
+        ax, ay, az = self.axes()
+        Z, Y, X = np.meshgrid(az, ay, ax, indexing='ij')
+        return np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+    def shape(self):
+        return tuple(max(v, 1) for v in self.n)
+
+    def info_text(self):
+        """Grid Information block of the analysis log (print_grid_3d_info, grid_module.f90:159-192)."""
+        s = O.STICKS
+        L = [' ' * 27 + 'Grid Information (Angstrom)', s,
+             ' ' * 10 + ''.join('%s%s  ' % (lab, O.fortran_f(v, 12, 4)) for lab, v in
+                                zip(('StepX: ', 'StepY: ', 'StepZ: '), self.step)), s]
+        for k, ax in enumerate('XYZ'):
+            L += [' ' * 10 + '%sminGrid:%s  %smaxGrid:%s  %s NPoints:%7d' % (
+                ax, O.fortran_f(self.lo[k], 10, 4), ax, O.fortran_f(self.hi[k], 10, 4), ax, self.n[k]), s]
+        return '\n'.join(L) + '\n'
+
+
+def cubic_grid(coord_ang, n=(30, 30, 30), offset=10.0, lo=None, hi=None):
+    """create_cubic_grid: the bounding box of the atoms +- offset (Angstrom), or lo / hi."""
+    c = np.asarray(coord_ang, dtype=np.float64).reshape(-1, 3)
+    lo = c.min(axis=0) - offset if lo is None else lo
+    hi = c.max(axis=0) + offset if hi is None else hi
+    return Grid(lo, hi, n)
+
+
+def plane_grid(coord_ang, plane, n=(30, 30), offset=10.0, lo=None, hi=None):
+    """create_plane_grid: plane 'xy', 'xz' or 'yz'; the fixed axis has bounds 0 and
+    no points (its coordinate is given when the plane is evaluated)."""
+    axes = {'xy': (0, 1), 'xz': (0, 2), 'yz': (1, 2)}[plane]
+    c = np.asarray(coord_ang, dtype=np.float64).reshape(-1, 3)
+    glo, ghi, gn = np.zeros(3), np.zeros(3), [0, 0, 0]
+    for a, m in zip(axes, n):
+        glo[a] = c[:, a].min() - offset if lo is None else lo[a]
+        ghi[a] = c[:, a].max() + offset if hi is None else hi[a]
+        gn[a] = m
+    g = Grid(glo, ghi, gn)
+    g.plane = plane
+    return g
+
+
+def _points_bohr(grid, third=0.0):
+    """Grid points in bohr; a plane's fixed coordinate is `third` (Angstrom)."""
+    pts = grid.points_ang()
+    plane = getattr(grid, 'plane', None)
+    if plane is not None:
+        fixed = {'xy': 2, 'xz': 1, 'yz': 0}[plane]
+        pts[:, fixed] = third
+    return pts * M.TO_BOHR
+
+
+def field_on_grid(solver, x, i_pol, grid, e0, third=0.0):
+    """|E| / E0 on the grid (nx, ny, nz) for solution x of polarisation i_pol."""
+    E, _ = solver.field_at_points(i_pol, x, _points_bohr(grid, third))
+    v = np.sqrt((E.real ** 2 + E.imag ** 2).sum(axis=1)) / e0
+    nx, ny, nz = grid.shape()
+    return v.reshape(nz, ny, nx).transpose(2, 1, 0)
+
+
+def density_on_grid(solver, x, grid, third=0.0):
+    """The plasmon density (complex) on the grid (nx, ny, nz)."""
+    _, rho = solver.field_at_points(0, x, _points_bohr(grid, third))
+    nx, ny, nz = grid.shape()
+    return rho.reshape(nz, ny, nx).transpose(2, 1, 0)
+
+
+def cube_text(grid, values, z=None, coord_ang=None, centres_ang=None, title='Generated by plasmonX analysis'):
+    """write_cube_file: atoms (z, coord_ang) or, for BEM, tessera centres."""
+    vals = np.asarray(values, dtype=np.float64)
+    nx, ny, nz = vals.shape
+    bem = centres_ang is not None
+    pos = np.asarray(centres_ang if bem else coord_ang, dtype=np.float64).reshape(-1, 3)
+    f12 = lambda v: O.fortran_f(v, 12, 6)  # noqa: E731
+    L = [title, '',
+         '%8d' % len(pos) + ''.join(f12(v * M.TO_BOHR) for v in grid.lo),
+         '%8d' % nx + f12(grid.step[0] * M.TO_BOHR) + f12(0.0) + f12(0.0),
+         '%8d' % ny + f12(0.0) + f12(grid.step[1] * M.TO_BOHR) + f12(0.0),
+         '%8d' % nz + f12(0.0) + f12(0.0) + f12(grid.step[2] * M.TO_BOHR)]
+    for a in range(len(pos)):
+        L.append('%5d ' % (0 if bem else int(z[a])) + O.fortran_f(0.0, 10, 6) +
+                 ''.join(f12(v * M.TO_BOHR) for v in pos[a]))
+    for i in range(nx):
+        for j in range(ny):
+            row = vals[i, j]
+            row = np.where(np.abs(row) > 1.0e-99, row, 0.0)
+            for k0 in range(0, nz, 6):
+                L.append(''.join(' ' + O.fortran_e(v, 14, 6) for v in row[k0:k0 + 6]))
+    return '\n'.join(L) + '\n'
+
+
+def maximum(grid, values):
+    """Value and grid coordinates (Angstrom) of the first maximum in Fortran order."""
+    v = np.asarray(values)
+    flat = v.transpose(2, 1, 0).ravel()            # x fastest
+    idx = int(np.argmax(flat))
+    nx, ny, _ = v.shape
+    i, j, k = idx % nx, (idx // nx) % ny, idx // (nx * ny)
+    return float(flat[idx]), grid.lo + np.array([i, j, k]) * grid.step
+
+
+def maximum_lines(kind, pol_name, grid, values):
+    """print_quantity_analysis_3d lines: kind 'Field', 'RhoRe' or 'RhoIm'."""
+    m, at = maximum(grid, values)
+    return ('  %s%sX%sY%sZ%sMax.\n' % (kind, ' ' * 11, ' ' * 16, ' ' * 16, ' ' * 13) +
+            '   %s  %s   %s\n' % (pol_name, ''.join(O.fortran_f(c, 15, 5) + '  ' for c in at),
+                                 O.fortran_e(m, 13, 6)))
+
+
+def read_archive(path):
+    """The .info description and the .freq solutions of a run's .tar.gz:
+    (info dict, {freq label: (variable, freq eV, {'x'|'y'|'z': complex array})})."""
+    sols = {}
+    info = None
+    with tarfile.open(path) as tf:
+        for m in tf.getmembers():
+            text = tf.extractfile(m).read().decode()
+            if m.name.endswith('.info'):
+                info = O.read_info(text)
+            elif m.name.endswith('.freq'):
+                label = m.name[:-5].rsplit('-', 1)[1]
+                sols[label] = O.read_freq(text)
+    if info is None:
+        raise ValueError('%s holds no .info file' % path)
+    return info, sols
+
+
+def problem_from_info(info):
+    """A dynamic atomistic problem with the geometry, widths and dynamic parameters of a
+    .info file (what the analysis step needs: positions, r_q, r_mu, E0)."""
+    from .inputs import Problem
+    if info['model'] not in ('wfq', 'wfqfmu'):
+        raise ValueError('analysis on the device: atomistic runs only (the .info model is %r)' % info['model'])
+    names = [t[0] for t in info['types']]
+    nt = len(names)
+    par = [t[1] for t in info['types']]
+    if info['model'] == 'wfq':
+        chi, eta, rq = ([p[k] for p in par] for k in range(3))
+        alpha, rmu = [0.0] * nt, [0.0] * nt
+    else:
+        chi, eta, alpha, rq, rmu = ([p[k] for p in par] for k in range(5))
+    dyn = np.array(info['dynamic'])
+    # each atom takes the type of its element (the .info names the types by element)
+    type_of_z = {M.atomic_number(nm): t for t, nm in enumerate(names)}
+    try:
+        types = [type_of_z[int(v)] for v in info['z']]
+    except KeyError:
+        raise ValueError('an atom whose element names no atom type of the .info')
+    freqs = np.asarray(info.get('freqs_ev', []), dtype=np.float64) / M.AU_TO_EV
+    return Problem(info['model'], info['coord_ang'], names, types, eta, rq, rmu, dyn[:, 0], dyn[:, 1], [1.0] * nt,
+                   dyn[:, 2], np.diag(dyn[:, 3]), np.diag(dyn[:, 4]), freqs, e0=info['e0'],
+                   alpha_w=None if info['model'] == 'wfq' else np.zeros((nt, len(freqs)), complex),
+                   fermi_energy=dyn[:, 5], kernel=info['kernel'], chi=chi, alpha=alpha,
+                   mol_index=info['mol_index'], atom_names=[names[t] for t in types])
+
+
+def cube_path(root, pol_name, freq_label, suffix=''):
+    """<root>-<Ex|Ey|Ez>-<freq f12.10><suffix>.cube, as plot_field_or_density names them."""
+    return '%s-%s-%s%s.cube' % (root, pol_name, freq_label, suffix)
+
+
+def write_cubes(path, solver, info, solution, pols=('x', 'y', 'z'), what='field', n=(30, 30, 30), offset=10.0,
+                root=None):
+    """Cube files of one frequency's solutions (a read_freq triple) for the given
+    polarisations: |E|/E0 (what='field') or the density's real and imaginary parts."""
+    variable, ev, blocks = solution
+    label = O.fortran_f(ev, 12, 10).strip()
+    if root is None:
+        root = path[:-len('.tar.gz')] if path.endswith('.tar.gz') else os.path.splitext(path)[0]
+    grid = cubic_grid(info['coord_ang'], n, offset)
+    written = []
+    for p in pols:
+        if p not in blocks:
+            continue
+        i_pol = 'xyz'.index(p)
+        pol_name = 'E' + p
+        if what == 'field':
+            v = field_on_grid(solver, blocks[p], i_pol, grid, info['e0'])
+            outs = [(cube_path(root, pol_name, label), v)]
+        else:
+            rho = density_on_grid(solver, blocks[p], grid)
+            outs = [(cube_path(root, pol_name, label, '-densityRe'), rho.real),
+                    (cube_path(root, pol_name, label, '-densityIm'), rho.imag)]
+        for fn, v in outs:
+            with open(fn, 'w') as f:
+                f.write(cube_text(grid, v, info['z'], info['coord_ang']))
+            written.append(fn)
+    return grid, written

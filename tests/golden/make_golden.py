@@ -273,11 +273,25 @@ def one_analysis(name, ref, stride=5):
     vals = [float(v) for l in cube[6 + n_atoms:] for v in l.split()]
     assert len(vals) == dims[0] * dims[1] * dims[2]
     idx = list(range(0, len(vals), stride))
+    # the cube header after its title line, and the analysis log's grid block and
+    # the maximum lines of this polarisation
+    cube_head = cube[2:6 + n_atoms]
+    logs = [f for f in os.listdir(os.path.join(tdir, 'reference', 'post_process_' + name)) if f.endswith('.log')]
+    with open(os.path.join(tdir, 'reference', 'post_process_' + name, logs[0])) as f:
+        log = f.read().splitlines()
+    g = log.index(next(l for l in log if 'Grid Information (Angstrom)' in l))
+    log_grid = log[g:g + 10]
+    log_max = []
+    for k, l in enumerate(log):
+        if l.startswith('   E' + 'xyz'[pol] + ' ') and k > 0 and 'Max.' in log[k - 1]:
+            log_max += [log[k - 1], l]
+    out_extra = {'cube_head': cube_head, 'log_grid': log_grid, 'log_max': log_max}
     out = {'name': name, 'model': model, 'e0': e0, 'coords_ang': coords, 'z': zs, 'rq': rq, 'rmu': rmu,
            'pol': pol, 'quantity': what, 'x': x, 'n': dims, 'offset_ang': 10.0,
            'cube_origin_bohr': [float(v) for v in cube[2].split()[1:4]],
            'cube_step_bohr': [float(cube[3 + k].split()[1 + k]) for k in range(3)],
            'sample_index': idx, 'sample_value': [vals[i] for i in idx]}
+    out.update(out_extra)
     odir = os.path.join(HERE, name)
     os.makedirs(odir, exist_ok=True)
     with open(os.path.join(odir, 'analysis.json'), 'w') as f:

@@ -51,3 +51,66 @@ def test_oracle_reproduces_reference_cube(name):
     tol = 5.01e-6 * np.abs(ref) + 1e-30
     bad = np.abs(v - ref) > tol
     assert not bad.any(), (np.nonzero(bad)[0][:5], v[bad][:5], ref[bad][:5])
+
+
+# ---- the product's grid, cube and maximum formatting (plasmonx_b200/analysis.py) ----
+
+def _grid(a):
+    from plasmonx_b200 import analysis as A
+    return A.cubic_grid(np.array(a['coords_ang']), tuple(a['n']), a['offset_ang'])
+
+
+@pytest.mark.parametrize('name', NAMES)
+def test_grid_block_matches_reference_log(name):
+    with open(os.path.join(GOLDEN, name, 'analysis.json')) as f:
+        a = json.load(f)
+    mine = _grid(a).info_text().splitlines()
+    assert [l.rstrip() for l in mine] == [l.rstrip() for l in a['log_grid']]
+
+
+@pytest.mark.parametrize('name', NAMES)
+def test_cube_header_matches_reference(name):
+    """Origin, steps and atoms of the cube header: the same numbers as printed (the
+    reference's archived cubes come from a release that wrote the counts as i5; the
+    current writer, plot_module.f90:512, uses i8)."""
+    from plasmonx_b200 import analysis as A
+    with open(os.path.join(GOLDEN, name, 'analysis.json')) as f:
+        a = json.load(f)
+    g = _grid(a)
+    text = A.cube_text(g, np.zeros(tuple(a['n'])), a['z'], np.array(a['coords_ang']))
+    head = text.splitlines()[2:6 + len(a['z'])]
+    assert [l.split() for l in head] == [l.split() for l in a['cube_head']]
+    atom_lines = head[4:]
+    assert all(m == r for m, r in zip(atom_lines, a['cube_head'][4:]))     # (i5,1x,f10.6,3f12.6) unchanged
+
+
+@pytest.mark.parametrize('name', NAMES)
+def test_maximum_lines_match_reference_log(name):
+    """The oracle's full grid, through the product's grid order and maximum search,
+    gives the maximum the reference's analysis log printed (value at E13.6; the
+    location is the reference's or a symmetric point whose value ties within 1e-12)."""
+    from plasmonx_b200 import analysis as A
+    a, coords, _, x, _, _ = load_case(name)
+    g = _grid(a)
+    pts = g.points_ang() * TO_BOHR
+    N = coords.shape[0]
+    E, rho = field_and_density(coords, np.full(N, a['rq']), np.full(N, a['rmu']), x, a['e0'], a['pol'], pts,
+                               a['model'] == 'wfqfmu')
+    nx, ny, nz = a['n']
+    shape = lambda v: v.reshape(nz, ny, nx).transpose(2, 1, 0)  # noqa: E731
+    pol = 'E' + 'xyz'[a['pol']]
+    if a['quantity'] == 'field':
+        blocks = [('Field', shape(np.sqrt((np.abs(E) ** 2).sum(axis=1)) / a['e0']))]
+    else:
+        blocks = [('RhoRe', shape(rho.real)), ('RhoIm', shape(rho.imag))]
+    ref = a['log_max']
+    for b, (kind, vals) in enumerate(blocks):
+        lines = A.maximum_lines(kind, pol, g, vals).splitlines()
+        assert lines[0] == ref[2 * b]
+        mine, theirs = lines[1].split(), ref[2 * b + 1].split()
+        assert mine[0] == theirs[0] and mine[4] == theirs[4]
+        if mine[1:4] != theirs[1:4]:
+            at = np.array([float(v) for v in theirs[1:4]])
+            ijk = np.rint((at - g.lo) / g.step).astype(int)
+            m, _ = A.maximum(g, vals)
+            assert abs(vals[tuple(ijk)] - m) <= 1e-12 * abs(m)

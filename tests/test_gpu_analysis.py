@@ -2,6 +2,8 @@
 oracle's restatement of the reference's analysis step; relative 1e-12 norm-wise,
 on random points around the particle and on points sitting on atoms (inside the
 0.1 bohr cut-off of the field terms)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -55,3 +57,67 @@ def test_field_and_density_reproduce_reference_cubes(name):
     v = quantity(a, E, rho)
     ref = np.array(a['sample_value'])
     assert np.all(np.abs(v - ref) <= 5.01e-6 * np.abs(ref) + 1e-30)
+
+
+@pytest.mark.parametrize('name', ['analysis_field_3d_x_wfq_sodium', 'analysis_field_3d_x_y_z_wfqfmu_ag',
+                                  'analysis_density_3d_x_wfq_sodium'])
+def test_full_grid_on_device_reproduces_reference_analysis(name, tmp_path):
+    """The whole 30^3 grid through the product's analysis module: the cube's sampled
+    values at E14.6 and the maximum line of the reference's analysis log."""
+    from plasmonx_b200 import analysis as A
+    from tests.test_analysis_golden import load_case
+    a, coords, _, x, _, _ = load_case(name)
+    metal = {11: 'Na', 47: 'Ag', 79: 'Au'}[a['z'][0]]
+    p = configs.build(a['model'], np.array(a['coords_ang']), [metal], np.zeros(len(coords), np.int32),
+                      np.array([0.1]), e0=a['e0'])
+    g = A.cubic_grid(np.array(a['coords_ang']), tuple(a['n']), a['offset_ang'])
+    pol = 'E' + 'xyz'[a['pol']]
+    with _ctx() as ctx:
+        with Solver(p, ctx=ctx, store_t=False) as sv:
+            if a['quantity'] == 'field':
+                blocks = [('Field', A.field_on_grid(sv, x, a['pol'], g, a['e0']))]
+            else:
+                rho = A.density_on_grid(sv, x, g)
+                blocks = [('RhoRe', rho.real), ('RhoIm', rho.imag)]
+    # the cube of the quantity the reference test wrote
+    cube = A.cube_text(g, blocks[0][1], a['z'], np.array(a['coords_ang'])).splitlines()[6 + len(a['z']):]
+    vals = np.array([float(v) for l in cube for v in l.split()])
+    ref = np.array(a['sample_value'])
+    mine = vals[np.array(a['sample_index'])]
+    assert np.all(np.abs(mine - ref) <= 1.0001e-6 * np.abs(ref) + 1e-30)    # one unit of the 6th digit
+    assert np.mean(mine == ref) > 0.99                                         # and mostly the same digits
+    for b, (kind, v) in enumerate(blocks):
+        lines = A.maximum_lines(kind, pol, g, v).splitlines()
+        theirs = a['log_max'][2 * b + 1].split()
+        assert lines[0] == a['log_max'][2 * b] and lines[1].split()[4] == theirs[4]
+        at = np.array([float(t) for t in theirs[1:4]])
+        ijk = tuple(np.rint((at - g.lo) / g.step).astype(int))
+        m, _ = A.maximum(g, v)
+        assert abs(v[ijk] - m) <= 1e-12 * abs(m)
+
+
+def test_analysis_from_a_run_archive(tmp_path):
+    """A spectrum packed with save_info / save_freq, read back as the reference's
+    analysis program reads it, gives the same field on the grid as the run's solver."""
+    from plasmonx_b200 import analysis as A
+    from plasmonx_b200 import outputs as O
+    p = configs.particle('Na', 'sphere', 8.0, n_freq=2, method='inversion')
+    stem = str(tmp_path / 'na')
+    with _ctx() as ctx:
+        with Solver(p, ctx=ctx) as sv:
+            out = O.solve_spectrum(sv, stem, save_freq=True, save_info=True)
+            info, sols = A.read_archive(out['paths']['tar'])
+            assert info['n_atoms'] == p.n_atoms and len(sols) == 2
+            label = sorted(sols)[0]
+            g = A.cubic_grid(info['coord_ang'], (12, 10, 8), 5.0)
+            direct = A.field_on_grid(sv, sols[label][2]['x'], 0, g, p.e0)
+        q = A.problem_from_info(info)
+        with Solver(q, ctx=ctx, store_t=False) as sv2:
+            grid, files = A.write_cubes(stem + '.tar.gz', sv2, info, sols[label], pols=('x',), n=(12, 10, 8),
+                                        offset=5.0)
+            again = A.field_on_grid(sv2, sols[label][2]['x'], 0, grid, info['e0'])
+    assert np.allclose(again, direct, rtol=1e-12, atol=0)
+    assert [os.path.basename(f) for f in files] == ['na-Ex-%s.cube' % label]
+    with open(files[0]) as f:
+        text = f.read().splitlines()
+    assert text[0] == 'Generated by plasmonX analysis' and int(text[2].split()[0]) == p.n_atoms
