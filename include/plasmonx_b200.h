@@ -173,6 +173,16 @@ plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *desc, plx_geom **out
  * complex (either may be NULL).  Atomistic models only. */
 plx_status plx_field_at_points(plx_geom *geom, int32_t i_pol, const double *x, int32_t n_points,
                                const double *points, double *field_out, double *density_out);
+/* BEM field at points for the analysis step (calculate_induced_field_at_point_bem,
+ * src/bem/bem_module.f90:1152-1222): the tesserae as point charges q (complex
+ * n_tess, the area-weighted charges a run's .freq file holds) at their centres
+ * (3 x n_tess, bohr); a point whose distance to the centres' mean exceeds its
+ * nearest tessera's by more than 0.5 Angstrom sees E0 along i_pol plus the
+ * charges' field, any other point zero.  points: 3 x n_points, bohr;
+ * field_out: 3 x n_points complex.  Needs no geometry (the analysis of a run's
+ * archive has the centres and charges only). */
+plx_status plx_bem_field_at_points(plx_ctx *ctx, int32_t n_tess, const double *centres, const double *q, double e0,
+                                   int32_t i_pol, int32_t n_points, const double *points, double *field_out);
 /* get_neighbours (src/target/target_module.f90:417-464) on the device: per atom
  * the number of atoms within the nearest-neighbour distance r0 of the pair
  * (counting the atom itself) and the per-type counts the wFQFMu dipole diagonal

@@ -49,3 +49,25 @@ def field_and_density(coord, rq, rmu, x, e0, i_pol, points, fmu):
         g = np.exp(-r2 / (Rm * Rm)) / (math.pi ** 1.5 * Rm ** 3)
         dens -= np.einsum('pn,pn->p', 2.0 * g / (Rm * Rm), np.einsum('pnk,nk->pn', d, mu))
     return E, dens
+
+
+def bem_field(centres, q, e0, i_pol, points):
+    """calculate_induced_field_at_point_bem (src/bem/bem_module.f90:1152-1222) with
+    calculate_induced_field_q_bem (src/matrix/matrix_module.f90:1444-1464): centres
+    (n, 3) and points (P, 3) in bohr, q the (area-weighted) complex charges.  A point
+    is outside when it lies farther from the centre of mass (mean of the centres)
+    than its nearest tessera plus 0.5 Angstrom; inside, the field is zero; outside,
+    E0 along i_pol minus sum q d / |d|^3 (d = centre - point, |d| > 0.1 bohr)."""
+    com = centres.mean(axis=0)
+    out = np.zeros((points.shape[0], 3), dtype=np.complex128)
+    margin = 0.5 * 1.8897261254578281
+    for p, pt in enumerate(points):
+        d = centres - pt[None, :]
+        r = np.sqrt((d ** 2).sum(axis=1))
+        l = int(np.argmin(r))                    # the first nearest tessera
+        if np.sqrt(((pt - com) ** 2).sum()) <= np.sqrt(((centres[l] - com) ** 2).sum()) + margin:
+            continue
+        out[p, i_pol] = e0
+        far = r > 1.0e-1
+        out[p] -= ((d[far] * (q[far] / r[far] ** 3)[:, None])).sum(axis=0)
+    return out

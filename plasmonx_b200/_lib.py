@@ -22,7 +22,8 @@ EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes
            'plx_set_frequencies', 'plx_matvec', 'plx_rhs', 'plx_gmres_solver', 'plx_complex_inversion',
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
            'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points',
-           'plx_static_n_var', 'plx_static_solve', 'plx_principal_axes', 'plx_neighbour_counts']
+           'plx_static_n_var', 'plx_static_solve', 'plx_principal_axes', 'plx_neighbour_counts',
+           'plx_bem_field_at_points']
 STATIC_FF = {'fq': 0, 'fqfmu': 1}
 KERNEL = {'coulomb': 0, 'ohno': 1, 'gaussian': 2}
 STATIC_WHAT = {'energy': 0, 'static': 1}
@@ -106,6 +107,7 @@ def load():
     lib.plx_contract_noalloc.argtypes = [vp, C.c_int32, C.c_void_p, C.c_void_p]
     lib.plx_field_at_points.argtypes = [vp, C.c_int32, _dp, C.c_int32, _dp, _dp, _dp]
     lib.plx_neighbour_counts.argtypes = [vp, C.c_int32, C.c_int32, _dp, _ip, _ip, _dp, _ip, _ip]
+    lib.plx_bem_field_at_points.argtypes = [vp, C.c_int32, _dp, _dp, C.c_double, C.c_int32, C.c_int32, _dp, _dp]
     lib.plx_static_n_var.restype = C.c_int64
     lib.plx_static_n_var.argtypes = [C.POINTER(StaticDesc)]
     lib.plx_static_solve.argtypes = [vp, C.POINTER(StaticDesc), C.c_int32, _dp, _dp, _dp]

@@ -102,6 +102,22 @@ def field_on_grid(solver, x, i_pol, grid, e0, third=0.0):
     return v.reshape(nz, ny, nx).transpose(2, 1, 0)
 
 
+def bem_field_on_grid(ctx, centres_ang, q, e0, i_pol, grid, third=0.0):
+    """|E| / E0 of a BEM solution on the grid: the tessera charges q (area-weighted,
+    as a .freq file holds them) at their centres, zero inside the surface
+    (plx_bem_field_at_points)."""
+    from . import _lib
+    c = np.ascontiguousarray(np.asarray(centres_ang, dtype=np.float64) * M.TO_BOHR)
+    qq = np.ascontiguousarray(q, dtype=np.complex128)
+    pts = np.ascontiguousarray(_points_bohr(grid, third))
+    E = np.zeros((pts.shape[0], 3), dtype=np.complex128)
+    ctx.check(ctx.lib.plx_bem_field_at_points(ctx.h, len(c), _lib.ptr(c), _lib.ptr(qq.view(np.float64)), float(e0),
+                                              int(i_pol), pts.shape[0], _lib.ptr(pts), _lib.ptr(E.view(np.float64))))
+    v = np.sqrt((E.real ** 2 + E.imag ** 2).sum(axis=1)) / e0
+    nx, ny, nz = grid.shape()
+    return v.reshape(nz, ny, nx).transpose(2, 1, 0)
+
+
 def density_on_grid(solver, x, grid, third=0.0):
     """The plasmon density (complex) on the grid (nx, ny, nz)."""
     _, rho = solver.field_at_points(0, x, _points_bohr(grid, third))
@@ -206,19 +222,28 @@ def cube_path(root, pol_name, freq_label, suffix=''):
 def write_cubes(path, solver, info, solution, pols=('x', 'y', 'z'), what='field', n=(30, 30, 30), offset=10.0,
                 root=None):
     """Cube files of one frequency's solutions (a read_freq triple) for the given
-    polarisations: |E|/E0 (what='field') or the density's real and imaginary parts."""
+    polarisations: |E|/E0 (what='field') or the density's real and imaginary parts.
+    `solver` is a Solver of the run's geometry for atomistic runs, a Context for BEM
+    runs (field only, as in the reference)."""
     variable, ev, blocks = solution
     label = O.fortran_f(ev, 12, 10).strip()
     if root is None:
         root = path[:-len('.tar.gz')] if path.endswith('.tar.gz') else os.path.splitext(path)[0]
-    grid = cubic_grid(info['coord_ang'], n, offset)
+    bem = info['model'] == 'bem'
+    if bem and what != 'field':
+        raise ValueError('Density plot not allowed for BEM')
+    pos = info['centres_ang'] if bem else info['coord_ang']
+    grid = cubic_grid(pos, n, offset)
     written = []
     for p in pols:
         if p not in blocks:
             continue
         i_pol = 'xyz'.index(p)
         pol_name = 'E' + p
-        if what == 'field':
+        if bem:
+            v = bem_field_on_grid(solver, info['centres_ang'], blocks[p], info['e0'], i_pol, grid)
+            outs = [(cube_path(root, pol_name, label), v)]
+        elif what == 'field':
             v = field_on_grid(solver, blocks[p], i_pol, grid, info['e0'])
             outs = [(cube_path(root, pol_name, label), v)]
         else:
@@ -227,6 +252,6 @@ def write_cubes(path, solver, info, solution, pols=('x', 'y', 'z'), what='field'
                     (cube_path(root, pol_name, label, '-densityIm'), rho.imag)]
         for fn, v in outs:
             with open(fn, 'w') as f:
-                f.write(cube_text(grid, v, info['z'], info['coord_ang']))
+                f.write(cube_text(grid, v, centres_ang=pos) if bem else cube_text(grid, v, info['z'], pos))
             written.append(fn)
     return grid, written

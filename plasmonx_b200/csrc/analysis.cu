@@ -10,6 +10,8 @@
 //       - sum_i 2 exp(-r^2/Rmu^2) / (pi^3/2 Rmu^5) (mu_i . d)
 // One thread per point; the atoms (position, widths, charge, dipole) are
 // staged through shared memory in tiles.
+#include <vector>
+
 #include "pair_tiles.cuh"
 #include "plx_internal.h"
 
@@ -99,7 +101,88 @@ __global__ void __launch_bounds__(kPts) field_points(int N, int nv, int fmu, int
     if (dens) dens[p] = make_double2(dr, di);
 }
 
+// BEM field at points (calculate_induced_field_at_point_bem,
+// src/bem/bem_module.f90:1152-1222, with calculate_induced_field_q_bem,
+// src/matrix/matrix_module.f90:1444-1464): the point's first nearest tessera l
+// decides inside / outside -- outside when |p - com| > |c_l - com| + 0.5 A,
+// com the mean of the centres; inside, the field is zero; outside,
+// E = E0 e_pol - sum_i q_i d_i / |d_i|^3 over |d_i| > 0.1 bohr, d_i = c_i - p.
+// One thread per point; the centres and charges are read through the cache.
+__global__ void __launch_bounds__(kPts) bem_field_points(int n, int P, int pol, double e0, double margin,
+                                                         double cx, double cy, double cz,
+                                                         const double *__restrict__ c /*[3][n]*/,
+                                                         const double2 *__restrict__ q,
+                                                         const double *__restrict__ pts /*[3][P]*/,
+                                                         double2 *__restrict__ field) {
+    const int p = blockIdx.x * kPts + threadIdx.x;
+    if (p >= P) return;
+    const double px = pts[p], py = pts[P + p], pz = pts[2 * P + p];
+    double lowest = 1.0e6;
+    int l = 0;
+    for (int i = 0; i < n; ++i) {
+        const double dx = c[i] - px, dy = c[n + i] - py, dz = c[2 * n + i] - pz;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        if (lowest > r) {
+            lowest = r;
+            l = i;
+        }
+    }
+    const double ex = c[l] - cx, ey = c[n + l] - cy, ez = c[2 * n + l] - cz;
+    const double gx = px - cx, gy = py - cy, gz = pz - cz;
+    double er[3] = {0.0, 0.0, 0.0}, ei[3] = {0.0, 0.0, 0.0};
+    if (sqrt(gx * gx + gy * gy + gz * gz) > sqrt(ex * ex + ey * ey + ez * ez) + margin) {
+        er[pol] = e0;
+        for (int i = 0; i < n; ++i) {
+            const double d[3] = {c[i] - px, c[n + i] - py, c[2 * n + i] - pz};
+            const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (r > 1.0e-1) {
+                const double r3 = r * (r * r);
+                const double2 qi = q[i];
+                for (int k = 0; k < 3; ++k) {
+                    er[k] -= d[k] * qi.x / r3;
+                    ei[k] -= d[k] * qi.y / r3;
+                }
+            }
+        }
+    }
+    for (int k = 0; k < 3; ++k) field[3LL * p + k] = make_double2(er[k], ei[k]);
+}
+
 }  // namespace
+
+void bem_field_at_points(plx_ctx *ctx, int n, const double *centres, const double *q, double e0, int pol, int P,
+                         const double *points, double *field_out) {
+    if (n < 1 || P < 0 || !centres || !q || !points || !field_out)
+        throw Error(PLX_ERR_ARG, "BEM field at points: empty surface or null array");
+    if (pol < 0 || pol > 2) throw Error(PLX_ERR_ARG, "polarisation index must be 0, 1 or 2");
+    if (P == 0) return;
+    std::vector<double> c(3 * (size_t)n), pts(3 * (size_t)P);
+    double com[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            c[(size_t)k * n + i] = centres[3 * (size_t)i + k];
+            com[k] += centres[3 * (size_t)i + k] / n;
+        }
+    for (int i = 0; i < P; ++i)
+        for (int k = 0; k < 3; ++k) pts[(size_t)k * P + i] = points[3 * (size_t)i + k];
+    cudaStream_t st = ctx->stream;
+    DevArray<double> d_c, d_q, d_p, d_f;
+    d_c.alloc(ctx, c.size());
+    d_q.alloc(ctx, 2 * (size_t)n);
+    d_p.alloc(ctx, pts.size());
+    d_f.alloc(ctx, 6 * (size_t)P);
+    PLX_CHECK_CUDA(cudaMemcpyAsync(d_c.p, c.data(), c.size() * 8, cudaMemcpyHostToDevice, st));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(d_q.p, q, 2 * (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(d_p.p, pts.data(), pts.size() * 8, cudaMemcpyHostToDevice, st));
+    const double margin = 0.5 * 1.8897261254578281;   // 0.5 Angstrom in bohr
+    bem_field_points<<<n_blocks(P, kPts), kPts, 0, st>>>(n, P, pol, e0, margin, com[0], com[1], com[2], d_c.p,
+                                                         reinterpret_cast<const double2 *>(d_q.p), d_p.p,
+                                                         reinterpret_cast<double2 *>(d_f.p));
+    ctx->launches++;
+    PLX_CHECK_CUDA(cudaGetLastError());
+    PLX_CHECK_CUDA(cudaMemcpyAsync(field_out, d_f.p, 6 * (size_t)P * 8, cudaMemcpyDeviceToHost, st));
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+}
 
 void field_at_points(plx_geom *g, int pol, const double *d_x, int P, const double *d_pts, double *d_field,
                      double *d_dens) {

@@ -339,6 +339,15 @@ plx_status plx_field_at_points(plx_geom *g, int32_t i_pol, const double *x, int3
     });
 }
 
+plx_status plx_bem_field_at_points(plx_ctx *ctx, int32_t n_tess, const double *centres, const double *q, double e0,
+                                   int32_t i_pol, int32_t n_points, const double *points, double *field_out) {
+    if (!ctx) return PLX_ERR_ARG;
+    return guarded(ctx, [&] {
+        set_device(ctx);
+        bem_field_at_points(ctx, n_tess, centres, q, e0, i_pol, n_points, points, field_out);
+    });
+}
+
 plx_status plx_neighbour_counts(plx_ctx *ctx, int32_t n_atoms, int32_t n_types, const double *coord_ang,
                                 const int32_t *atom_type, const int32_t *type_z, const double *r0,
                                 int32_t *neighbours_out, int32_t *n_neighbours_out) {

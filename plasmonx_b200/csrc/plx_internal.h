@@ -279,6 +279,9 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
 void field_at_points(plx_geom *g, int pol, const double *d_x, int P, const double *d_pts, double *d_field,
                      double *d_dens);
 
+void bem_field_at_points(plx_ctx *ctx, int n, const double *centres, const double *q, double e0, int pol, int P,
+                         const double *points, double *field_out);
+
 // neighbours.cu: neighbour counts per atom (cell list on the device)
 void neighbour_counts(plx_ctx *ctx, int n, int nt, const double *coord_ang, const int32_t *atom_type,
                       const int32_t *type_z, const double *r0, int32_t *nb_out, int32_t *n_nb_out);

@@ -238,6 +238,7 @@ ANALYSIS = {
     'analysis_field_3d_x_wfq_sodium': ('-Ex-1.5800000000.cube', 'field', 0, '1.5800000000'),
     'analysis_field_3d_x_y_z_wfqfmu_ag': ('-Ez-3.0000000000.cube', 'field', 2, '3.0000000000'),
     'analysis_density_3d_x_wfq_sodium': ('-Ex-1.5800000000-densityRe.cube', 'density_re', 0, '1.5800000000'),
+    'analysis_field_3d_y_bem': ('-Ey-1.9100000000.cube', 'field', 1, '1.9100000000'),
 }
 
 
@@ -254,16 +255,23 @@ def one_analysis(name, ref, stride=5):
             info = f.read().splitlines()
         with open(os.path.join(work, '%s-%s.freq' % (name, flabel))) as f:
             freq = f.read().splitlines()
-    n_atoms = int(info[0].split(':')[1])
     model = info[5].split(':')[1].strip()
     e0 = float(info[7].split(':')[1])
     g0 = info.index('Input Geometry (angstrom)') + 1
-    coords = [[float(v) for v in l.split()[2:5]] for l in info[g0:g0 + n_atoms]]
-    zs = [int(float(l.split()[0])) for l in info[g0:g0 + n_atoms]]
-    p0 = next(i for i, l in enumerate(info) if l.startswith('Parameters:'))
-    par = [float(v) for v in info[p0 + 2].split()[1:]]
-    rq = par[2] if model == 'wfq' else par[3]
-    rmu = par[4] if model == 'wfqfmu' else 0.0
+    if model == 'bem':
+        # tessera centres (i8, 3 f25.16); the cube lists them as atoms 0
+        n_atoms = int(info[2].split(':')[1])
+        coords = [[float(v) for v in l.split()[1:4]] for l in info[g0:g0 + n_atoms]]
+        zs = [0] * n_atoms
+        rq = rmu = 0.0
+    else:
+        n_atoms = int(info[0].split(':')[1])
+        coords = [[float(v) for v in l.split()[2:5]] for l in info[g0:g0 + n_atoms]]
+        zs = [int(float(l.split()[0])) for l in info[g0:g0 + n_atoms]]
+        p0 = next(i for i, l in enumerate(info) if l.startswith('Parameters:'))
+        par = [float(v) for v in info[p0 + 2].split()[1:]]
+        rq = par[2] if model == 'wfq' else par[3]
+        rmu = par[4] if model == 'wfqfmu' else 0.0
     heads = [i for i, l in enumerate(freq) if l.startswith('complex')]
     rows = freq[heads[pol] + 1:(heads[pol + 1] if pol + 1 < len(heads) else len(freq))]
     x = [[float(l.split()[1]), float(l.split()[2])] for l in rows if l.strip()]

@@ -60,7 +60,10 @@ def _grid(a):
     return A.cubic_grid(np.array(a['coords_ang']), tuple(a['n']), a['offset_ang'])
 
 
-@pytest.mark.parametrize('name', NAMES)
+ALL = NAMES + ['analysis_field_3d_y_bem']
+
+
+@pytest.mark.parametrize('name', ALL)
 def test_grid_block_matches_reference_log(name):
     with open(os.path.join(GOLDEN, name, 'analysis.json')) as f:
         a = json.load(f)
@@ -68,7 +71,7 @@ def test_grid_block_matches_reference_log(name):
     assert [l.rstrip() for l in mine] == [l.rstrip() for l in a['log_grid']]
 
 
-@pytest.mark.parametrize('name', NAMES)
+@pytest.mark.parametrize('name', ALL)
 def test_cube_header_matches_reference(name):
     """Origin, steps and atoms of the cube header: the same numbers as printed (the
     reference's archived cubes come from a release that wrote the counts as i5; the
@@ -114,3 +117,33 @@ def test_maximum_lines_match_reference_log(name):
             ijk = np.rint((at - g.lo) / g.step).astype(int)
             m, _ = A.maximum(g, vals)
             assert abs(vals[tuple(ijk)] - m) <= 1e-12 * abs(m)
+
+
+def _bem_case():
+    with open(os.path.join(GOLDEN, 'analysis_field_3d_y_bem', 'analysis.json')) as f:
+        a = json.load(f)
+    centres = np.array(a['coords_ang']) * TO_BOHR
+    q = np.array(a['x'])[:, 0] + 1j * np.array(a['x'])[:, 1]
+    return a, centres, q
+
+
+def test_oracle_reproduces_reference_bem_cube_and_maximum():
+    """BEM field |E|/E0 (point charges at the tessera centres, zero inside the
+    surface) against the reference's BEM analysis test: the sampled cube values at
+    E14.6 and the maximum line of its log."""
+    from oracle.analysis import bem_field
+    from plasmonx_b200 import analysis as A
+    a, centres, q = _bem_case()
+    g = _grid(a)
+    pts = g.points_ang() * TO_BOHR
+    E = bem_field(centres, q, a['e0'], a['pol'], pts)
+    v = np.sqrt((np.abs(E) ** 2).sum(axis=1)) / a['e0']
+    nx, ny, nz = a['n']
+    vals = v.reshape(nz, ny, nx).transpose(2, 1, 0)
+    flat = vals.ravel()                 # cube order: x outer, z fastest
+    idx = np.array(a['sample_index'])
+    ref = np.array(a['sample_value'])
+    assert np.all(np.abs(flat[idx] - ref) <= 5.01e-6 * np.abs(ref) + 1e-30)
+    assert np.mean(ref == 0.0) > 0.01           # the inside of the surface is zero
+    lines = A.maximum_lines('Field', 'Ey', g, vals).splitlines()
+    assert lines == a['log_max']

@@ -121,3 +121,30 @@ def test_analysis_from_a_run_archive(tmp_path):
     with open(files[0]) as f:
         text = f.read().splitlines()
     assert text[0] == 'Generated by plasmonX analysis' and int(text[2].split()[0]) == p.n_atoms
+
+
+def test_bem_field_on_device_reproduces_reference_analysis(tmp_path):
+    """The BEM field kernel over the whole 30^3 grid against the oracle (1e-12) and the
+    reference's BEM analysis test (cube samples at E14.6, maximum line)."""
+    from oracle.analysis import bem_field
+    from plasmonx_b200 import analysis as A
+    from tests.test_analysis_golden import TO_BOHR, _bem_case, _grid
+    a, centres, q = _bem_case()
+    g = _grid(a)
+    with _ctx() as ctx:
+        vals = A.bem_field_on_grid(ctx, np.array(a['coords_ang']), q, a['e0'], a['pol'], g)
+        pts = g.points_ang()[::37] * TO_BOHR
+        import ctypes as C  # noqa: F401
+        from plasmonx_b200 import _lib
+        c = np.ascontiguousarray(np.array(a['coords_ang']) * TO_BOHR)
+        E = np.zeros((len(pts), 3), dtype=np.complex128)
+        pts = np.ascontiguousarray(pts)
+        ctx.check(ctx.lib.plx_bem_field_at_points(ctx.h, len(c), _lib.ptr(c), _lib.ptr(q.view(np.float64)),
+                                                  a['e0'], a['pol'], len(pts), _lib.ptr(pts),
+                                                  _lib.ptr(E.view(np.float64))))
+    Er = bem_field(centres, q, a['e0'], a['pol'], pts)
+    assert np.linalg.norm(E - Er) <= 1e-12 * np.linalg.norm(Er)
+    flat = vals.ravel()
+    ref = np.array(a['sample_value'])
+    assert np.all(np.abs(flat[np.array(a['sample_index'])] - ref) <= 5.01e-6 * np.abs(ref) + 1e-30)
+    assert A.maximum_lines('Field', 'Ey', g, vals).splitlines() == a['log_max']
