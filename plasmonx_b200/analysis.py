@@ -13,13 +13,16 @@ grid around the particle and writes |E|/E0 or the plasmon density on it:
     field over its six real components, divided by E0;
   * files: the cube file (write_cube_file, plot_module.f90:496-562: origin and
     steps in bohr, atoms as atomic number, 0.0 and bohr coordinates, values
-    E14.6 six per line with z fastest) and the maximum's log lines
-    (print_quantity_analysis_3d, plot_module.f90:620-669: the first maximum
-    in Fortran order, x fastest).
+    E14.6 six per line with z fastest), the binary .plt (write_plt_file,
+    :452-490), the plane .csv (write_csv_file, :568-611), the maximum's log
+    lines (print_quantity_analysis_3d, :620-669: the first maximum in Fortran
+    order, x fastest) and the effective volume and area of a slab
+    (print_effective_volume_area, :680-735).
 Grid arrays here are indexed [i, j, k] = [x, y, z].
 """
 import os
 import tarfile
+from fractions import Fraction
 
 import numpy as np
 
@@ -38,7 +41,14 @@ class Grid:
                               for k in range(3)])
 
     def axes(self):
-        return [self.lo[k] + np.arange(max(self.n[k], 1)) * self.step[k] for k in range(3)]
+        """Coordinates along each axis, lo + i * step rounded once (as a fused
+        multiply-add): the reference's build contracts min_coord + (i-1)*step this
+        way, which its plane .csv files show in their last printed digit."""
+        out = []
+        for k in range(3):
+            lo, st = Fraction(float(self.lo[k])), Fraction(float(self.step[k]))
+            out.append(np.array([float(lo + i * st) for i in range(max(self.n[k], 1))]))
+        return out
 
     def points_ang(self):
         """(nx * ny * nz, 3) points, x fastest (the reference's loop order)."""
@@ -125,6 +135,64 @@ def density_on_grid(solver, x, grid, third=0.0):
     return rho.reshape(nz, ny, nx).transpose(2, 1, 0)
 
 
+def on_plane(grid, values):
+    """A plane grid's (n1, n2) array from a (nx, ny, nz) array with one fixed axis."""
+    fixed = {'xy': 2, 'xz': 1, 'yz': 0}[grid.plane]
+    return np.take(values, 0, axis=fixed)
+
+
+def plane_csv_text(grid, values):
+    """write_csv_file (plot_module.f90:568-611): one line per point, x and y the two
+    in-plane coordinates (Angstrom) and the value, E25.16 each followed by three
+    blanks; a blank line after each row of the first in-plane axis."""
+    i1, i2 = {'xy': (0, 1), 'xz': (0, 2), 'yz': (1, 2)}[grid.plane]
+    v = np.asarray(values, dtype=np.float64)
+    n1, n2 = v.shape
+    ax = grid.axes()
+    L = []
+    for i in range(n1):
+        x = ax[i1][i]
+        for j in range(n2):
+            y = ax[i2][j]
+            q = v[i, j] if abs(v[i, j]) > 1.0e-99 else 0.0
+            L.append(''.join(O.fortran_e(t, 25, 16) + '   ' for t in (x, y, q)))
+        L.append('')
+    return '\n'.join(L) + '\n'
+
+
+def plt_bytes(grid, values):
+    """write_plt_file (plot_module.f90:452-490): one unformatted record of int32 3,
+    200, nz, ny, nx, float32 z, y and x bounds, then the values as float32 with x
+    fastest."""
+    import struct
+    v = np.asarray(values, dtype=np.float64)
+    nx, ny, nz = v.shape
+    head = struct.pack('<5i', 3, 200, nz, ny, nx)
+    head += np.array([grid.lo[2], grid.hi[2], grid.lo[1], grid.hi[1], grid.lo[0], grid.hi[0]],
+                     dtype='<f4').tobytes()
+    return head + v.transpose(2, 1, 0).astype('<f4').tobytes()
+
+
+def effective_volume_lines(pol_name, grid, values):
+    """print_effective_volume_area (plot_module.f90:680-735) for |E|/E0 on a slab:
+    V = sum(|E|^2) dx dy dz / max(|E|)^2 and A = V / (the slab's smallest extent)."""
+    v = np.asarray(values, dtype=np.float64)
+    integral = float((v ** 2).sum()) * grid.step[0] * grid.step[1] * grid.step[2]
+    peak = float(v.max()) ** 2
+    ext = grid.hi - grid.lo
+    k = int(np.argmin(ext))
+    if not all(ext[k] < ext[o] for o in range(3) if o != k):
+        raise ValueError('The provided grid cannot be used for effective volume or area calculations')
+    if ext[k] < 1.0e-14:
+        raise ValueError('The minimum distance in the grid is zero')
+    vol = integral / peak
+    area = vol / ext[k]
+    return (' Calculation of effective volume and area for polarization: %s\n' % pol_name +
+            ' The slice has minimum distance in %s direction: %s Angstrom.\n' % ('XYZ'[k], O.fortran_f(ext[k], 6, 3)) +
+            '\n Effective Volume : %s nm^3\n' % O.fortran_f(vol / 10 ** 3, 15, 5) +
+            ' Effective Area   : %s nm^2\n' % O.fortran_f(area / 10 ** 2, 15, 5))
+
+
 def cube_text(grid, values, z=None, coord_ang=None, centres_ang=None, title='Generated by plasmonX analysis'):
     """write_cube_file: atoms (z, coord_ang) or, for BEM, tessera centres."""
     vals = np.asarray(values, dtype=np.float64)
@@ -156,7 +224,8 @@ def maximum(grid, values):
     idx = int(np.argmax(flat))
     nx, ny, _ = v.shape
     i, j, k = idx % nx, (idx // nx) % ny, idx // (nx * ny)
-    return float(flat[idx]), grid.lo + np.array([i, j, k]) * grid.step
+    ax = grid.axes()
+    return float(flat[idx]), np.array([ax[0][i], ax[1][j], ax[2][k]])
 
 
 def maximum_lines(kind, pol_name, grid, values):
