@@ -117,7 +117,17 @@ def test_solve_matches_oracle(ctx, name):
     scale = np.abs(ref['results']).max(axis=0) + 1e-300
     err = np.abs(out['results'] - ref['results']) / scale
     if method == 'inversion':
-        assert err.max() < 1e-10
+        # two FP64 LU solves of the same A(w) agree to ~cond(A) eps in the solution
+        # (held to 50 eps cond per frequency); a result column that is small at some
+        # frequencies (Im alpha of graphene at its lowest frequency, cond 1.4e4)
+        # carries that error relative to the whole solution, so the results are held
+        # to 1e-9 of their column scale
+        x, xr = out['x'], np.asarray(ref['x'])
+        dx = np.linalg.norm((x - xr).reshape(len(x), -1), axis=1) / np.linalg.norm(xr.reshape(len(x), -1), axis=1)
+        op = model.Operator(s)
+        cond = np.array([np.linalg.cond(op.matrix(i)) for i in range(len(x))])
+        assert np.all(dx <= 50 * 2.22e-16 * cond)
+        assert err.max() < 1e-9
     else:
         # same algorithm at the same (loose) tolerance; differences are round-off
         # amplified by the Krylov recurrence, bounded by the tolerance itself.
