@@ -63,8 +63,8 @@ class Grid:
         """Grid Information block of the analysis log (print_grid_3d_info, grid_module.f90:159-192)."""
         s = O.STICKS
         L = [' ' * 27 + 'Grid Information (Angstrom)', s,
-             ' ' * 10 + ''.join('%s%s  ' % (lab, O.fortran_f(v, 12, 4)) for lab, v in
-                                zip(('StepX: ', 'StepY: ', 'StepZ: '), self.step)), s]
+             (' ' * 10 + ''.join('%s%s  ' % (lab, O.fortran_f(v, 12, 4)) for lab, v in
+                                 zip(('StepX: ', 'StepY: ', 'StepZ: '), self.step))).rstrip(), s]
         for k, ax in enumerate('XYZ'):
             L += [' ' * 10 + '%sminGrid:%s  %smaxGrid:%s  %s NPoints:%7d' % (
                 ax, O.fortran_f(self.lo[k], 10, 4), ax, O.fortran_f(self.hi[k], 10, 4), ax, self.n[k]), s]
@@ -143,8 +143,8 @@ def on_plane(grid, values):
 
 def plane_csv_text(grid, values):
     """write_csv_file (plot_module.f90:568-611): one line per point, x and y the two
-    in-plane coordinates (Angstrom) and the value, E25.16 each followed by three
-    blanks; a blank line after each row of the first in-plane axis."""
+    in-plane coordinates (Angstrom) and the value, E25.16 each, three blanks apart;
+    a blank line after each row of the first in-plane axis."""
     i1, i2 = {'xy': (0, 1), 'xz': (0, 2), 'yz': (1, 2)}[grid.plane]
     v = np.asarray(values, dtype=np.float64)
     n1, n2 = v.shape
@@ -155,7 +155,7 @@ def plane_csv_text(grid, values):
         for j in range(n2):
             y = ax[i2][j]
             q = v[i, j] if abs(v[i, j]) > 1.0e-99 else 0.0
-            L.append(''.join(O.fortran_e(t, 25, 16) + '   ' for t in (x, y, q)))
+            L.append('   '.join(O.fortran_e(t, 25, 16) for t in (x, y, q)))   # trailing 3x writes nothing
         L.append('')
     return '\n'.join(L) + '\n'
 
@@ -234,6 +234,61 @@ def maximum_lines(kind, pol_name, grid, values):
     return ('  %s%sX%sY%sZ%sMax.\n' % (kind, ' ' * 11, ' ' * 16, ' ' * 16, ' ' * 13) +
             '   %s  %s   %s\n' % (pol_name, ''.join(O.fortran_f(c, 15, 5) + '  ' for c in at),
                                  O.fortran_e(m, 13, 6)))
+
+
+# van der Waals radii (Angstrom) the .pqr files carry (assign_atomic_radius,
+# src/target/target_module.f90:581-632); 0 for elements without one
+VDW_RADIUS = {'H': 1.20, 'He': 1.40, 'Li': 1.82, 'Be': 1.53, 'B': 1.92, 'C': 1.70, 'N': 1.55, 'O': 1.52,
+              'F': 1.47, 'Ne': 1.54, 'Na': 2.27, 'Mg': 1.73, 'Al': 1.84, 'Si': 2.10, 'P': 1.80, 'S': 1.80,
+              'Cl': 1.75, 'Ar': 1.88, 'Ag': 1.72, 'Au': 1.66}
+
+
+def element_symbol(z):
+    """assign_atom_name (src/target/target_module.f90:524-575): the element symbol
+    of an atomic number the reference knows, '' otherwise."""
+    for name, num in M.ELEMENTS.items():
+        if num == int(z):
+            return name.capitalize()
+    return ''
+
+
+def pqr_line(k, name, xyz_ang, value, radius, bem=False):
+    """One line of write_pqr_file (plot_module.f90:401-446)."""
+    f8 = ''.join(O.fortran_f(v, 8, 3) for v in xyz_ang)
+    if bem:
+        return 'ATOM   %4d   X  DUM     1    %s%s %s' % (k, f8, O.fortran_e(value, 11, 3), O.fortran_f(1.0, 5, 3))
+    return 'ATOM   %4d  %s    X     1    %s%s %s' % (k, _a(name, 2) if len(name) < 2 else name[:2], f8,
+                                                 O.fortran_e(value, 11, 3), O.fortran_f(radius, 5, 3))
+
+
+def _a(v, w):
+    return str(v).rjust(w)[:w]
+
+
+def pqr_text(info, values):
+    """A .pqr file of one polarisation's real or imaginary charges (values, n_var)."""
+    bem = info['model'] == 'bem'
+    if not bem and info['forcefield'] == 'fqfmu':
+        raise ValueError('PQR not implemented for FQFMu')
+    pos = info['centres_ang'] if bem else info['coord_ang']
+    L = []
+    for k in range(len(pos)):
+        name = '' if bem else element_symbol(info['z'][k])
+        L.append(pqr_line(k + 1, name, pos[k], values[k], VDW_RADIUS.get(name, 0.0), bem))
+    return '\n'.join(L) + '\n'
+
+
+def xyz_text(info):
+    """plot_xyz (plot_module.f90:20-67): the count, a blank line, then element (or X
+    for tesserae) and the Angstrom coordinates, f25.16."""
+    bem = info['model'] == 'bem'
+    pos = info['centres_ang'] if bem else info['coord_ang']
+    L = [str(len(pos)).ljust(10), '']       # adjustl of an i10 field
+    for k in range(len(pos)):
+        name = 'X ' if bem else element_symbol(info['z'][k]).ljust(2)
+        # (a2,2x,3(f25.16,1x)): the trailing 1x writes nothing
+        L.append(name + '  ' + ' '.join(O.fortran_f(v, 25, 16) for v in pos[k]))
+    return '\n'.join(L) + '\n'
 
 
 def read_archive(path):

@@ -33,6 +33,7 @@ Numbers are formatted as Fortran's E and F edit descriptors print them
 (``fortran_e``: ``0.ddddddE+xx``, the leading zero dropped when the width is
 exhausted by a sign, as gfortran does).
 """
+import math
 import os
 
 import numpy as np
@@ -62,7 +63,8 @@ def fortran_e(x, w, d):
     """Fortran Ew.d: 0.<d digits>E<sign><2 digits>, right-justified in w columns."""
     x = float(x)
     if x == 0.0:
-        body = '0.' + '0' * d + 'E+00'
+        # gfortran keeps the sign of a negative zero
+        body = ('-' if math.copysign(1.0, x) < 0 else '') + '0.' + '0' * d + 'E+00'
     else:
         mant, ex = ('%.*e' % (d - 1, abs(x))).split('e')
         e = int(ex) + 1
@@ -147,8 +149,9 @@ def freq_text(w_au, x, variable='Charges', weights=None):
     for c, lab in enumerate('xyz'):
         lines.append('complex %s: %s. freq = %s' % (variable, lab, fortran_f(ev, 25, 16)))
         for i in range(x.shape[0]):
-            lines.append('%8d     %s   %s   ' % (i + 1, fortran_f(x[i, c].real * wts[i], 25, 16),
-                                               fortran_f(x[i, c].imag * wts[i], 25, 16)))
+            # (i8,5x,2(f25.16,3x)): a trailing 3x writes nothing at the end of a record
+            lines.append('%8d     %s   %s' % (i + 1, fortran_f(x[i, c].real * wts[i], 25, 16),
+                                             fortran_f(x[i, c].imag * wts[i], 25, 16)))
     return '\n'.join(lines) + '\n'
 
 

@@ -22,7 +22,8 @@ With ``--analysis`` it instead stores, for three analysis tests of the
 reference, the inputs of the field / density step and a sample of the cube
 file the reference wrote (``<name>/analysis.json``).  With ``--analysis-extra`` it stores, for four more analysis tests (a plane
 of |E|/E0, planes of the density, an effective volume, the binary .plt
-format), their inputs and sampled outputs in ``analysis_extra/``.  With
+format), their inputs and sampled outputs in ``analysis_extra/``; with
+``--pqr-xyz`` sampled lines of its .pqr and .xyz outputs.  With
 ``--info`` it copies three
 ``.info`` files and one ``.freq`` file out of the reference's analysis-test
 tarballs into ``info/`` (the files its analysis tool reads).  With ``--static`` it
@@ -506,7 +507,51 @@ def one_analysis_extra(name, ref, stride=7):
     print('analysis_extra/' + name, kind)
 
 
+def pqr_xyz(ref, stride=4):
+    """Sampled lines of the reference's .pqr and .xyz outputs with the .info / .freq
+    values each line is written from (``analysis_extra/pqr_xyz.json``)."""
+    import glob
+    import tarfile
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from plasmonx_b200 import outputs as O
+    cases = []
+    for name, label in (('analysis_pqr_wfq_sodium', '1.5800000000'), ('analysis_pqr_bem', '1.9100000000')):
+        with tarfile.open(os.path.join(ref, 'tests', name, name + '.tar.gz')) as tf:
+            info = O.read_info(tf.extractfile(name + '.info').read().decode())
+            _, _, blocks = O.read_freq(tf.extractfile('%s-%s.freq' % (name, label)).read().decode())
+        bem = info['model'] == 'bem'
+        pos = info['centres_ang'] if bem else info['coord_ang']
+        for pol, part in (('x', 'Re'), ('z', 'Im')):
+            f = glob.glob(os.path.join(ref, 'tests', name, 'reference', '*', '%s-E%s-%s-%s.pqr' % (name, pol, label,
+                                                                                                  part)))[0]
+            lines = open(f).read().splitlines()
+            vals = blocks[pol].real if part == 'Re' else blocks[pol].imag
+            idx = list(range(0, len(lines), stride))
+            cases.append({'kind': 'pqr', 'name': name, 'bem': bem, 'index': idx, 'lines': [lines[i] for i in idx],
+                          'pos': [list(pos[i]) for i in idx], 'value': [float(vals[i]) for i in idx],
+                          'z': [0 if bem else int(info['z'][i]) for i in idx]})
+    for name in ('analysis_xyz', 'analysis_xyz_bem'):
+        with tarfile.open(os.path.join(ref, 'tests', name, name + '.tar.gz')) as tf:
+            mem = [m for m in tf.getnames() if m.endswith('.info')][0]
+            info = O.read_info(tf.extractfile(mem).read().decode())
+        bem = info['model'] == 'bem'
+        pos = info['centres_ang'] if bem else info['coord_ang']
+        lines = open(glob.glob(os.path.join(ref, 'tests', name, 'reference', '*', '*.xyz'))[0]).read().splitlines()
+        idx = list(range(0, len(pos), stride))
+        cases.append({'kind': 'xyz', 'name': name, 'bem': bem, 'head': lines[:2], 'n': len(pos), 'index': idx,
+                      'lines': [lines[2 + i] for i in idx], 'pos': [list(pos[i]) for i in idx],
+                      'z': [0 if bem else int(info['z'][i]) for i in idx]})
+    odir = os.path.join(HERE, 'analysis_extra')
+    os.makedirs(odir, exist_ok=True)
+    with open(os.path.join(odir, 'pqr_xyz.json'), 'w') as f:
+        json.dump(cases, f)
+    print('analysis_extra/pqr_xyz.json', len(cases), 'cases')
+
+
 if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[1] == '--pqr-xyz':
+        pqr_xyz(sys.argv[2])
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--analysis-extra':
         for nm in ANALYSIS_EXTRA:
             one_analysis_extra(nm, sys.argv[2])

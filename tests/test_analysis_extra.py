@@ -4,7 +4,8 @@ by ``make_golden.py --analysis-extra``): the oracle's field / density through th
 product's grids and writers (plasmonx_b200/analysis.py) reproduce the reference's
 grid block, the plane .csv lines (coordinates to every printed digit, values to
 1e-10), the .plt header and values (float32, to one unit in the last place) and
-the effective volume and area lines.  The device kernel is held to the same files
+the effective volume and area lines; the .pqr and .xyz writers reproduce the
+reference's lines character for character (``--pqr-xyz`` samples).  The device kernel is held to the same files
 in test_gpu_analysis.py."""
 import json
 import os
@@ -82,7 +83,7 @@ def check_outputs(a, g, vals):
             assert len(mine) == ref['n_lines']
             for i, line in zip(ref['index'], ref['lines']):
                 m, r = mine[i].split(), line.split()
-                assert m[:2] == r[:2], (i, mine[i], line)
+                assert m[:2] == r[:2] and len(mine[i]) == len(line), (i, mine[i], line)
                 if r:
                     a_, b_ = float(m[2]), float(r[2])
                     assert abs(a_ - b_) <= 1e-10 * abs(b_) + 1e-300, (i, mine[i], line)
@@ -107,3 +108,32 @@ def test_oracle_through_writers_reproduces_reference(name):
     g = grid_of(a)
     f, d = oracle_fns(a)
     check_outputs(a, g, values_by(a, g, f, d))
+
+
+def _pqr_xyz_cases():
+    with open(os.path.join(EXTRA, 'pqr_xyz.json')) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize('case', range(6))
+def test_pqr_and_xyz_lines_match_reference(case):
+    """write_pqr_file / plot_xyz: the reference's .pqr (atoms and tesserae, real and
+    imaginary charges) and .xyz lines, character for character."""
+    from plasmonx_b200 import analysis as A
+    c = _pqr_xyz_cases()[case]
+    if c['kind'] == 'pqr':
+        # a charge the .freq file prints as -0.0000000000000000 comes out of the
+        # reference's reader as +0 or -0 (its .pqr shows both for the same text):
+        # the sign of a zero charge is not compared
+        same_zero = lambda t: t.replace('-0.000E+00', ' 0.000E+00')  # noqa: E731
+        for k, line, pos, v, z in zip(c['index'], c['lines'], c['pos'], c['value'], c['z']):
+            name = '' if c['bem'] else A.element_symbol(z)
+            mine = A.pqr_line(k + 1, name, pos, v, A.VDW_RADIUS.get(name, 0.0), c['bem'])
+            assert same_zero(mine) == same_zero(line)
+    else:
+        info = {'model': 'bem' if c['bem'] else 'wfq', 'z': c['z'],
+                ('centres_ang' if c['bem'] else 'coord_ang'): np.array(c['pos'])}
+        text = A.xyz_text(info).splitlines()
+        assert text[2:] == c['lines']
+        assert A.xyz_text(dict(info, **{('centres_ang' if c['bem'] else 'coord_ang'):
+                                        np.zeros((c['n'], 3))}, z=[0] * c['n'])).splitlines()[:2] == c['head']
