@@ -163,6 +163,7 @@ const char *plx_last_error(const plx_ctx *ctx) { return ctx ? ctx->last_error.c_
 uint64_t plx_ctx_bytes_in_use(const plx_ctx *ctx) { return ctx ? ctx->in_use : 0; }
 
 plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *d, int32_t store_t, plx_geom **out) {
+    TraceRange trace_("plx_geometry_create");
     if (!ctx || !d || !out) return PLX_ERR_ARG;
     *out = nullptr;
     plx_geom *g = new plx_geom();
@@ -236,6 +237,7 @@ plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *d, int32_t
 }
 
 plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *d, plx_geom **out) {
+    TraceRange trace_("plx_bem_create");
     if (!ctx || !d || !out) return PLX_ERR_ARG;
     *out = nullptr;
     plx_geom *g = new plx_geom();
@@ -314,6 +316,7 @@ plx_status plx_field_at_points(plx_geom *g, int32_t i_pol, const double *x, int3
                                double *field_out, double *density_out) {
     if (!g || !x || !points || n_points < 0) return PLX_ERR_ARG;
     return guarded(g->ctx, [&] {
+        TraceRange trace_("plx_field_at_points");
         set_device(g->ctx);
         if (is_bem(g)) throw Error(PLX_ERR_UNSUPPORTED, "field at points: atomistic models only");
         if (i_pol < 0 || i_pol > 2) throw Error(PLX_ERR_ARG, "polarisation index must be 0, 1 or 2");
@@ -343,6 +346,7 @@ plx_status plx_bem_field_at_points(plx_ctx *ctx, int32_t n_tess, const double *c
                                    int32_t i_pol, int32_t n_points, const double *points, double *field_out) {
     if (!ctx) return PLX_ERR_ARG;
     return guarded(ctx, [&] {
+        TraceRange trace_("plx_bem_field_at_points");
         set_device(ctx);
         bem_field_at_points(ctx, n_tess, centres, q, e0, i_pol, n_points, points, field_out);
     });
@@ -353,6 +357,7 @@ plx_status plx_neighbour_counts(plx_ctx *ctx, int32_t n_atoms, int32_t n_types, 
                                 int32_t *neighbours_out, int32_t *n_neighbours_out) {
     if (!ctx) return PLX_ERR_ARG;
     return guarded(ctx, [&] {
+        TraceRange trace_("plx_neighbour_counts");
         set_device(ctx);
         neighbour_counts(ctx, n_atoms, n_types, coord_ang, atom_type, type_z, r0, neighbours_out, n_neighbours_out);
     });
@@ -364,6 +369,7 @@ plx_status plx_static_solve(plx_ctx *ctx, const plx_static_desc *desc, int32_t w
                             double *energy, double *polar) {
     if (!ctx || !desc) return PLX_ERR_ARG;
     return guarded(ctx, [&] {
+        TraceRange trace_("plx_static_solve");
         set_device(ctx);
         static_solve(ctx, desc, what, variables, energy, polar);
     });
@@ -406,6 +412,7 @@ plx_status plx_gmres_solver(plx_geom *g, int32_t i_freq, double *x, int32_t on_t
     if (!g || !x) return PLX_ERR_ARG;
     plx_status conv = PLX_OK;
     plx_status s = guarded(g->ctx, [&] {
+        TraceRange trace_("plx_gmres_solver");
         set_device(g->ctx);
         if (i_freq < 0 || i_freq >= g->n_freq) throw Error(PLX_ERR_ARG, "frequency index out of range");
         (void)max_iter;   // no restart: the reference errors after the first cycle
@@ -435,6 +442,7 @@ plx_status plx_gmres_solver(plx_geom *g, int32_t i_freq, double *x, int32_t on_t
 plx_status plx_complex_inversion(plx_geom *g, int32_t i_freq, double *variables_w) {
     if (!g || !variables_w) return PLX_ERR_ARG;
     return guarded(g->ctx, [&] {
+        TraceRange trace_("plx_complex_inversion");
         set_device(g->ctx);
         if (i_freq < 0 || i_freq >= g->n_freq) throw Error(PLX_ERR_ARG, "frequency index out of range");
         const int n = g->n_var;
@@ -451,6 +459,7 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
     if (!g || !desc) return PLX_ERR_ARG;
     plx_status first_bad = PLX_OK;
     plx_status s = guarded(g->ctx, [&] {
+        TraceRange trace_("plx_solve");
         plx_ctx *ctx = g->ctx;
         set_device(ctx);
         cudaStream_t st = ctx->stream;
@@ -683,6 +692,7 @@ plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t 
 plx_status plx_contract(plx_geom *g, int32_t count, const double *X, double *S, int32_t how) {
     if (!g || !X || !S) return PLX_ERR_ARG;
     return guarded(g->ctx, [&] {
+        TraceRange trace_("plx_contract");
         set_device(g->ctx);
         if (count < 1 || how < 0 || how > 3) throw Error(PLX_ERR_ARG, "bad column count or contraction kind");
         const int n = g->n_var;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <mutex>
 #include <set>
@@ -21,6 +22,15 @@
     } while (0)
 
 namespace plx {
+
+// NVTX range over a scope: the library's phases show up by name in Nsight
+// Systems timelines (no cost without a tool attached).
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
 
 struct Error {
     plx_status code;

@@ -95,6 +95,7 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
     std::vector<double> rn(C);
     std::vector<char> live(C, 1);
     for (int outer = 0;; ++outer) {
+        TraceRange trace_("refinement step");
         column_norms<<<C, 256, 0, st>>>(n, R.p, nrm.p);
         ctx->launches++;
         PLX_CHECK_CUDA(cudaMemcpyAsync(rn.data(), nrm.p, C * 8, cudaMemcpyDeviceToHost, st));
