@@ -145,6 +145,9 @@ void plx_ctx_destroy(plx_ctx *ctx);
 const char *plx_last_error(const plx_ctx *ctx);
 /* Device bytes currently held by the context (geometries + solver state). */
 uint64_t plx_ctx_bytes_in_use(const plx_ctx *ctx);
+/* Kernels the library has launched on this context since its creation (its own
+ * kernels; cuBLAS / cuSOLVER launches are not counted). */
+int64_t plx_ctx_launches(const plx_ctx *ctx);
 
 /* ---- geometry -------------------------------------------------------------- */
 

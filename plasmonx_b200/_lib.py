@@ -23,7 +23,7 @@ EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
            'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points',
            'plx_static_n_var', 'plx_static_solve', 'plx_principal_axes', 'plx_neighbour_counts',
-           'plx_bem_field_at_points']
+           'plx_bem_field_at_points', 'plx_ctx_launches']
 STATIC_FF = {'fq': 0, 'fqfmu': 1}
 KERNEL = {'coulomb': 0, 'ohno': 1, 'gaussian': 2}
 STATIC_WHAT = {'energy': 0, 'static': 1}
@@ -85,6 +85,8 @@ def load():
     lib.plx_last_error.argtypes = [vp]
     lib.plx_ctx_bytes_in_use.restype = C.c_uint64
     lib.plx_ctx_bytes_in_use.argtypes = [vp]
+    lib.plx_ctx_launches.restype = C.c_int64
+    lib.plx_ctx_launches.argtypes = [vp]
     lib.plx_geometry_create.argtypes = [vp, C.POINTER(GeometryDesc), C.c_int32, C.POINTER(vp)]
     lib.plx_bem_create.argtypes = [vp, C.POINTER(BemDesc), C.POINTER(vp)]
     lib.plx_geometry_destroy.argtypes = [vp]

@@ -162,6 +162,8 @@ const char *plx_last_error(const plx_ctx *ctx) { return ctx ? ctx->last_error.c_
 
 uint64_t plx_ctx_bytes_in_use(const plx_ctx *ctx) { return ctx ? ctx->in_use : 0; }
 
+int64_t plx_ctx_launches(const plx_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
 plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *d, int32_t store_t, plx_geom **out) {
     TraceRange trace_("plx_geometry_create");
     if (!ctx || !d || !out) return PLX_ERR_ARG;
@@ -235,6 +237,7 @@ plx_status plx_geometry_create(plx_ctx *ctx, const plx_geometry_desc *d, int32_t
     *out = g;
     return PLX_OK;
 }
+
 
 plx_status plx_bem_create(plx_ctx *ctx, const plx_bem_desc *d, plx_geom **out) {
     TraceRange trace_("plx_bem_create");

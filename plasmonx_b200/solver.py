@@ -56,6 +56,11 @@ class Context:
     def bytes_in_use(self):
         return int(self.lib.plx_ctx_bytes_in_use(self.h))
 
+    @property
+    def launches(self):
+        """Kernels the library has launched on this context (its own kernels)."""
+        return int(self.lib.plx_ctx_launches(self.h))
+
     def close(self):
         if self.h:
             self.lib.plx_ctx_destroy(self.h)
