@@ -73,6 +73,7 @@ TESTS = [
     'wfqfmu_ag_read_xyz',
     'wfqfmu_au_read_xyz',
     'wfqfmu_hetero_agau_read_xyz',
+    'bem_dpcm_external_brendel_bormann_ag',
 ]
 
 NUM = r'[-+]?\d*\.\d+(?:[EeDd][-+]?\d+)?'
@@ -243,6 +244,11 @@ def one(name, ref):
                 fn = line.split(':', 1)[1].strip()
                 if fn != 'none':
                     shutil.copy(os.path.join(tdir, fn), os.path.join(odir, os.path.basename(fn)))
+            if line.startswith('bem permittivity file:'):
+                fn = line.split(':', 1)[1].strip()
+                if fn != 'none':
+                    with open(os.path.join(odir, os.path.basename(fn)), 'w') as f:
+                        f.write(csv_subset(os.path.join(tdir, fn), fev))
             if 'wfqfmu file:' in line:
                 fn = line.split(':', 1)[1].strip()
                 if fn != 'none':
