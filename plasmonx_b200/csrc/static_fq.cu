@@ -288,6 +288,128 @@ __global__ void multipliers(int m, int ncols, int64_t ld, int n, int64_t nv, con
     V[(int64_t)c * nv + n + k] = (Bt[f] - Z[f]) / (-sqrt((double)(hi[k] - lo[k])));
 }
 
+// ---------------------------------------------------------------------------
+// mixed-precision Cholesky with FP64 iterative refinement (the published
+// algorithm of LAPACK's dsposv: factor in single precision, correct in double
+// until ||r||_inf < ||x||_inf ||A||_inf eps sqrt(n) for every column, at most
+// 30 corrections; otherwise the caller factors in double precision)
+// ---------------------------------------------------------------------------
+
+__global__ void to_float(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+__global__ void add_float(int64_t n, const float *__restrict__ d, double *__restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += (double)d[i];
+}
+
+// out[c] = max_i |A(i, c)|, one block per column
+__global__ void col_max_abs(int rows, const double *__restrict__ A, double *__restrict__ out) {
+    __shared__ double red[256];
+    const double *a = A + (int64_t)blockIdx.x * rows;
+    double m = 0.0;
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) m = fmax(m, fabs(a[i]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+// out[c] = sum_i |A(i, c)| (column sums; the row sums of a symmetric matrix)
+__global__ void col_sum_abs(int rows, const double *__restrict__ A, double *__restrict__ out) {
+    __shared__ double red[256];
+    const double *a = A + (int64_t)blockIdx.x * rows;
+    double t = 0.0;
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) t += fabs(a[i]);
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+// K (n x n, FP64, kept) X = B (n x ncols, right-hand sides in, solutions out);
+// false when the single-precision factor fails or the corrections stall
+bool mixed_cholesky(plx_ctx *ctx, int n, int ncols, const double *K, double *B, int *iterations) {
+    cudaStream_t st = ctx->stream;
+    cusolverDnHandle_t h = solver_handle(ctx);
+    const int64_t nn = (int64_t)n * n, nb = (int64_t)n * ncols;
+    DevArray<float> Kf, Rf, fwork;
+    DevArray<double> X, R, B0, norms, colsum;
+    DevArray<int32_t> info;
+    Kf.alloc(ctx, nn);
+    Rf.alloc(ctx, nb);
+    X.alloc(ctx, nb);
+    R.alloc(ctx, nb);
+    B0.alloc(ctx, nb);
+    norms.alloc(ctx, 2 * (size_t)ncols);
+    colsum.alloc(ctx, n);
+    info.alloc(ctx, 1);
+    const int grid = (int)std::min<int64_t>(n_blocks(nn, 256), 148 * 16);
+    to_float<<<grid, 256, 0, st>>>(nn, K, Kf.p);
+    col_sum_abs<<<n, 256, 0, st>>>(n, K, colsum.p);
+    ctx->launches += 2;
+    PLX_CHECK_CUDA(cudaGetLastError());
+    int lwork = 0;
+    if (cusolverDnSpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, n, Kf.p, n, &lwork) != CUSOLVER_STATUS_SUCCESS)
+        throw Error(PLX_ERR_CUDA, "cusolverDnSpotrf_bufferSize failed");
+    fwork.alloc(ctx, std::max(lwork, 1));
+    if (cusolverDnSpotrf(h, CUBLAS_FILL_MODE_LOWER, n, Kf.p, n, fwork.p, lwork, info.p) != CUSOLVER_STATUS_SUCCESS)
+        throw Error(PLX_ERR_CUDA, "cusolverDnSpotrf failed");
+    int hinfo = 0;
+    std::vector<double> cs(n);
+    PLX_CHECK_CUDA(cudaMemcpyAsync(&hinfo, info.p, 4, cudaMemcpyDeviceToHost, st));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(cs.data(), colsum.p, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (hinfo != 0) return false;
+    const double anrm = *std::max_element(cs.begin(), cs.end());
+    const double cte = anrm * std::ldexp(1.0, -53) * std::sqrt((double)n);
+    PLX_CHECK_CUDA(cudaMemcpyAsync(B0.p, B, nb * 8, cudaMemcpyDeviceToDevice, st));
+    PLX_CHECK_CUDA(cudaMemsetAsync(X.p, 0, nb * 8, st));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(R.p, B, nb * 8, cudaMemcpyDeviceToDevice, st));
+    const double one = 1.0, minus = -1.0;
+    std::vector<double> hn(2 * (size_t)ncols);
+    const int gb = (int)std::min<int64_t>(n_blocks(nb, 256), 148 * 8);
+    for (int it = 0; it <= 30; ++it) {
+        // correction d = K^-1 r in single precision; x += d; r = b - K x
+        to_float<<<gb, 256, 0, st>>>(nb, R.p, Rf.p);
+        ctx->launches++;
+        if (cusolverDnSpotrs(h, CUBLAS_FILL_MODE_LOWER, n, ncols, Kf.p, n, Rf.p, n, info.p) != CUSOLVER_STATUS_SUCCESS)
+            throw Error(PLX_ERR_CUDA, "cusolverDnSpotrs failed");
+        add_float<<<gb, 256, 0, st>>>(nb, Rf.p, X.p);
+        ctx->launches++;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(R.p, B0.p, nb * 8, cudaMemcpyDeviceToDevice, st));
+        if (cublasDgemm(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_N, n, ncols, n, &minus, K, n, X.p, n, &one, R.p, n) !=
+            CUBLAS_STATUS_SUCCESS)
+            throw Error(PLX_ERR_CUDA, "cublasDgemm failed");
+        col_max_abs<<<ncols, 256, 0, st>>>(n, R.p, norms.p);
+        col_max_abs<<<ncols, 256, 0, st>>>(n, X.p, norms.p + ncols);
+        ctx->launches += 2;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        PLX_CHECK_CUDA(cudaMemcpyAsync(hn.data(), norms.p, hn.size() * 8, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        bool done = true;
+        for (int c = 0; c < ncols; ++c) {
+            if (!std::isfinite(hn[c]) || !std::isfinite(hn[ncols + c])) return false;
+            if (!(hn[c] < hn[ncols + c] * cte) && hn[c] != 0.0) done = false;
+        }
+        if (done) {
+            PLX_CHECK_CUDA(cudaMemcpyAsync(B, X.p, nb * 8, cudaMemcpyDeviceToDevice, st));
+            PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+            *iterations = it + 1;
+            return true;
+        }
+    }
+    return false;
+}
+
 // blocks disjoint and inside the charge rows: the elimination applies
 bool blocks_disjoint(const std::vector<int32_t> &lo, const std::vector<int32_t> &hi) {
     std::vector<int> order(lo.size());
@@ -302,15 +424,19 @@ bool blocks_disjoint(const std::vector<int32_t> &lo, const std::vector<int32_t> 
 
 namespace plx {
 
+bool finish_eliminated(plx_ctx *ctx, const StaticDims &s, int N, int nr, int nrhs, const int32_t *d_keep,
+                       const int32_t *d_lo, const int32_t *d_hi, const double *K, const double *B, const double *Bt,
+                       const double *Br, const double *Rr, double *variables, double *energy, double *polar);
+
 // The constrained solve by elimination (see reflect_rows); false when the
 // matrix without the constraint rows is not positive definite (Cholesky
 // breaks down), and the caller then factors the full system by LU.
-bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int potential, double e0, const double *mins,
+bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int mode, int potential, double e0, const double *mins,
                       const double *d_pos, const int32_t *d_type, const double *d_par,
                       const std::vector<int32_t> &lo, const std::vector<int32_t> &hi, const int32_t *d_lo,
                       const int32_t *d_hi, double *variables, double *energy, double *polar) {
     cudaStream_t st = ctx->stream;
-    const int n = s.n, m = s.n_mol, nv = s.n_var;
+    const int n = s.n, m = s.n_mol;
     const int N = s.fmu ? 4 * n : n;          // unknowns without the constraint rows
     const int nrhs = what == PLX_STATIC_FIELD ? 3 : 1;
     const int ncols = nrhs + (polar ? 3 : 0);  // the polarizability adds R as right-hand sides
@@ -327,7 +453,7 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int potential
             if (!removed[i]) keep.push_back(i);
     }
     const int nr = (int)keep.size();
-    DevArray<double> K, Kr, B, Bt, Br, Rr, Y, Z, V, work, P;
+    DevArray<double> K, Kr, B, Bt, Br, Rr, work;
     DevArray<int32_t> d_keep, info;
     K.alloc(ctx, (size_t)N * N);
     Kr.alloc(ctx, (size_t)nr * nr);
@@ -365,6 +491,18 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int potential
                                        st));
     }
 
+    const double dr = nr;
+    if (mode == 0) {
+        // single-precision Cholesky refined in double; Kr stays intact for the
+        // double-precision factorisation if the refinement gives up
+        prof_begin(ctx);
+        int iters = 0;
+        const bool ok = mixed_cholesky(ctx, nr, ncols, Kr.p, Br.p, &iters);
+        prof_end(ctx, kProfStaticFactor, ok ? dr * dr * dr / 3.0 + iters * 4.0 * dr * dr * ncols : 0.0,
+                 ok ? 4.0 * dr * dr : 0.0);
+        if (ok) return finish_eliminated(ctx, s, N, nr, nrhs, d_keep.p, d_lo, d_hi, K.p, B.p, Bt.p, Br.p,
+                                         Rr.p, variables, energy, polar);
+    }
     prof_begin(ctx);
     cusolverDnHandle_t h = solver_handle(ctx);
     int lwork = 0;
@@ -384,22 +522,33 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int potential
     if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, nr, ncols, Kr.p, nr, Br.p, nr, info.p) != CUSOLVER_STATUS_SUCCESS)
         throw Error(PLX_ERR_CUDA, "cusolverDnDpotrs failed");
     check_info(ctx, info, "DPOTRS of the reduced static matrix");
-    const double dr = nr;
     prof_end(ctx, kProfStaticFactor, dr * dr * dr / 3.0 + 2.0 * dr * dr * ncols, 8.0 * dr * dr);
+    return finish_eliminated(ctx, s, N, nr, nrhs, d_keep.p, d_lo, d_hi, K.p, B.p, Bt.p, Br.p, Rr.p, variables,
+                             energy, polar);
+}
 
-    // back to the original basis: y (removed rows zero), x = H y, multipliers
+// Back to the original basis after the reduced solve (Br holds the reduced
+// solutions, and R^T-side columns for the polarizability after the first nrhs):
+// y with the removed rows zero, the multipliers from the removed rows, x = H y,
+// the variables in the reference's order, the energy and the polarizability.
+bool finish_eliminated(plx_ctx *ctx, const StaticDims &s, int N, int nr, int nrhs, const int32_t *d_keep,
+                       const int32_t *d_lo, const int32_t *d_hi, const double *K, const double *B, const double *Bt,
+                       const double *Br, const double *Rr, double *variables, double *energy, double *polar) {
+    cudaStream_t st = ctx->stream;
+    const int n = s.n, m = s.n_mol, nv = s.n_var;
+    DevArray<double> Y, Z, V, P;
     Y.alloc(ctx, (size_t)N * nrhs);
     Z.alloc(ctx, (size_t)N * nrhs);
     V.alloc(ctx, (size_t)nv * nrhs);
     PLX_CHECK_CUDA(cudaMemsetAsync(Y.p, 0, (size_t)N * nrhs * 8, st));
-    scatter_kept<<<dim3(n_blocks(nr, 128), nrhs), 128, 0, st>>>(nr, nrhs, N, d_keep.p, Br.p, Y.p);
+    scatter_kept<<<dim3(n_blocks(nr, 128), nrhs), 128, 0, st>>>(nr, nrhs, N, d_keep, Br, Y.p);
     {
         const double one = 1.0, zero = 0.0;  // Z = (H K H) y
-        if (cublasDgemm(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_N, N, nrhs, N, &one, K.p, N, Y.p, N, &zero, Z.p,
+        if (cublasDgemm(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_N, N, nrhs, N, &one, K, N, Y.p, N, &zero, Z.p,
                         N) != CUBLAS_STATUS_SUCCESS)
             throw Error(PLX_ERR_CUDA, "cublasDgemm failed");
     }
-    multipliers<<<n_blocks((int64_t)m * nrhs, 128), 128, 0, st>>>(m, nrhs, N, n, nv, d_lo, d_hi, Bt.p, Z.p, V.p);
+    multipliers<<<n_blocks((int64_t)m * nrhs, 128), 128, 0, st>>>(m, nrhs, N, n, nv, d_lo, d_hi, Bt, Z.p, V.p);
     reflect_rows<<<n_blocks((int64_t)m * nrhs, 128), 128, 0, st>>>(m, nrhs, N, d_lo, d_hi, Y.p);
     ctx->launches += 3;
     PLX_CHECK_CUDA(cudaGetLastError());
@@ -411,7 +560,7 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int potential
                                          nrhs, cudaMemcpyDeviceToDevice, st));
     if (energy) {
         double dot = 0.0;  // the constraint rows' right-hand side is zero
-        if (cublasDdot(blas_handle(ctx), N, Y.p, 1, B.p, 1, &dot) != CUBLAS_STATUS_SUCCESS)
+        if (cublasDdot(blas_handle(ctx), N, Y.p, 1, B, 1, &dot) != CUBLAS_STATUS_SUCCESS)
             throw Error(PLX_ERR_CUDA, "cublasDdot failed");
         *energy = -0.5 * dot;
     }
@@ -421,7 +570,7 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int potential
         // R^T Z (Z^T J Z)^-1 Z^T R: the reference's
         // R^T J^-1 R - (L^T J^-1 R)^T (L^T J^-1 L)^-1 (L^T J^-1 R) for disjoint constraints
         P.alloc(ctx, 9);
-        gemm_tn(ctx, 3, 3, nr, Rr.p, nr, Br.p + (size_t)nrhs * nr, nr, P.p);
+        gemm_tn(ctx, 3, 3, nr, Rr, nr, Br + (size_t)nrhs * nr, nr, P.p);
         PLX_CHECK_CUDA(cudaMemcpyAsync(polar, P.p, 9 * 8, cudaMemcpyDeviceToHost, st));
     }
     PLX_CHECK_CUDA(cudaStreamSynchronize(st));
@@ -501,8 +650,8 @@ void static_solve(plx_ctx *ctx, const plx_static_desc *d, int what, double *vari
     PLX_CHECK_CUDA(cudaMemcpyAsync(d_hi.p, hi.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st));
 
     const int nrhs = what == PLX_STATIC_FIELD ? 3 : 1;
-    if (d->factorization == 0 && blocks_disjoint(lo, hi) &&
-        solve_eliminated(ctx, s, what, d->rhs_potential, d->e0, mins, d_pos.p, d_type.p, d_par.p, lo, hi, d_lo.p,
+    if (d->factorization != 1 && blocks_disjoint(lo, hi) &&
+        solve_eliminated(ctx, s, what, d->factorization, d->rhs_potential, d->e0, mins, d_pos.p, d_type.p, d_par.p, lo, hi, d_lo.p,
                          d_hi.p, variables, energy, polar))
         return;
     A.alloc(ctx, (size_t)nv * nv);
