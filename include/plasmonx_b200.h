@@ -323,13 +323,12 @@ typedef struct {
     const double *r_mu;         /* Gaussian dipole width (FQFMu) */
     double e0;                  /* field intensity (a.u.) */
     int32_t factorization;      /* 0 automatic: the charge constraints eliminated on a
-                                   null-space basis and the rest factored by Cholesky in
-                                   single precision with double-precision iterative
-                                   refinement (LAPACK dsposv's algorithm), falling back
-                                   to a double-precision Cholesky, and to LU of the full
-                                   system where elimination does not apply;
-                                   1 LU of the full system (the reference's form);
-                                   2 elimination with a double-precision Cholesky */
+                                   null-space basis and the rest factored by a
+                                   double-precision Cholesky, LU of the full system where
+                                   that does not apply; 1 LU of the full system (the
+                                   reference's form); 2 as 0 with the Cholesky factor in
+                                   single precision and double-precision iterative
+                                   refinement (LAPACK dsposv's algorithm) */
 } plx_static_desc;
 
 /* n_var of a static problem, or -1 for an invalid description. */

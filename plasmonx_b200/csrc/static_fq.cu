@@ -22,7 +22,9 @@
 //     with, for water, 1/16 of the LU's flops.  When the constraint blocks
 //     overlap (ragged molecules under the reference's indexing) or Cholesky
 //     breaks down, or when asked, the full system is factored by pivoted LU
-//     (dgetrf / dgetrs);
+//     (dgetrf / dgetrs).  On request the reduced system is factored in single
+//     precision and refined in double (mixed_cholesky); measured on B200 it
+//     does not beat the double-precision factor at these sizes;
 //   * the ground-state energy -1/2 x.b (calculate_energy_fq, fq_module.f90:358-374)
 //     and the FQ static polarizability
 //     R^T J^-1 R - (L^T J^-1 R)^T (L^T J^-1 L)^-1 (L^T J^-1 R), J the charge
@@ -492,7 +494,7 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int mode, int
     }
 
     const double dr = nr;
-    if (mode == 0) {
+    if (mode == 2) {
         // single-precision Cholesky refined in double; Kr stays intact for the
         // double-precision factorisation if the refinement gives up
         prof_begin(ctx);

@@ -29,7 +29,7 @@ from .outputs import fortran_f
 from .solver import Context
 
 
-FACTORIZATION = {'auto': 0, 'lu': 1, 'cholesky': 2}
+FACTORIZATION = {'auto': 0, 'lu': 1, 'cholesky_mixed': 2}
 
 
 def atoms_per_molecule(mol_index):
@@ -79,11 +79,11 @@ class StaticProblem:
         self.what = what
         self.method = method
         if factorization not in FACTORIZATION:
-            raise ValueError("factorization must be 'auto', 'lu' or 'cholesky'")
-        # 'auto': charge constraints eliminated, the rest factored by a single-precision
-        # Cholesky refined in double (double-precision Cholesky, then LU of the full
-        # system, where that does not apply); 'cholesky': elimination with a
-        # double-precision Cholesky; 'lu': LU of the full system, the reference's form
+            raise ValueError("factorization must be 'auto', 'lu' or 'cholesky_mixed'")
+        # 'auto': charge constraints eliminated, the rest factored by a double-precision
+        # Cholesky (LU of the full system where that does not apply); 'cholesky_mixed':
+        # the same with a single-precision factor refined in double; 'lu': LU of the
+        # full system, the reference's form
         self.factorization = factorization
         self.type_names = list(type_names)
         nt = len(self.type_names)

@@ -51,7 +51,7 @@ def _oracle(p):
                       p.rhs_form, p.e0)
 
 
-@pytest.mark.parametrize('factorization', ['auto', 'cholesky', 'lu'])
+@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed', 'lu'])
 @pytest.mark.parametrize('name', CASES)
 def test_golden_static_matches_oracle_and_log(ctx, name, factorization):
     p = StaticProblem.from_keyword_file(os.path.join(GOLDEN, name, 'input.kw'))
@@ -83,7 +83,7 @@ SYNTH = [(ff, kernel, what, form, e0)
          for what, form, e0 in (('energy', 'field', 0.0), ('static', 'field', 1e-3), ('static', 'potential', 2e-3))]
 
 
-@pytest.mark.parametrize('factorization', ['auto', 'cholesky', 'lu'])
+@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed', 'lu'])
 @pytest.mark.parametrize('ff,kernel,what,form,e0', SYNTH, ids=lambda v: str(v))
 def test_water_clusters_match_oracle(ctx, ff, kernel, what, form, e0, factorization):
     p = water_cluster(40, ff, kernel, what=what, rhs_form=form, e0=e0, seed=7, factorization=factorization)
@@ -96,14 +96,14 @@ def test_water_clusters_match_oracle(ctx, ff, kernel, what, form, e0, factorizat
         assert _rel(out['polar'], ref['polar']) < 1e-11
 
 
-@pytest.mark.parametrize('factorization', ['auto', 'cholesky'])
+@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed'])
 @pytest.mark.parametrize('ff,what', [('fq', 'energy'), ('fq', 'static'), ('fqfmu', 'energy')])
 def test_elimination_is_the_default_path(ctx, ff, what, factorization):
     """With positive definite blocks (Ohno, Gaussian) the reduced system is factored
-    by Cholesky -- in single precision with double-precision refinement by default,
-    in double precision on request: the profiled flops are those of a reduced
-    Cholesky (plus the corrections), not of the full LU, and the answers agree
-    with the LU form."""
+    by Cholesky -- in double precision by default, in single precision with
+    double-precision refinement on request: the profiled flops are those of a
+    reduced Cholesky (plus the corrections), not of the full LU, and the answers
+    agree with the LU form."""
     p = water_cluster(40, ff, what=what, e0=1e-3, seed=7, factorization=factorization)
     ctx.profile(True)
     auto = StaticSolver(p, ctx=ctx).solve()
@@ -113,7 +113,7 @@ def test_elimination_is_the_default_path(ctx, ff, what, factorization):
     nr = (n if ff == 'fq' else 4 * n) - m
     ncols = (1 if what == 'energy' else 3) + (3 if (ff == 'fq' and what == 'static') else 0)
     chol = nr ** 3 / 3.0
-    if factorization == 'cholesky':
+    if factorization == 'auto':
         assert abs(fl - (chol + 2.0 * nr * nr * ncols)) <= 1e-9 * fl
     else:
         iters = (fl - chol) / (4.0 * nr * nr * ncols)
