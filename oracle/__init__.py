@@ -17,11 +17,17 @@ Contents
   solve.py     the three solver modes per frequency
                (``src/solvers/algorithm_module.f90:189-630``)
   bem.py       DPCM/IEFPCM boundary-element restatement (``src/bem/bem_module.f90``)
+  analysis.py  induced field and density at points, atomistic and BEM (the
+               reference's analysis step, ``src/matrix/matrix_module.f90:1140-1464``)
+  static.py    static FQ / FQFMu solves and the principal-axis rotation
+               (``src/forcefield/fq_module.f90``, ``fqfmu_module.f90``)
   pairs.c      C/OpenMP restatement of the on-the-fly pair kernels
                (``src/matrix/matrix_module.f90:727-1125``), the timed CPU baseline
 
 Parity pins: the oracle is checked against the numbers printed in the
-reference's own regression logs (``tests/*/reference/*.log``) by
-``tests/test_oracle_golden.py``; the extracted fixtures live in
-``tests/golden/`` together with the script that extracted them.
+reference's own regression logs and output files (``tests/*/reference/``) by
+``tests/test_oracle_golden.py``, ``test_static_golden.py``,
+``test_analysis_golden.py`` and ``test_analysis_extra.py``; the extracted
+fixtures live in ``tests/golden/`` together with the script that extracted
+them.
 """

@@ -28,3 +28,19 @@ def test_reference_arm_prints_the_contract_line():
     assert d['cpu_baseline']['kind'] == 'port' and d['cpu_baseline']['cores'] >= 1
     assert d['e2e'] == {'value': d['value'], 'unit': d['unit'], 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}
     assert d['config']['n_var'] == 41892
+
+
+def test_static_reference_arm_prints_the_contract_line():
+    """The static workload's reference arm: the oracle's solve of a small water cluster."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--config',
+                          'fq_water', '--waters', '40', '--steps', '1', '--warmup', '0'], capture_output=True,
+                         text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip().startswith('{')]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d['impl'] == 'reference' and d['metric'] == bench.STATIC_METRIC and d['unit'] == 'solves/s'
+    assert d['config']['n_var'] == 160 and d['value'] > 0
+    assert d['e2e']['h2d_bytes_per_step'] == 0 and d['cpu_baseline']['kind'] == 'port'
