@@ -20,10 +20,11 @@ script
   4. copies the test's backup files (``bk/*.plasmonX.bk``, restart tests).
 With ``--analysis`` it instead stores, for three analysis tests of the
 reference, the inputs of the field / density step and a sample of the cube
-file the reference wrote (``<name>/analysis.json``).  With ``--analysis-extra`` it stores, for four more analysis tests (a plane
-of |E|/E0, planes of the density, an effective volume, the binary .plt
-format), their inputs and sampled outputs in ``analysis_extra/``; with
-``--pqr-xyz`` sampled lines of its .pqr and .xyz outputs.  With
+file the reference wrote (``<name>/analysis.json``).  With ``--analysis-grids`` it stores, for fourteen more analysis tests
+(planes, user-bounded planes and slabs with their effective volume, the
+binary .plt format, wFQFMu densities, a BEM plane), their inputs and sampled
+outputs in ``analysis_grids/``; with ``--pqr-xyz`` sampled lines of its .pqr
+and .xyz outputs in ``analysis_extra/``.  With
 ``--info`` it copies three
 ``.info`` files and one ``.freq`` file out of the reference's analysis-test
 tarballs into ``info/`` (the files its analysis tool reads).  With ``--static`` it
@@ -449,68 +450,88 @@ def copy_info(ref):
                 print('info/' + m)
 
 
-# analysis tests on planes, with an effective volume, and with the binary .plt
-# format: test name -> (polarisation, frequency label, output kind, options)
-ANALYSIS_EXTRA = {
-    'analysis_field_2d_x_yz_wfq_sodium': (0, '1.5800000000', 'plane', {'plane': 'yz', 'third': 6.35,
-                                                                      'files': ['-Ex-1.5800000000-p-6.35.csv']}),
-    'analysis_density_2d_x_wfq_sodium': (0, '1.5800000000', 'plane', {
-        'plane': 'xy', 'third': 6.35, 'files': ['-Ex-1.5800000000-p-6.35-densityRe.csv',
-                                                '-Ex-1.5800000000-p-6.35-densityIm.csv']}),
-    'analysis_field_volume_x_wfq_sodium': (0, '1.5800000000', 'volume', {'lo': [53.0, 0.0, 0.0],
-                                                                         'hi': [55.0, 10.0, 10.0]}),
-    'analysis_field_3d_x_wfq_sodium_plt': (0, '1.5800000000', 'plt', {}),
-}
+# every grid-producing analysis test the reference has beyond the three cube
+# tests above: planes (one or several), user-bounded planes and slabs, the
+# binary .plt format, wFQFMu densities, BEM planes
+ANALYSIS_GRIDS = [
+    'analysis_field_2d_x_yz_wfq_sodium', 'analysis_density_2d_x_wfq_sodium',
+    'analysis_density_2d_x_wfq_sodium_n_planes', 'analysis_density_2d_y_xy_wfqfmu_ag',
+    'analysis_field_2d_y_xy_bem', 'analysis_field_2d_z_xz_wfqfmu_ag', 'analysis_field_2d_z_xz_wfqfmu_ag_reduced',
+    'analysis_field_volume_x_wfq_sodium', 'analysis_field_volume_z_wfqfmu_au',
+    'analysis_field_3d_x_wfq_sodium_plt', 'analysis_density_3d_x_wfq_sodium_plt',
+    'analysis_field_3d_x_y_z_wfqfmu_ag_plt', 'analysis_density_3d_y_wfqfmu_au', 'analysis_density_3d_y_wfqfmu_au_plt',
+]
 
 
-def one_analysis_extra(name, ref, stride=7):
-    """Inputs and sampled outputs of one plane / volume / plt analysis test
-    (``analysis_extra/<name>.json``)."""
+def _analysis_options(test_text):
+    """The analysis command line of a reference test: its options as a dict."""
+    line = re.search(r"input_files=\['[^ ]+ (.*?)'\]", test_text).group(1)
+    toks = line.replace('=', ' ').split()
+    opts, k = {}, 0
+    while k < len(toks):
+        key = toks[k].lstrip('-')
+        if k + 1 < len(toks) and not re.fullmatch(r'-[a-z_]+', toks[k + 1]):
+            opts[key] = toks[k + 1]
+            k += 2
+        else:
+            opts[key] = True
+            k += 1
+    return opts
+
+
+def one_analysis_grid(name, ref, max_lines=150):
+    """Inputs and sampled outputs of one grid analysis test (``analysis_grids/<name>.json``)."""
     import struct
     import tarfile
-    pol, flabel, kind, opts = ANALYSIS_EXTRA[name]
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from plasmonx_b200 import outputs as O
     tdir = os.path.join(ref, 'tests', name)
+    opts = _analysis_options(open(os.path.join(tdir, 'test')).read())
+    label = O.fortran_f(float(opts['freq']), 12, 10).strip()
     with tarfile.open(os.path.join(tdir, name + '.tar.gz')) as tf:
-        info = tf.extractfile(name + '.info').read().decode().splitlines()
-        freq = tf.extractfile('%s-%s.freq' % (name, flabel)).read().decode().splitlines()
-    n_atoms = int(info[0].split(':')[1])
-    g0 = info.index('Input Geometry (angstrom)') + 1
-    p0 = next(i for i, l in enumerate(info) if l.startswith('Parameters:'))
-    heads = [i for i, l in enumerate(freq) if l.startswith('complex')]
-    rows = freq[heads[pol] + 1:(heads[pol + 1] if pol + 1 < len(heads) else len(freq))]
-    out = {'name': name, 'model': info[5].split(':')[1].strip(), 'e0': float(info[7].split(':')[1]),
-           'coords_ang': [[float(v) for v in l.split()[2:5]] for l in info[g0:g0 + n_atoms]],
-           'z': [int(float(l.split()[0])) for l in info[g0:g0 + n_atoms]],
-           'rq': float(info[p0 + 2].split()[3]), 'pol': pol, 'kind': kind, 'options': opts,
-           'x': [[float(l.split()[1]), float(l.split()[2])] for l in rows if l.strip()]}
+        info = O.read_info(tf.extractfile(name + '.info').read().decode())
+        _, _, blocks = O.read_freq(tf.extractfile('%s-%s.freq' % (name, label)).read().decode())
+    pols = list(opts['field_dir']) if 'field_dir' in opts else ['x', 'y', 'z']
+    bem = info['model'] == 'bem'
+    out = {'name': name, 'model': info['model'], 'e0': info['e0'], 'what': opts['w'], 'label': label,
+           'pols': pols, 'options': {k: v for k, v in opts.items() if k not in ('w', 'n', 'freq')},
+           'x': {p: [[float(v.real), float(v.imag)] for v in blocks[p]] for p in pols}}
+    if bem:
+        out['centres_ang'] = info['centres_ang'].tolist()
+    else:
+        par = info['types'][0][1]
+        out.update(coords_ang=info['coord_ang'].tolist(), z=[int(v) for v in info['z']],
+                   rq=par[2] if info['model'] == 'wfq' else par[3], rmu=par[4] if info['model'] == 'wfqfmu' else 0.0)
     post = os.path.join(tdir, 'reference', 'post_process_' + name)
     log = open(os.path.join(post, name + '_analysis.log')).read().splitlines()
     g = next(i for i, l in enumerate(log) if 'Grid Information (Angstrom)' in l)
     out['log_grid'] = log[g:g + 10]
-    if kind == 'plane':
-        out['csv'] = {}
-        for suffix in opts['files']:
-            lines = open(os.path.join(post, 'planes', opts['plane'], name + suffix)).read().splitlines()
-            idx = list(range(0, len(lines), max(stride, len(lines) // 600)))
-            out['csv'][suffix] = {'n_lines': len(lines), 'index': idx, 'lines': [lines[i] for i in idx]}
-    elif kind == 'volume':
-        v = next(i for i, l in enumerate(log) if 'Calculation of effective volume' in l)
-        out['volume_lines'] = log[v:v + 5]
-        m = next(i for i, l in enumerate(log) if 'Max.' in l and l.startswith('  Field'))
-        out['log_max'] = log[m:m + 2]
-    elif kind == 'plt':
-        data = open(os.path.join(post, '%s-Ex-%s.plt' % (name, flabel)), 'rb').read()
-        head_i = list(struct.unpack('<5i', data[:20]))
-        head_f = list(struct.unpack('<6f', data[20:44]))
-        vals = struct.unpack('<%df' % ((len(data) - 44) // 4), data[44:])
-        idx = list(range(0, len(vals), 10))
-        out['plt'] = {'bytes': len(data), 'head_i': head_i, 'head_f': head_f, 'index': idx,
-                      'values': [vals[i] for i in idx]}
-    odir = os.path.join(HERE, 'analysis_extra')
+    out['log_max'] = [log[i:i + 2] for i, l in enumerate(log) if 'Max.' in l and not l.startswith(' Max. Freq')]
+    v = [i for i, l in enumerate(log) if 'Calculation of effective volume' in l]
+    out['volume_lines'] = [log[i:i + 5] for i in v]
+    files = {}
+    for fn in sorted(os.listdir(post)) + sorted(os.path.join('planes', d, f) for d in
+                                                (os.listdir(os.path.join(post, 'planes'))
+                                                 if os.path.isdir(os.path.join(post, 'planes')) else [])
+                                                for f in os.listdir(os.path.join(post, 'planes', d))):
+        path = os.path.join(post, fn)
+        if fn.endswith('.csv') or fn.endswith('.cube'):
+            lines = open(path).read().splitlines()
+            idx = list(range(0, len(lines), max(1, len(lines) // max_lines)))
+            files[os.path.basename(fn)] = {'n_lines': len(lines), 'index': idx, 'lines': [lines[i] for i in idx]}
+        elif fn.endswith('.plt'):
+            data = open(path, 'rb').read()
+            vals = struct.unpack('<%df' % ((len(data) - 44) // 4), data[44:])
+            idx = list(range(0, len(vals), max(1, len(vals) // max_lines)))
+            files[os.path.basename(fn)] = {'bytes': len(data), 'head_i': list(struct.unpack('<5i', data[:20])),
+                                           'head_f': list(struct.unpack('<6f', data[20:44])), 'index': idx,
+                                           'values': [vals[i] for i in idx]}
+    out['files'] = files
+    odir = os.path.join(HERE, 'analysis_grids')
     os.makedirs(odir, exist_ok=True)
     with open(os.path.join(odir, name + '.json'), 'w') as f:
         json.dump(out, f)
-    print('analysis_extra/' + name, kind)
+    print('analysis_grids/' + name, sorted(files))
 
 
 def pqr_xyz(ref, stride=4):
@@ -555,12 +576,12 @@ def pqr_xyz(ref, stride=4):
 
 
 if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[1] == '--analysis-grids':
+        for nm in ANALYSIS_GRIDS:
+            one_analysis_grid(nm, sys.argv[2])
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--pqr-xyz':
         pqr_xyz(sys.argv[2])
-        sys.exit(0)
-    if len(sys.argv) > 2 and sys.argv[1] == '--analysis-extra':
-        for nm in ANALYSIS_EXTRA:
-            one_analysis_extra(nm, sys.argv[2])
         sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--info':
         copy_info(sys.argv[2])

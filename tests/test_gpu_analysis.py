@@ -150,21 +150,30 @@ def test_bem_field_on_device_reproduces_reference_analysis(tmp_path):
     assert A.maximum_lines('Field', 'Ey', g, vals).splitlines() == a['log_max']
 
 
-@pytest.mark.parametrize('name', ['analysis_field_2d_x_yz_wfq_sodium', 'analysis_density_2d_x_wfq_sodium',
-                                  'analysis_field_volume_x_wfq_sodium', 'analysis_field_3d_x_wfq_sodium_plt'])
-def test_planes_volume_and_plt_on_device_reproduce_reference(name):
-    """The device kernel through the product's plane, volume and .plt writers against
-    the reference's analysis tests (as test_analysis_extra.py does with the oracle)."""
+def _grid_cases():
+    from tests import analysis_grid_cases as G
+    return G.GRIDS
+
+
+@pytest.mark.parametrize('name', _grid_cases())
+def test_grid_analyses_on_device_reproduce_reference(name):
+    """The device kernels through the product's grids and writers against every grid
+    analysis test of the reference (as test_analysis_extra.py does with the oracle)."""
     from plasmonx_b200 import analysis as A
-    from tests.test_analysis_extra import check_outputs, grid_of, load, values_by
-    a = load(name)
-    coords = np.array(a['coords_ang'])
-    p = configs.build(a['model'], coords, ['Na'], np.zeros(len(coords), np.int32), np.array([0.1]), e0=a['e0'])
-    assert np.isclose(p.r_q[0], a['rq'])
-    x = np.array(a['x'])[:, 0] + 1j * np.array(a['x'])[:, 1]
-    g = grid_of(a)
+    from tests import analysis_grid_cases as G
+    a = G.load(name)
+    g = G.grid_for(a)
     with _ctx() as ctx:
-        with Solver(p, ctx=ctx, store_t=False) as sv:
-            vals = values_by(a, g, lambda gg, t: A.field_on_grid(sv, x, a['pol'], gg, a['e0'], t),
-                             lambda gg, t: A.density_on_grid(sv, x, gg, t))
-    check_outputs(a, g, vals)
+        if a['model'] == 'bem':
+            files = G.outputs(a, g, lambda x, ip, gg, t: A.bem_field_on_grid(ctx, a['centres_ang'], x, a['e0'], ip,
+                                                                             gg, t), None)
+        else:
+            metal = {11: 'Na', 47: 'Ag', 79: 'Au'}[a['z'][0]]
+            coords = np.array(a['coords_ang'])
+            p = configs.build(a['model'], coords, [metal], np.zeros(len(coords), np.int32), np.array([0.1]),
+                              e0=a['e0'])
+            assert np.isclose(p.r_q[0], a['rq']) and (a['model'] == 'wfq' or np.isclose(p.r_mu[0], a['rmu']))
+            with Solver(p, ctx=ctx, store_t=False) as sv:
+                files = G.outputs(a, g, lambda x, ip, gg, t: A.field_on_grid(sv, x, ip, gg, a['e0'], t),
+                                  lambda x, gg, t: A.density_on_grid(sv, x, gg, t))
+    G.check(a, g, files)
