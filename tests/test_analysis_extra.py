@@ -76,3 +76,51 @@ def test_pqr_and_xyz_lines_match_reference(case):
         assert text[2:] == c['lines']
         assert A.xyz_text(dict(info, **{('centres_ang' if c['bem'] else 'coord_ang'):
                                         np.zeros((c['n'], 3))}, z=[0] * c['n'])).splitlines()[:2] == c['head']
+
+
+class _OracleFieldSolver:
+    """field_at_points answered by the oracle (the host logic of the analysis flow
+    runs on the CPU; the device kernel is checked in test_gpu_analysis.py)."""
+
+    def __init__(self, prob):
+        self.p = prob
+
+    def field_at_points(self, i_pol, x, points):
+        p = self.p
+        return field_and_density(p.coord, p.r_q[p.atom_types], p.r_mu[p.atom_types], x, p.e0, i_pol, points,
+                                 p.model == 'wfqfmu')
+
+
+def test_archive_to_cubes_on_the_host(tmp_path):
+    """A spectrum packed with save_info / save_freq, read back by read_archive, turned
+    into a problem by problem_from_info and into cube files by write_cubes: names,
+    headers and values as the reference's analysis program writes them."""
+    from plasmonx_b200 import analysis as A
+    from plasmonx_b200 import configs
+    from plasmonx_b200 import outputs as O
+    from tests.test_outputs import OracleSolver
+    p = configs.particle('Na', 'sphere', 7.0, n_freq=2, method='inversion')
+    stem = str(tmp_path / 'na')
+    kw = stem + '.kw'
+    with open(kw, 'w') as f:
+        f.write(p.to_keyword_text())
+    run = O.solve_spectrum(OracleSolver(p, kw), stem, save_freq=True, save_info=True)
+    info, sols = A.read_archive(run['paths']['tar'])
+    q = A.problem_from_info(info)
+    assert q.n_atoms == p.n_atoms and np.allclose(q.coord, p.coord, rtol=1e-15, atol=1e-13)
+    label = sorted(sols)[0]
+    grid, files = A.write_cubes(run['paths']['tar'], _OracleFieldSolver(q), info, sols[label], pols=('x', 'z'),
+                                n=(8, 7, 6), offset=4.0)
+    assert [os.path.basename(f) for f in files] == ['na-Ex-%s.cube' % label, 'na-Ez-%s.cube' % label]
+    with open(files[0]) as f:
+        lines = f.read().splitlines()
+    assert lines[0] == 'Generated by plasmonX analysis' and lines[1] == ''
+    assert int(lines[2].split()[0]) == p.n_atoms and int(lines[3].split()[0]) == 8
+    vals = np.array([float(v) for l in lines[6 + p.n_atoms:] for v in l.split()])
+    direct = A.field_on_grid(_OracleFieldSolver(q), sols[label][2]['x'], 0, grid, info['e0'])
+    assert vals.size == 8 * 7 * 6
+    assert np.allclose(vals, direct.ravel(), rtol=5.01e-6, atol=0)
+    # densities: real and imaginary cubes
+    _, dfiles = A.write_cubes(run['paths']['tar'], _OracleFieldSolver(q), info, sols[label], pols=('y',),
+                              what='density', n=(5, 5, 5), offset=3.0)
+    assert [os.path.basename(f)[-15:] for f in dfiles] == ['-densityRe.cube', '-densityIm.cube']
