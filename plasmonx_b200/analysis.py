@@ -326,6 +326,8 @@ def problem_from_info(info):
     dyn = np.array(info['dynamic'])
     # each atom takes the type of its element (the .info names the types by element)
     type_of_z = {M.atomic_number(nm): t for t, nm in enumerate(names)}
+    if len(type_of_z) != nt:
+        raise ValueError('two atom types of the .info share an element: atoms cannot be mapped to them')
     try:
         types = [type_of_z[int(v)] for v in info['z']]
     except KeyError:
