@@ -45,3 +45,29 @@ def test_missing_library_raises(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, '_lib', None)
     with pytest.raises(OSError):
         _lib.load()
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Every descriptor struct of the header has the same size and field offsets in
+    C (compiled here with gcc against include/plasmonx_b200.h) as in the ctypes
+    binding the Python host side passes."""
+    import ctypes as C
+    from plasmonx_b200 import _lib
+    structs = {'plx_geometry_desc': _lib.GeometryDesc, 'plx_bem_desc': _lib.BemDesc,
+               'plx_solve_desc': _lib.SolveDesc, 'plx_static_desc': _lib.StaticDesc}
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "plasmonx_b200.h"', 'int main(void) {']
+    for cname, cls in structs.items():
+        src.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in cls._fields_:
+            src.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
+    src.append('return 0; }')
+    c = tmp_path / 'layout.c'
+    c.write_text('\n'.join(src))
+    exe = tmp_path / 'layout'
+    subprocess.run(['gcc', '-I', os.path.join(ROOT, 'include'), str(c), '-o', str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split('\n')
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in structs.items():
+        assert got[(cname, 'sizeof')] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
