@@ -345,39 +345,77 @@ def cube_path(root, pol_name, freq_label, suffix=''):
     return '%s-%s-%s%s.cube' % (root, pol_name, freq_label, suffix)
 
 
+def _quantities(solver, info, x, i_pol, what, grid, third=0.0):
+    """[(suffix, values)] of one polarisation: |E|/E0, or the density's two parts."""
+    if info['model'] == 'bem':
+        if what != 'field':
+            raise ValueError('Density plot not allowed for BEM')
+        return [('', bem_field_on_grid(solver, info['centres_ang'], x, info['e0'], i_pol, grid, third))]
+    if what == 'field':
+        return [('', field_on_grid(solver, x, i_pol, grid, info['e0'], third))]
+    rho = density_on_grid(solver, x, grid, third)
+    return [('-densityRe', rho.real), ('-densityIm', rho.imag)]
+
+
+def _root(path, root):
+    if root is not None:
+        return root
+    return path[:-len('.tar.gz')] if path.endswith('.tar.gz') else os.path.splitext(path)[0]
+
+
 def write_cubes(path, solver, info, solution, pols=('x', 'y', 'z'), what='field', n=(30, 30, 30), offset=10.0,
-                root=None):
-    """Cube files of one frequency's solutions (a read_freq triple) for the given
-    polarisations: |E|/E0 (what='field') or the density's real and imaginary parts.
-    `solver` is a Solver of the run's geometry for atomistic runs, a Context for BEM
-    runs (field only, as in the reference)."""
+                root=None, lo=None, hi=None, fmt='cube'):
+    """The 3D files of one frequency's solutions (a read_freq triple) for the given
+    polarisations, named as plot_field_or_density names them (plot_module.f90:124-292):
+    |E|/E0 (what='field') or the density's real and imaginary parts, as cube files
+    (fmt='cube') or binary .plt files (fmt='plt'), on the atoms' box widened by
+    `offset` or on the bounds lo / hi.  `solver` is a Solver of the run's geometry for
+    atomistic runs, a Context for BEM runs (field only, as in the reference).
+    Returns the grid and the paths written."""
     variable, ev, blocks = solution
     label = O.fortran_f(ev, 12, 10).strip()
-    if root is None:
-        root = path[:-len('.tar.gz')] if path.endswith('.tar.gz') else os.path.splitext(path)[0]
+    root = _root(path, root)
     bem = info['model'] == 'bem'
-    if bem and what != 'field':
-        raise ValueError('Density plot not allowed for BEM')
     pos = info['centres_ang'] if bem else info['coord_ang']
-    grid = cubic_grid(pos, n, offset)
+    grid = cubic_grid(pos, n, offset, lo=lo, hi=hi)
     written = []
     for p in pols:
         if p not in blocks:
             continue
-        i_pol = 'xyz'.index(p)
-        pol_name = 'E' + p
-        if bem:
-            v = bem_field_on_grid(solver, info['centres_ang'], blocks[p], info['e0'], i_pol, grid)
-            outs = [(cube_path(root, pol_name, label), v)]
-        elif what == 'field':
-            v = field_on_grid(solver, blocks[p], i_pol, grid, info['e0'])
-            outs = [(cube_path(root, pol_name, label), v)]
-        else:
-            rho = density_on_grid(solver, blocks[p], grid)
-            outs = [(cube_path(root, pol_name, label, '-densityRe'), rho.real),
-                    (cube_path(root, pol_name, label, '-densityIm'), rho.imag)]
-        for fn, v in outs:
-            with open(fn, 'w') as f:
-                f.write(cube_text(grid, v, centres_ang=pos) if bem else cube_text(grid, v, info['z'], pos))
+        for suffix, v in _quantities(solver, info, blocks[p], 'xyz'.index(p), what, grid):
+            fn = cube_path(root, 'E' + p, label, suffix)
+            if fmt == 'plt':
+                fn = fn[:-len('.cube')] + '.plt'
+                with open(fn, 'wb') as f:
+                    f.write(plt_bytes(grid, v))
+            else:
+                with open(fn, 'w') as f:
+                    f.write(cube_text(grid, v, centres_ang=pos) if bem else cube_text(grid, v, info['z'], pos))
             written.append(fn)
+    return grid, written
+
+
+def write_planes(path, solver, info, solution, plane, start, n_plane=1, step=0.0, pols=('x', 'y', 'z'),
+                 what='field', n=(100, 100), offset=10.0, root=None, lo=None, hi=None):
+    """The plane .csv files of one frequency's solutions (plot_field_on_planes /
+    plot_density_on_planes, plot_module.f90:299-394): planes at start + i * step
+    (i < n_plane) of the fixed axis, named <root>-E<p>-<freq>-p-<coordinate, f20.2>.csv
+    (with -densityRe / -densityIm for the density).  Returns the grid and the paths."""
+    variable, ev, blocks = solution
+    label = O.fortran_f(ev, 12, 10).strip()
+    root = _root(path, root)
+    pos = info['centres_ang'] if info['model'] == 'bem' else info['coord_ang']
+    grid = plane_grid(pos, plane, n, offset, lo=lo, hi=hi)
+    written = []
+    for p in pols:
+        if p not in blocks:
+            continue
+        for k in range(n_plane):
+            third = start + k * step
+            tag = '-p-' + O.fortran_f(third, 20, 2).strip()
+            for suffix, v in _quantities(solver, info, blocks[p], 'xyz'.index(p), what, grid, third):
+                fn = '%s-E%s-%s%s%s.csv' % (root, p, label, tag, suffix)
+                with open(fn, 'w') as f:
+                    f.write(plane_csv_text(grid, on_plane(grid, v)))
+                written.append(fn)
     return grid, written

@@ -124,3 +124,31 @@ def test_archive_to_cubes_on_the_host(tmp_path):
     _, dfiles = A.write_cubes(run['paths']['tar'], _OracleFieldSolver(q), info, sols[label], pols=('y',),
                               what='density', n=(5, 5, 5), offset=3.0)
     assert [os.path.basename(f)[-15:] for f in dfiles] == ['-densityRe.cube', '-densityIm.cube']
+
+
+def test_plane_and_plt_writers_name_files_as_the_reference(tmp_path):
+    """write_planes / write_cubes(fmt='plt') write the files the reference's analysis
+    program writes for the same options (names from its plane and .plt tests)."""
+    from plasmonx_b200 import analysis as A
+    from plasmonx_b200 import configs
+    from plasmonx_b200 import outputs as O
+    from tests.test_outputs import OracleSolver
+    p = configs.particle('Na', 'sphere', 7.0, n_freq=1, method='inversion')
+    stem = str(tmp_path / 'na')
+    with open(stem + '.kw', 'w') as f:
+        f.write(p.to_keyword_text())
+    run = O.solve_spectrum(OracleSolver(p, stem + '.kw'), stem, save_freq=True, save_info=True)
+    info, sols = A.read_archive(run['paths']['tar'])
+    sv = _OracleFieldSolver(A.problem_from_info(info))
+    label = sorted(sols)[0]
+    g, files = A.write_planes(run['paths']['tar'], sv, info, sols[label], 'xy', 6.35, n_plane=3, step=0.5,
+                              pols=('x',), what='density', n=(6, 5))
+    names = [os.path.basename(f) for f in files]
+    assert names == ['na-Ex-%s-p-%s-density%s.csv' % (label, c, part) for c in ('6.35', '6.85', '7.35')
+                     for part in ('Re', 'Im')]
+    with open(files[0]) as f:
+        lines = f.read().splitlines()
+    assert len(lines) == 6 * 5 + 6 and lines[5] == ''
+    g3, pl = A.write_cubes(run['paths']['tar'], sv, info, sols[label], pols=('x',), n=(4, 4, 4), fmt='plt')
+    assert [os.path.basename(f) for f in pl] == ['na-Ex-%s.plt' % label]
+    assert os.path.getsize(pl[0]) == 44 + 4 * 64
