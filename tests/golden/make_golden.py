@@ -77,6 +77,30 @@ TESTS = [
     'bem_dpcm_external_brendel_bormann_ag',
 ]
 
+# tests whose geometry the reference's geom generator (a submodule absent from
+# the tree) built; their logs print it, and that printed geometry stands in
+GEOM_TESTS = [
+    'wfq_sodium_geom_rod',
+    'wfq_sodium_geom_sphere',
+    'wfq_graphene_geom_disk',
+    'wfq_graphene_geom_ribbon_main_armchair',
+    'wfq_graphene_geom_ribbon_main_zigzag',
+    'wfq_graphene_geom_ring',
+    'wfq_graphene_geom_triangle_armchair',
+    'wfq_graphene_geom_triangle_zigzag',
+    'wfqfmu_ag_geom_decahedron',
+    'wfqfmu_ag_geom_dimer_bowtie',
+    'wfqfmu_ag_geom_rod_x',
+    'wfqfmu_ag_geom_sphere',
+    'wfqfmu_ag_geom_sphere_units',
+    'wfqfmu_au_geom_cuboctahedron',
+    'wfqfmu_au_geom_dimer_z',
+    'wfqfmu_au_geom_icosahedron',
+    'wfqfmu_au_geom_paraboloid',
+    'wfqfmu_hetero_agau_geom_rod_core_shell',
+    'wfqfmu_hetero_agau_geom_sphere_core_shell',
+]
+
 NUM = r'[-+]?\d*\.\d+(?:[EeDd][-+]?\d+)?'
 
 XYZ_STUB = '''class _Atom:
@@ -220,12 +244,59 @@ def main(ref):
                        stderr=subprocess.DEVNULL)
 
 
+def log_geometry(text):
+    """(symbol, x, y, z) strings of the log's 'Input Geometry (Ang)' block
+    (print_geometry, src/target/target_module.f90:1501-1508: F20.6 in Angstrom)."""
+    rows = []
+    for line in text.split('Input Geometry (Ang)', 1)[1].splitlines():
+        p = line.split()
+        if len(p) != 5 or not p[0].isdigit():
+            if rows:
+                break
+            continue
+        assert int(p[0]) == len(rows) + 1
+        rows.append(tuple(p[1:]))
+    return rows
+
+
+def geom_front_end(ref, tdir, yaml_name, work):
+    """The keyword file of a test whose geometry the geom generator built (the
+    generator is not in the reference tree): the test's YAML with its
+    input_geometry section replaced by an external .xyz of the geometry its log
+    printed, run through the same front end (geometry from the generator and from
+    an .xyz reach the keyword writer in the same form, geom_interface.py:427-438
+    and io_operations.py:107-118)."""
+    import yaml
+    name = os.path.basename(tdir)
+    with open(os.path.join(tdir, 'reference', name + '.log')) as f:
+        rows = log_geometry(f.read())
+    src = os.path.join(work, 'src')
+    os.makedirs(src)
+    with open(os.path.join(tdir, yaml_name)) as f:
+        data = yaml.safe_load(f)
+    data['input_geometry'] = {'external xyz file': 'printed_geometry.xyz'}
+    with open(os.path.join(src, yaml_name), 'w') as f:
+        yaml.safe_dump(data, f, sort_keys=False)
+    with open(os.path.join(src, 'printed_geometry.xyz'), 'w') as f:
+        f.write('%d\n\n' % len(rows) + ''.join('%s %s %s %s\n' % r for r in rows))
+    kw = run_front_end(ref, src, yaml_name, os.path.join(work, 'run'))
+    # the keyword file carries the printed coordinates, in order
+    lines = kw.split('input_geometry', 1)[1].splitlines()[1:1 + len(rows)]
+    for line, r in zip(lines, rows):
+        p = line.split()
+        assert p[0] == r[0] and all(abs(float(a) - float(b)) <= 5e-7 for a, b in zip(p[2:5], r[1:])), (line, r)
+    return kw
+
+
 def one(name, ref):
     if True:
         tdir = os.path.join(ref, 'tests', name)
         yamls = [f for f in os.listdir(tdir) if f.endswith('.yaml')]
         with tempfile.TemporaryDirectory() as work:
-            kw = run_front_end(ref, tdir, yamls[0], work)
+            if name in GEOM_TESTS:
+                kw = geom_front_end(ref, tdir, yamls[0], work)
+            else:
+                kw = run_front_end(ref, tdir, yamls[0], work)
         odir = os.path.join(HERE, name)
         os.makedirs(odir, exist_ok=True)
         with open(os.path.join(odir, 'input.kw'), 'w') as f:
@@ -598,6 +669,12 @@ if __name__ == '__main__':
     if len(sys.argv) > 2 and sys.argv[1] == '--analysis':
         for nm in ANALYSIS:
             one_analysis(nm, sys.argv[2])
+        sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[1] == '--geom':
+        import subprocess
+        for nm in GEOM_TESTS:
+            subprocess.run([sys.executable, os.path.abspath(__file__), '--one', nm, sys.argv[2]], check=True,
+                           stderr=subprocess.DEVNULL)
         sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == '--one':
         one(sys.argv[2], sys.argv[3])

