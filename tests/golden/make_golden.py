@@ -18,6 +18,10 @@ script
      traces, when printed the full dynamic matrix, the maxima analysis and the
      frequencies recovered from backup files;
   4. copies the test's backup files (``bk/*.plasmonX.bk``, restart tests).
+With ``--geom`` it does the same for the tests whose geometry the reference's
+``geom`` generator built (a submodule that is not in the reference tree): the
+test's YAML is given an external .xyz of the geometry its log printed in place
+of the generator section.
 With ``--analysis`` it instead stores, for three analysis tests of the
 reference, the inputs of the field / density step and a sample of the cube
 file the reference wrote (``<name>/analysis.json``).  With ``--analysis-grids`` it stores, for fourteen more analysis tests
