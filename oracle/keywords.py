@@ -8,8 +8,6 @@ atomtype name`` lines open a new block, ``parameters interaction name: A->B``
 addresses the (A, B) entry of the Fermi d/s matrices, and the geometry follows
 the ``input_geometry`` line as ``name imol x y z`` (Angstrom).
 """
-import numpy as np
-
 TO_BOHR = 1.8897261254578281
 AU_TO_EV = 27.211386245981
 

@@ -134,7 +134,6 @@ def test_bem_field_on_device_reproduces_reference_analysis(tmp_path):
     with _ctx() as ctx:
         vals = A.bem_field_on_grid(ctx, np.array(a['coords_ang']), q, a['e0'], a['pol'], g)
         pts = g.points_ang()[::37] * TO_BOHR
-        import ctypes as C  # noqa: F401
         from plasmonx_b200 import _lib
         c = np.ascontiguousarray(np.array(a['coords_ang']) * TO_BOHR)
         E = np.zeros((len(pts), 3), dtype=np.complex128)

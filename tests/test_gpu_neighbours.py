@@ -37,7 +37,6 @@ def test_device_counts_match_oracle_on_reference_inputs(ctx, name):
 
 
 def _device_counts(ctx, ang, types, type_z, r0):
-    import ctypes as C
     from plasmonx_b200 import _lib
     n, nt = len(types), len(type_z)
     nb = np.zeros((n, nt), dtype=np.int32)

@@ -5,7 +5,6 @@ import threading
 import time
 
 import numpy as np
-import pytest
 
 from plasmonx_b200 import configs
 from plasmonx_b200.serving import Server, ServeRequest, footprint, request_pool, run_mix
