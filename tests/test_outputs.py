@@ -12,10 +12,11 @@ import shutil
 import numpy as np
 import pytest
 
-from oracle import model, solve as osolve
+from oracle import bem as obem, model, solve as osolve
 from plasmonx_b200 import outputs as O
 from plasmonx_b200.inputs import Problem
-from tests.conftest import GOLDEN
+from tests.conftest import GOLDEN, golden_dirs
+from tests.printed import agrees
 
 RESTART = ['wfq_sodium_restart', 'wfqfmu_ag_restart']
 
@@ -84,6 +85,43 @@ def test_restart_recovers_backups_and_prints_the_maxima(name, tmp_path):
     assert tab.shape == (len(p.freqs), 21)
     np.testing.assert_allclose(tab[:, 1:], out["results"], rtol=5.01e-6, atol=0)      # E14.6
     assert len(glob.glob(stem + '-*.freq')) == len(p.freqs) - len(out['recovered'])
+
+
+def _maxima_cases():
+    out = []
+    for name in golden_dirs():
+        with open(os.path.join(GOLDEN, name, 'expected.json')) as f:
+            if 'maxima' in json.load(f) and name not in RESTART:
+                out.append(name)
+    return out
+
+
+@pytest.mark.parametrize('name', _maxima_cases())
+def test_maxima_of_every_printed_spectrum(name):
+    """print_maxima (algorithm_module.f90:907-978) over the oracle's spectrum: the
+    states, frequencies (F10.3 eV) and values (E12.5) of every fixture whose log
+    prints a maxima block (the restart cases above go through solve_spectrum)."""
+    d = os.path.join(GOLDEN, name)
+    with open(os.path.join(d, 'expected.json')) as f:
+        exp = json.load(f)
+    kw = os.path.join(d, 'input.kw')
+    with open(kw) as f:
+        kind = dict(l.split(':', 1) for l in f.read().splitlines()
+                    if ':' in l and not l.startswith('#'))['output maxima analysis'].strip()
+    if name.startswith('bem_'):
+        b = obem.Bem(kw)
+        freqs, results = b.freqs, b.solve()['results']
+    else:
+        s = model.System.from_keywords(kw)
+        freqs = s.freqs
+        results = osolve.solve(s, method='inversion' if s.method == 'inversion' else 'gmres')['results']
+    peaks = O.maxima(freqs, np.asarray(results), kind)
+    assert exp['maxima']['n_freq'] == len(freqs)
+    assert len(peaks) == len(exp['maxima']['rows'])
+    for (state, ev, v), (pev, pv), k in zip(peaks, exp['maxima']['rows'], range(len(peaks))):
+        assert state == k + 1
+        assert O.fortran_f(ev, 10, 3).strip() == '%.3f' % pev
+        assert agrees(v, pv, 5), (ev, v, pv)
 
 
 def test_fortran_edit_descriptors():
