@@ -1,7 +1,7 @@
 """Benchmark of the per-frequency response solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config ag_sphere|na_sphere|bowtie|bem_sphere|bem_rod|fq_water|fqfmu_water]
+                    [--config ag_sphere|na_sphere|bowtie|bem_sphere|bem_rod|fq_water|fqfmu_water|field_grid]
                     [--precision fp64|mixed_bf16x3] [--n-tess 2000] [--bem-variant dpcm|iefpcm]
 
 Workload (default): the wFQFMu silver sphere -- fcc a = 4.086 A cut to a 35 A
@@ -48,6 +48,16 @@ eliminated, the Cholesky factorisation, the energy.  The CPU arm times the
 oracle's NumPy restatement (threaded LAPACK LU of the full system).  A step
 takes milliseconds: run --steps 100 so that the clock sampler sees the timed
 region.
+
+Analysis workload (--config field_grid): |E|/E0 and the plasmon density of a
+wFQFMu solution (seeded synthetic charges and dipoles; the cost does not depend
+on their values) of a 20 A silver sphere (1,961 atoms) on a --grid^3 cubic
+grid (default 100^3 = 1e6 points, the atoms' box widened by 10 A), the
+reference analysis program's field / density step.  One step = the whole grid.
+`value` is grid points/s from the kernel's CUDA-event time, `e2e` the same
+through Solver.field_at_points with host points in and host field and density
+out.  The line also times the device neighbour counts (plx_neighbour_counts)
+of the default 10,473-atom silver sphere against the host all-pairs count.
 
 BEM workloads (--config bem_sphere / bem_rod): a 10 nm sphere or a 40 x 10 nm
 prolate rod meshed into --n-tess tesserae (20 nu^2; 2000, 8000, 20480) with a
@@ -379,9 +389,140 @@ def run_static(args):
         pg.destroy_process_group()
 
 
+POINTS_METRIC = 'grid points/s (|E|/E0 and density of a wFQFMu solution)'
+# FP64 operations per (point, atom) pair of field_points on the wFQFMu path
+# (adds, multiplies and divisions, each exp / erf / sqrt counted once): a lower
+# bound on the issued FP64 work, as the transcendentals cost several operations
+POINT_PAIR_OPS = 200.0
+FP64_NOMINAL_TFLOPS = 37.0
+
+
+def points_problem(args):
+    from plasmonx_b200 import configs
+    prob = configs.particle('Ag', 'sphere', args.radius or 20.0, n_freq=1, method='iterative')
+    n = args.grid
+    return prob, n
+
+
+def points_cpu(prob, x, pts, n_sample=4000):
+    """The oracle's NumPy restatement on a bounded sample of the grid -> points/s."""
+    from oracle.analysis import field_and_density
+    rng = np.random.default_rng(3)
+    sample = pts[rng.choice(len(pts), size=min(n_sample, len(pts)), replace=False)]
+    t0 = time.perf_counter()
+    field_and_density(prob.coord, prob.r_q[prob.atom_types], prob.r_mu[prob.atom_types], x, prob.e0, 0, sample,
+                      True)
+    dt = time.perf_counter() - t0
+    return len(sample) / dt, len(sample), dt
+
+
+def run_points(args):
+    rank, world, local, pg = dist_setup()
+    from plasmonx_b200 import analysis as A
+    from plasmonx_b200 import _lib
+    from plasmonx_b200.inputs import neighbour_counts
+    from plasmonx_b200.solver import Context, Solver
+    prob, n = points_problem(args)
+    ctx = Context(local)
+    sv = Solver(prob, ctx=ctx, store_t=False)
+    x = np.random.default_rng(5).standard_normal((sv.n_var, 2)) @ np.array([1.0, 1j])
+    grid = A.cubic_grid(prob.coord_ang, (n, n, n), 10.0)
+    pts = A._points_bohr(grid)
+    P = len(pts)
+    for _ in range(args.warmup):
+        sv.field_at_points(0, x, pts)
+    barrier(pg, local)
+    ctx.profile(True)
+    launches0 = ctx.launches
+    with Clocks(local) as clk:
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            field, dens = sv.field_at_points(0, x, pts)
+        barrier(pg, local)
+        wall = time.perf_counter() - t0
+    launches = ctx.launches - launches0
+    prof = ctx.profile_read(7)
+    ctx.profile(False)
+    value, total_pts, dev_ms = job_throughput(pg, local, P * args.steps, prof['ms'])
+    e2e_s = allmax(pg, wall, local)
+    avg_ms = prof['ms'] / max(1, prof['launches'])
+    achieved = POINT_PAIR_OPS * P * prob.n_atoms / (avg_ms / 1e3) / 1e12
+    roof = {'kernel': 'field_points (one thread per point, atoms staged in shared memory)', 'bound': 'fp64',
+            'achieved': achieved, 'peak': FP64_NOMINAL_TFLOPS, 'unit': 'TFLOP/s', 'frac': achieved / FP64_NOMINAL_TFLOPS,
+            'peak_kind': 'nominal FP64 (no measured FP64 figure on this pool)',
+            'ops_per_pair': POINT_PAIR_OPS, 'pairs_per_launch': float(P) * prob.n_atoms, 'avg_launch_ms': avg_ms,
+            'bytes_per_launch': prof['bytes'] / max(1, prof['launches']), 'traffic': None}
+    # device neighbour counts of the default silver sphere against the host all-pairs count
+    big = make_problem('ag_sphere', n_freq=1)
+    nt = len(big.type_names)
+    nb = np.zeros((big.n_atoms, nt), dtype=np.int32)
+    nnb = np.zeros(big.n_atoms, dtype=np.int32)
+    ang = np.ascontiguousarray(big.coord_ang, dtype=np.float64)
+    types = np.ascontiguousarray(big.atom_types, dtype=np.int32)
+    r0 = np.asfortranarray(big.r0).ravel(order='F')
+    ctx.profile(True)
+    for _ in range(3):
+        ctx.check(ctx.lib.plx_neighbour_counts(ctx.h, big.n_atoms, nt, _lib.ptr(ang), _lib.ptr(types, _lib._ip),
+                                               _lib.ptr(big.type_z, _lib._ip), _lib.ptr(r0), _lib.ptr(nb, _lib._ip),
+                                               _lib.ptr(nnb, _lib._ip)))
+    nprof = ctx.profile_read(8)
+    ctx.profile(False)
+    neigh = {'n_atoms': int(big.n_atoms), 'kernel_ms': nprof['ms'] / max(1, nprof['launches'])}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, ns, dt = points_cpu(prob, x, pts)
+        cpu = {'value': v, 'unit': 'points/s', 'cores': 1, 'kind': 'port',
+               'sample': '%d random points of the grid through the NumPy restatement, %.1f s' % (ns, dt)}
+        t0 = time.perf_counter()
+        nb_h, nn_h = neighbour_counts(big.coord_ang, big.atom_types, big.znum, nt)
+        neigh['host_all_pairs_s'] = time.perf_counter() - t0
+        neigh['identical'] = bool(np.array_equal(nn_h, nnb) and np.array_equal(nb_h, nb.T))
+    if rank == 0:
+        line = {'metric': POINTS_METRIC, 'value': value, 'unit': 'points/s', 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': dev_ms / args.steps, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic (seeded silver sphere, seeded solution vector)',
+                'config': {'workload': 'field and density of a wFQFMu Ag sphere R=%g A on a %d^3 grid'
+                                       % (args.radius or 20.0, n),
+                           'n_atoms': int(prob.n_atoms), 'n_points': int(P),
+                           'l2': 'each step writes %.0f MB of results (larger than L2)' % (P * 64 / 1e6)},
+                'e2e': {'value': total_pts / e2e_s, 'unit': 'points/s', 'h2d_bytes_per_step': int(pts.nbytes),
+                        'd2h_bytes_per_step': int(field.nbytes + dens.nbytes)},
+                'gpu_launches': int(launches), 'roofline': roof, 'cpu_baseline': cpu, 'clocks': clk.summary(),
+                'wall_s_timed': wall, 'neighbours': neigh}
+        print(json.dumps(line), flush=True)
+    sv.close()
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def run_reference(args):
     rank, world, local, pg = dist_setup()
     if rank != 0:
+        return
+    if args.config == 'field_grid':
+        from plasmonx_b200 import analysis as A
+        prob, n = points_problem(args)
+        x = np.random.default_rng(5).standard_normal((prob.n_var, 2)) @ np.array([1.0, 1j])
+        pts = A._points_bohr(A.cubic_grid(prob.coord_ang, (n, n, n), 10.0))
+        for _ in range(args.warmup):
+            points_cpu(prob, x, pts, 100)
+        runs = [points_cpu(prob, x, pts) for _ in range(args.steps)]
+        v = float(np.mean([r[0] for r in runs]))
+        line = {'metric': POINTS_METRIC, 'value': v, 'unit': 'points/s', 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': 1000.0 * len(pts) / v, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic (seeded silver sphere, seeded solution vector)',
+                'config': {'workload': 'field and density of a wFQFMu Ag sphere R=%g A on a %d^3 grid'
+                                       % (args.radius or 20.0, n), 'n_atoms': int(prob.n_atoms),
+                           'n_points': int(len(pts))}, 'impl': 'reference',
+                'cpu_baseline': {'value': v, 'unit': 'points/s', 'cores': 1, 'kind': 'port',
+                                 'sample': '%d random grid points per step through the NumPy restatement'
+                                           % runs[0][1]},
+                'e2e': {'value': v, 'unit': 'points/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+        print(json.dumps(line), flush=True)
         return
     if args.config in ('fq_water', 'fqfmu_water'):
         prob = static_problem(args)
@@ -427,7 +568,9 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', default='ag_sphere',
-                    choices=['ag_sphere', 'na_sphere', 'bowtie', 'bem_sphere', 'bem_rod', 'fq_water', 'fqfmu_water'])
+                    choices=['ag_sphere', 'na_sphere', 'bowtie', 'bem_sphere', 'bem_rod', 'fq_water', 'fqfmu_water',
+                             'field_grid'])
+    ap.add_argument('--grid', type=int, default=100, help='grid points per axis of field_grid')
     ap.add_argument('--waters', type=int, default=0, help='water molecules of fq_water / fqfmu_water')
     ap.add_argument('--n-tess', type=int, default=2000, help='BEM tesserae (20 nu^2)')
     ap.add_argument('--bowtie-edge', type=float, default=80.0, help='prism edge (A): 80 gives 5,850 atoms, 180 ~30k')
@@ -456,6 +599,8 @@ def main():
         return run_reference(args)
     if args.config in ('fq_water', 'fqfmu_water'):
         return run_static(args)
+    if args.config == 'field_grid':
+        return run_points(args)
 
     rank, world, local, pg = dist_setup()
     from plasmonx_b200.solver import Context, Solver

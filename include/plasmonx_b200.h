@@ -369,11 +369,15 @@ int64_t plx_last_solve_launches(const plx_geom *geom);
  * category: 0 tensor-core T contraction, 1 FP64 T contraction, 2 Arnoldi
  * orthogonalisation, 3 conductance and diagonal rows of the operator,
  * 4 least squares and solution updates, 5 static matrix and right-hand-side
- * build (plx_static_solve), 6 static dense LU factorisations and solves.  For
- * the contractions it also accumulates, per launch, the algorithmic flops
- * (2 n_var^2 x real columns) and bytes (the stored T once at its storage
- * precision, the input and output columns); for 5 the bytes written, for 6 the
- * LU flops (2/3 n^3 + 2 n^2 n_rhs).  Enabling resets the counters. */
+ * build (plx_static_solve), 6 static dense LU factorisations and solves,
+ * 7 field and density at points (plx_field_at_points, plx_bem_field_at_points:
+ * the kernel alone), 8 neighbour counts (plx_neighbour_counts: the kernel
+ * alone).  For the contractions it also accumulates, per launch, the
+ * algorithmic flops (2 n_var^2 x real columns) and bytes (the stored T once at
+ * its storage precision, the input and output columns); for 5 the bytes
+ * written, for 6 the LU flops (2/3 n^3 + 2 n^2 n_rhs); for 7 and 8 the bytes
+ * the kernel must read and write once (points, atoms or tesserae, results).
+ * Enabling resets the counters. */
 plx_status plx_profile_enable(plx_ctx *ctx, int32_t on);
 /* Reads one category: accumulated time (ms), sections, flops and bytes. */
 plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,

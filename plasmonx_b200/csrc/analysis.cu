@@ -20,6 +20,7 @@ namespace plx {
 namespace {
 
 constexpr int kPts = 128;
+constexpr int kProfPoints = 7;   // plx_profile_read category of the point kernels
 constexpr double kPi32 = 5.5683279968317078453;   // pi^(3/2)
 
 __global__ void __launch_bounds__(kPts) field_points(int N, int nv, int fmu, int pol, double e0, int P,
@@ -175,11 +176,13 @@ void bem_field_at_points(plx_ctx *ctx, int n, const double *centres, const doubl
     PLX_CHECK_CUDA(cudaMemcpyAsync(d_q.p, q, 2 * (size_t)n * 8, cudaMemcpyHostToDevice, st));
     PLX_CHECK_CUDA(cudaMemcpyAsync(d_p.p, pts.data(), pts.size() * 8, cudaMemcpyHostToDevice, st));
     const double margin = 0.5 * 1.8897261254578281;   // 0.5 Angstrom in bohr
+    prof_begin(ctx);
     bem_field_points<<<n_blocks(P, kPts), kPts, 0, st>>>(n, P, pol, e0, margin, com[0], com[1], com[2], d_c.p,
                                                          reinterpret_cast<const double2 *>(d_q.p), d_p.p,
                                                          reinterpret_cast<double2 *>(d_f.p));
     ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
+    prof_end(ctx, kProfPoints, 0.0, 8.0 * (5.0 * n + 9.0 * P));
     PLX_CHECK_CUDA(cudaMemcpyAsync(field_out, d_f.p, 6 * (size_t)P * 8, cudaMemcpyDeviceToHost, st));
     PLX_CHECK_CUDA(cudaStreamSynchronize(st));
 }
@@ -187,12 +190,15 @@ void bem_field_at_points(plx_ctx *ctx, int n, const double *centres, const doubl
 void field_at_points(plx_geom *g, int pol, const double *d_x, int P, const double *d_pts, double *d_field,
                      double *d_dens) {
     plx_ctx *ctx = g->ctx;
+    prof_begin(ctx);
     field_points<<<n_blocks(P, kPts), kPts, 0, ctx->stream>>>(
         g->n_atoms, g->n_var, g->model == PLX_WFQFMU, pol, g->e0, P, g->d_pos.p, g->d_par.p,
         reinterpret_cast<const double2 *>(d_x), d_pts, reinterpret_cast<double2 *>(d_field),
         reinterpret_cast<double2 *>(d_dens));
     ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
+    // atoms (positions, widths, the solution) once, points in, field and density out
+    prof_end(ctx, kProfPoints, 0.0, 8.0 * (5.0 * g->n_atoms + 2.0 * g->n_var + 3.0 * P + 6.0 * P + 2.0 * P));
 }
 
 }  // namespace plx

@@ -665,7 +665,7 @@ plx_status plx_profile_enable(plx_ctx *ctx, int32_t on) {
         PLX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->profile = on != 0;
         ctx->prof_used = 0;
-        for (int c = 0; c < 8; ++c) {
+        for (int c = 0; c < plx_ctx::kProfCategories; ++c) {
             ctx->prof_flops[c] = ctx->prof_bytes[c] = 0.0;
             ctx->prof_launches[c] = 0;
         }
@@ -674,7 +674,7 @@ plx_status plx_profile_enable(plx_ctx *ctx, int32_t on) {
 
 plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,
                             double *bytes) {
-    if (!ctx || category < 0 || category > 6) return PLX_ERR_ARG;
+    if (!ctx || category < 0 || category >= plx_ctx::kProfCategories) return PLX_ERR_ARG;
     return guarded(ctx, [&] {
         set_device(ctx);
         PLX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));

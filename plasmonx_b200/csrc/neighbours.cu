@@ -147,11 +147,14 @@ void neighbour_counts(plx_ctx *ctx, int n, int nt, const double *coord_ang, cons
     PLX_CHECK_CUDA(cudaMemcpyAsync(d_cell.p, cell_of.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
     PLX_CHECK_CUDA(cudaMemcpyAsync(d_start.p, start.data(), start.size() * 4, cudaMemcpyHostToDevice, st));
     PLX_CHECK_CUDA(cudaMemcpyAsync(d_atoms.p, atoms.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    prof_begin(ctx);
     neighbour_kernel<<<n_blocks(n, 128), 128, 0, st>>>(n, nt, d_xyz.p, d_type.p, d_tz.p, d_r0.p, d_cell.p,
                                                        d_start.p, d_atoms.p, dims[0], dims[1], dims[2], d_nb.p,
                                                        d_nnb.p);
     ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
+    // plx_profile_read category 8: coordinates, types and cell lists in, counts out
+    prof_end(ctx, 8, 0.0, 24.0 * n + 4.0 * (3.0 * n + start.size()) + 4.0 * (double)n * (nt + 1));
     PLX_CHECK_CUDA(cudaMemcpyAsync(nb_out, d_nb.p, (size_t)n * nt * 4, cudaMemcpyDeviceToHost, st));
     PLX_CHECK_CUDA(cudaMemcpyAsync(n_nb_out, d_nnb.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
     PLX_CHECK_CUDA(cudaStreamSynchronize(st));

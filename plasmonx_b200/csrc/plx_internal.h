@@ -89,8 +89,9 @@ struct plx_ctx {
     std::vector<cudaEvent_t> prof_events;   // pairs (start, stop), reused
     std::vector<int> prof_cat;              // category of each pair
     size_t prof_used = 0;                   // events in use
-    double prof_flops[8] = {}, prof_bytes[8] = {};
-    int64_t prof_launches[8] = {};
+    static constexpr int kProfCategories = 9;  // plx_profile_read categories 0..8
+    double prof_flops[kProfCategories] = {}, prof_bytes[kProfCategories] = {};
+    int64_t prof_launches[kProfCategories] = {};
 };
 
 struct plx_geom {

@@ -40,7 +40,7 @@ class Context:
         self.check(self.lib.plx_profile_enable(self.h, int(bool(on))))
 
     PROFILE_CATEGORIES = ('tc_contraction', 'fp64_contraction', 'orthogonalisation', 'operator_rows',
-                          'least_squares', 'static_assembly', 'static_factor')
+                          'least_squares', 'static_assembly', 'static_factor', 'points', 'neighbours')
 
     def profile_read(self, category=0):
         ms, fl, by = C.c_double(), C.c_double(), C.c_double()

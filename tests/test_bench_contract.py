@@ -44,3 +44,20 @@ def test_static_reference_arm_prints_the_contract_line():
     assert d['impl'] == 'reference' and d['metric'] == bench.STATIC_METRIC and d['unit'] == 'solves/s'
     assert d['config']['n_var'] == 160 and d['value'] > 0
     assert d['e2e']['h2d_bytes_per_step'] == 0 and d['cpu_baseline']['kind'] == 'port'
+
+
+def test_field_grid_reference_arm_prints_the_contract_line():
+    """The analysis workload's reference arm: the oracle's field and density on a
+    bounded sample of a small grid."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--config',
+                          'field_grid', '--radius', '8', '--grid', '12', '--steps', '1', '--warmup', '0'],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip().startswith('{')]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d['impl'] == 'reference' and d['metric'] == bench.POINTS_METRIC and d['unit'] == 'points/s'
+    assert d['config']['n_points'] == 12 ** 3 and d['value'] > 0
+    assert d['e2e']['h2d_bytes_per_step'] == 0 and d['cpu_baseline']['kind'] == 'port'
