@@ -450,7 +450,7 @@ def run_points(args):
     achieved = POINT_PAIR_OPS * P * prob.n_atoms / (avg_ms / 1e3) / 1e12
     roof = {'kernel': 'field_points (one thread per point, atoms staged in shared memory)', 'bound': 'fp64',
             'achieved': achieved, 'peak': FP64_NOMINAL_TFLOPS, 'unit': 'TFLOP/s', 'frac': achieved / FP64_NOMINAL_TFLOPS,
-            'peak_kind': 'nominal FP64 (no measured FP64 figure on this pool)',
+            'peak_kind': 'nominal FP64 (no measured FP64 peak available)',
             'ops_per_pair': POINT_PAIR_OPS, 'pairs_per_launch': float(P) * prob.n_atoms, 'avg_launch_ms': avg_ms,
             'bytes_per_launch': prof['bytes'] / max(1, prof['launches']), 'traffic': None}
     # device neighbour counts of the default silver sphere against the host all-pairs count
