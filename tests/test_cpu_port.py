@@ -6,10 +6,10 @@ import pytest
 
 from oracle import model
 from oracle.cpu_baseline import CpuOperator
-from tests.conftest import GOLDEN
+from tests.conftest import GOLDEN, golden_dirs
 
 
-@pytest.mark.parametrize('name', ['wfqfmu_hetero_agau_inversion', 'wfqfmu_ag_inversion', 'wfq_sodium_inversion'])
+@pytest.mark.parametrize('name', golden_dirs('atomistic'))
 def test_c_port_matvec_matches_oracle(name):
     s = model.System.from_keywords(os.path.join(GOLDEN, name, 'input.kw'))
     op = model.Operator(s)
