@@ -215,7 +215,7 @@ class Solver:
             out['x'] = x.transpose(0, 2, 1).copy()     # (F, n_var, 3) like variables_w
         if tr is not None:
             out['trace'] = tr
-        if st != _lib.PLX_OK and st not in (_lib.PLX_OK,):
+        if st != _lib.PLX_OK:
             out['error'] = PlxError(st, self.lib.plx_last_error(self.ctx.h).decode())
         return out
 
