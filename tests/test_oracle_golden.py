@@ -218,3 +218,25 @@ def test_bem_oracle_matches_reference_log(name):
     if name == 'bem_ief_accurate_inversion':
         pin.exact = pin.n            # see the docstring: within the runtest tolerance only
     pin.verify()
+
+
+@pytest.mark.parametrize('name', [n for n in CASES if '_geom_' in n or n.endswith('_inversion')])
+def test_oracle_polarizability_is_reciprocal(name):
+    """Reciprocity: the induced dipole along a of a field along b equals that along b
+    of a field along a, so alpha(w) is a symmetric complex tensor (not transposed
+    conjugate): T and the Drude/Fermi conductance are symmetric in the atom pair, and
+    D(w) is diagonal.  Held, at every 50th frequency of the fixtures solved by
+    inversion, to 50 eps cond(A(w)) of the largest entry: the LU solutions carry
+    that error, and entries that vanish by the particle's symmetry show it."""
+    s, _ = load(name)
+    if s.polarization != 'all':
+        pytest.skip('one polarisation only')
+    s.freqs = s.freqs[::50]
+    if s.alpha_w is not None:
+        s.alpha_w = s.alpha_w[:, ::50]
+    out = solve.solve(s, method='inversion')
+    op = model.Operator(s)
+    for i, P in enumerate(np.asarray(out['polar'])):
+        asym = np.abs(P - P.T).max() / np.abs(P).max()
+        if asym > 1e-12:
+            assert asym <= 50 * 2.22e-16 * np.linalg.cond(op.matrix(i)), (i, asym)
