@@ -21,13 +21,14 @@ Contents
                reference's analysis step, ``src/matrix/matrix_module.f90:1140-1464``)
   static.py    static FQ / FQFMu solves and the principal-axis rotation
                (``src/forcefield/fq_module.f90``, ``fqfmu_module.f90``)
-  pairs.c      C/OpenMP restatement of the on-the-fly pair kernels
+  pairs.c      C (POSIX threads) restatement of the on-the-fly pair kernels
                (``src/matrix/matrix_module.f90:727-1125``), the timed CPU baseline
 
 Parity pins: the oracle is checked against the numbers printed in the
 reference's own regression logs and output files (``tests/*/reference/``) by
 ``tests/test_oracle_golden.py``, ``test_static_golden.py``,
-``test_analysis_golden.py`` and ``test_analysis_extra.py``; the extracted
-fixtures live in ``tests/golden/`` together with the script that extracted
-them.
+``test_analysis_golden.py``, ``test_analysis_extra.py`` and
+``test_outputs.py`` (77 of the reference's 83 regression tests); the
+extracted fixtures live in ``tests/golden/`` together with the script that
+extracted them.
 """
