@@ -603,7 +603,7 @@ def main():
                     help="Arnoldi steps per freq-solve of the reference's algorithm (CPU arm)")
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--accuracy-freqs', type=int, default=5)
-    ap.add_argument('--radius', type=float, default=None, help='smaller sphere (profiling runs only)')
+    ap.add_argument('--radius', type=float, default=None, help='sphere radius in A: a smaller ag_sphere (profiling runs only), or the field_grid sphere (default 20)')
     ap.add_argument('--n-freq', type=int, default=None, help='fewer frequencies (profiling runs only)')
     ap.add_argument('--serving-requests', type=int, default=24, help='requests in the serving leg (0: skip)')
     ap.add_argument('--serving-rate', type=float, default=20.0, help='Poisson arrival rate, requests/s')
