@@ -24,8 +24,12 @@ One step = one spectrum: every frequency solved (201 freq-solves).  `value`
 is freq-solves/s over all ranks from the library's own CUDA-event timing of
 each solve (max over ranks); `e2e` is the same metric through the public
 Python API with host buffers: geometry upload and build, frequency tables,
-solve, results back to the host.  Under torchrun every rank solves its own
-replica of the spectrum (weak scaling; no collective on the data path).
+solve, results back to the host.  Under torchrun (N ranks, one per GPU) the
+spectrum has N times the frequencies over the same window, dealt round-robin
+into one block of the workload's frequency count per rank
+(plasmonx_b200.spectrum): every rank keeps its own resident geometry and
+Krylov state and the results rows are gathered to rank 0, the only
+collective on the data path (weak scaling: fixed work per rank).
 
 Serving leg (`serving` in the line): a seeded Poisson stream of spectrum
 requests (wFQ Na spheres, wFQFMu Ag/Au spheres and rods, BEM spheres and
@@ -34,10 +38,13 @@ rods; `--serving-scale small` keeps them at 500-4k atoms or tesserae and
 footprint, resident geometries, batching, two concurrent workers), reported as
 p50/p99 request latency and freq-solves/s.
 
-`--impl reference` times the reference's algorithm on the host CPU: the
-threaded C restatement of its on-the-fly product (oracle/pairs.c) over a
-bounded sample of matrix-vector products of the same geometry, turned into
-freq-solves/s with the Arnoldi step count per frequency-solve.
+`--impl reference` times the reference's algorithm on the host CPU, per part:
+the product of the workload's mode (on-memory: zgemv of the stored complex
+matrix, timed on a row slab and scaled; on the fly: the threaded C port of the
+reference's pair loops, oracle/pairs.c; BEM: dense D x) over at least 20
+products per run, and the CGS2 orthogonalisation at the mean basis size, then
+composes them into freq-solves/s with the Arnoldi step count per
+frequency-solve (marked extrapolated: a whole spectrum takes hours).
 
 Static workloads (--config fq_water / fqfmu_water): the static FQ / FQFMu solve
 (ground state: charges and energy) of a seeded cluster of --waters rigid water
@@ -80,12 +87,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = 'freq-solves/s at <=1e-6 rel sigma_abs err'
 PEAKS_FALLBACK = {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustained': 1400.0}
-# Arnoldi steps per frequency-solve of the default workload (mean over the 201
-# frequencies), measured with the FP64 GMRES on B200; used to turn the CPU
-# arm's timed matrix-vector products into freq-solves/s.
-# (the reference's GMRES, i.e. the plain FP64 form, at the bench's input tolerance 1e-12:
-# 335.6 mean Arnoldi steps per frequency on the default silver sphere)
-STEPS_PER_SOLVE = 335.6
+# Arnoldi steps per frequency-solve of the reference's GMRES (the plain FP64
+# form) at the bench's input tolerance 1e-12, mean over each workload's
+# spectrum, measured on B200; used to turn the CPU arm's timed products and
+# orthogonalisations into freq-solves/s.
+STEPS_PER_SOLVE = {'ag_sphere': 335.6, 'na_sphere': 60.0, 'bowtie': 600.0, 'bem_sphere': 60.0, 'bem_rod': 60.0}
 # measured DRAM bytes / algorithmic bytes of the tensor-core contraction (ncu, small case)
 TRAFFIC_RATIO = 1.004
 
@@ -122,6 +128,28 @@ def is_bem(prob):
     return getattr(prob, 'triangles', None) is not None
 
 
+def oracle_fixture(args, prob):
+    """The oracle's solutions of this workload at five frequencies, when
+    tests/golden/large holds them (default silver sphere, 80 A bow-tie), checked
+    against the geometry before use; None otherwise."""
+    name = {'ag_sphere': 'ag_sphere_r35', 'bowtie': 'agau_bowtie_e80'}.get(args.config)
+    if name is None or (args.config == 'ag_sphere' and args.radius not in (None, 35.0)) or \
+            (args.config == 'bowtie' and args.bowtie_edge != 80.0) or len(prob.freqs) != 201:
+        return None
+    path = os.path.join(ROOT, 'tests', 'golden', 'large', name + '.json')
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        fx = json.load(f)
+    c = np.asarray(prob.coord, dtype=np.float64)
+    if int(prob.n_atoms) != fx['geometry']['n_atoms'] or \
+            abs(float(np.sum(c)) - fx['geometry']['coord_sum']) > 1e-9 * max(1.0, fx['geometry']['coord_abs_sum']):
+        return None
+    fx['reference'] = ("oracle fixture tests/golden/large/%s.json: the reference GMRES restated on the CPU "
+                       "(C port of the on-the-fly product) to a relative residual of %g" % (name, fx['rel_tol']))
+    return fx
+
+
 def workload_desc(name, prob):
     if is_bem(prob):
         return {'workload': 'BEM %s %s, %s Green function' % (prob.variant.upper(),
@@ -138,7 +166,9 @@ def workload_desc(name, prob):
                          'bowtie': 'wFQFMu Ag-Au bow-tie'}[name],
             'n_atoms': int(prob.n_atoms), 'n_var': int(prob.n_var), 'n_freq': int(len(prob.freqs)),
             'polarization': prob.polarization, 'mode': prob.method, 'tolerance': prob.tolerance_input,
-            'l2': 'inputs larger than L2 (stored T %.1f GB)' % (8.0 * prob.n_var ** 2 / 1e9)}
+            'l2': ('inputs larger than L2 (stored T %.1f GB)' % (8.0 * prob.n_var ** 2 / 1e9))
+            if 8.0 * prob.n_var ** 2 > 126e6 else
+            'stored T %.1f MB fits in L2 (not flushed between steps)' % (8.0 * prob.n_var ** 2 / 1e6)}
 
 
 class Clocks:
@@ -251,46 +281,106 @@ def job_throughput(pg, local, solves, device_ms):
     return total / (slowest / 1000.0), total, slowest
 
 
-def cpu_sample_bem(prob, n_mv, steps_per_solve):
-    """Time n_mv dense D x products (threaded BLAS) of the oracle's BEM operator."""
-    import tempfile
-    from oracle import bem as obem
-    with tempfile.TemporaryDirectory() as d:
-        o = obem.Bem(prob.write_keyword_files(d, 'bench'))
-    D = np.ascontiguousarray(o.D)
-    rng = np.random.default_rng(0)
-    x = rng.standard_normal(o.n_var) + 1j * rng.standard_normal(o.n_var)
+def _blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        return max([d.get('num_threads', 1) for d in threadpool_info() if d.get('user_api') == 'blas'] or [1])
+    except Exception:
+        return os.cpu_count() or 1
 
-    def matvec(i, v):
-        # the real D applied to the real and imaginary parts at once (one n x 2 GEMM)
-        Y = D @ np.stack([v.real, v.imag], axis=1)
-        return Y[:, 0] + 1j * Y[:, 1] + o.z(i) * v
 
+def _time_products(matvec, x, n_min, budget_s):
+    """Mean seconds per product over at least n_min products (more while the budget lasts)."""
     matvec(0, x)
-    t0 = time.perf_counter()
-    for k in range(n_mv):
-        x = matvec(k % len(o.freqs), x)
+    done, t0 = 0, time.perf_counter()
+    while done < n_min or (time.perf_counter() - t0 < budget_s and done < 200):
+        x = matvec(done, x)
         x /= np.linalg.norm(x)
-    dt = (time.perf_counter() - t0) / n_mv
-    return 1.0 / (dt * steps_per_solve), dt, os.cpu_count()
+        done += 1
+    return (time.perf_counter() - t0) / done, done
 
 
-def cpu_sample(prob, n_mv, n_threads, steps_per_solve):
-    """Time n_mv on-the-fly products of the C restatement; return freq-solves/s."""
+def _time_orthogonalisation(n, j, reps=5):
+    """Seconds of one Arnoldi orthogonalisation of the reference at basis size j:
+    classical Gram-Schmidt with one re-orthogonalisation, four zgemv over the
+    n x j basis (gmres_module.f90:123-142; modified Gram-Schmidt below j = 25
+    moves the same bytes as 2 j vector operations)."""
+    rng = np.random.default_rng(1)
+    V = np.full((n, max(j, 1)), 0.5 + 0.25j)
+    V[:, 0] = rng.standard_normal(n)
+    w = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        h = V.conj().T @ w
+        w = w - V @ h
+        t = V.conj().T @ w
+        w = w - V @ t
+        w /= np.linalg.norm(w)
+    return (time.perf_counter() - t0) / reps
+
+
+def cpu_reference(prob, steps_per_solve, n_min=20, budget_s=20.0):
+    """The reference's per-frequency GMRES on the host cores, timed per part and
+    composed into freq-solves/s (extrapolated: a whole spectrum takes hours).
+
+    Per Arnoldi step the reference does one product and one orthogonalisation;
+    a freq-solve of s steps does s products plus one for the true residual, and
+    s orthogonalisations whose mean basis size is (s + 1) / 2.  The product is
+      on-memory atomistic: zgemv of the stored complex n x n matrix
+        (gmres_module.f90:111-119 on matrix_iterative, algorithm_module.f90:356-358),
+        timed on a row slab of that matrix and scaled to n rows;
+      on-the-fly atomistic: the C port of product_q_block_x / product_mu_block_x
+        and the conductance rows (oracle/pairs.c);
+      BEM: the dense complex D x of the oracle (threaded BLAS).
+    """
+    s_steps = float(steps_per_solve)
+    n = int(prob.n_var)
     if is_bem(prob):
-        return cpu_sample_bem(prob, max(n_mv, 20), steps_per_solve)
-    from oracle import keywords, model
-    from oracle.cpu_baseline import CpuOperator
-    s = model.System.from_keywords(keywords.read_keyword_text(prob.to_keyword_text()))
-    op = CpuOperator(s, n_threads=n_threads)
-    rng = np.random.default_rng(0)
-    x = rng.standard_normal(s.n_var) + 1j * rng.standard_normal(s.n_var)
-    t0 = time.perf_counter()
-    for k in range(n_mv):
-        x = op.matvec(k % len(s.freqs), x)
-        x /= np.linalg.norm(x)
-    dt = (time.perf_counter() - t0) / n_mv
-    return 1.0 / (dt * steps_per_solve), dt, op.n_threads
+        import tempfile
+        from oracle import bem as obem
+        with tempfile.TemporaryDirectory() as d:
+            o = obem.Bem(prob.write_keyword_files(d, 'bench'))
+        D = np.ascontiguousarray(o.D).astype(np.complex128)
+
+        def matvec(i, v):
+            return D @ v + o.z(i % len(o.freqs)) * v
+        x = np.random.default_rng(0).standard_normal(n) + 0j
+        t_mv, done = _time_products(matvec, x, n_min, budget_s)
+        what = 'dense complex D x (zgemv, threaded BLAS) of the %d-tessera operator' % n
+        cores = _blas_threads()
+    elif prob.method == 'iterative':
+        rows = min(n, max(1024, int(2.0e9 // (16 * n))))
+        A = np.full((rows, n), 0.5 + 0.25j)
+        A[:, 0] = 1.0
+
+        def matvec(i, v):
+            y = v.copy()
+            y[:rows] = A @ v
+            return y
+        x = np.random.default_rng(0).standard_normal(n) + 0j
+        t_slab, done = _time_products(matvec, x, n_min, budget_s)
+        t_mv = t_slab * n / rows
+        what = ('zgemv of the stored complex matrix (on-memory mode), a %d-row slab of the %d x %d matrix timed and '
+                'scaled to %d rows' % (rows, n, n, n))
+        cores = _blas_threads()
+        del A
+    else:
+        from oracle import keywords, model
+        from oracle.cpu_baseline import CpuOperator
+        s = model.System.from_keywords(keywords.read_keyword_text(prob.to_keyword_text()))
+        op = CpuOperator(s)
+        x = np.random.default_rng(0).standard_normal(n) + 1j * np.random.default_rng(1).standard_normal(n)
+        t_mv, done = _time_products(lambda i, v: op.matvec(i % len(s.freqs), v), x, min(n_min, 5), budget_s)
+        what = "on-the-fly A x of the C port of the reference's pair loops"
+        cores = op.n_threads
+    j_mid = max(1, int(round((s_steps + 1) / 2)))
+    t_orth = _time_orthogonalisation(n, j_mid)
+    t_solve = (s_steps + 1) * t_mv + s_steps * t_orth
+    return {'value': 1.0 / t_solve, 'unit': 'freq-solves/s', 'cores': int(cores), 'kind': 'port',
+            'extrapolated': True,
+            'sample': '%s: %d products timed, %.4f s each; CGS2 orthogonalisation at basis size %d: %.4f s; '
+                      'x %.1f Arnoldi steps per freq-solve' % (what, done, t_mv, j_mid, t_orth, s_steps),
+            'product_s': t_mv, 'orthogonalisation_s': t_orth, 'steps_per_solve': s_steps}
 
 
 STATIC_METRIC = 'static solves/s (ground state: charges and energy, FP64)'
@@ -554,24 +644,23 @@ def run_reference(args):
                 'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
         print(json.dumps(line), flush=True)
         return
-    prob = make_problem(args.config, n_tess=args.n_tess, bem_variant=args.bem_variant)
-    sps = args.steps_per_solve
-    vals = []
+    prob = make_problem(args.config, n_tess=args.n_tess, bem_variant=args.bem_variant, bowtie_edge=args.bowtie_edge)
+    prob.tolerance_input = args.tolerance
+    sps = args.steps_per_solve or STEPS_PER_SOLVE[args.config]
+    per_step = max(2, -(-20 // max(1, args.steps)))      # at least 20 products over the run
     for _ in range(args.warmup):
-        cpu_sample(prob, 1, 0, sps)
-    for _ in range(args.steps):
-        v, dt, nthr = cpu_sample(prob, args.cpu_matvecs, 0, sps)
-        vals.append(v)
-    v = float(np.mean(vals))
+        cpu_reference(prob, sps, n_min=1, budget_s=0.0)
+    runs = [cpu_reference(prob, sps, n_min=per_step, budget_s=2.0) for _ in range(args.steps)]
+    v = float(np.mean([r['value'] for r in runs]))
+    cpu = dict(runs[-1], value=v)
+    cpu['sample'] = ('%d timed steps; last: ' % len(runs)) + runs[-1]['sample']
     line = {'metric': METRIC, 'value': v, 'unit': 'freq-solves/s', 'n_gpus': world, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': 1000.0 / v * len(prob.freqs), 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': workload_desc(args.config, prob), 'impl': 'reference',
-            'cpu_baseline': {'value': v, 'unit': 'freq-solves/s', 'cores': nthr, 'kind': 'port',
-                             'sample': ('%d dense D x products (threaded BLAS) per step' % max(args.cpu_matvecs, 20)
-                                        if is_bem(prob) else
-                                        '%d on-the-fly A x products of the C restatement per step'
-                                        % args.cpu_matvecs) + ', x %.0f Arnoldi steps per freq-solve' % sps},
+            'warmup': args.warmup, 'ms_per_step': 1000.0 / v * len(prob.freqs), 'ms_per_step_extrapolated': True,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': dict(workload_desc(args.config, prob), precision='fp64 (the reference algorithm)'),
+            'impl': 'reference', 'cpu_baseline': cpu,
+            'note': 'one step = one spectrum; ms_per_step is extrapolated from the products and '
+                    'orthogonalisations timed in each step (a whole spectrum takes hours on the host)',
             'e2e': {'value': v, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
@@ -599,7 +688,7 @@ def main():
     ap.add_argument('--inner-tol', type=float, default=0.0)
     ap.add_argument('--e2e-steps', type=int, default=1)
     ap.add_argument('--cpu-matvecs', type=int, default=2)
-    ap.add_argument('--steps-per-solve', type=float, default=STEPS_PER_SOLVE,
+    ap.add_argument('--steps-per-solve', type=float, default=None,
                     help="Arnoldi steps per freq-solve of the reference's algorithm (CPU arm)")
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--accuracy-freqs', type=int, default=5)
@@ -619,25 +708,51 @@ def main():
 
     rank, world, local, pg = dist_setup()
     from plasmonx_b200.solver import Context, Solver
-    prob = make_problem(args.config, n_freq=args.n_freq, radius=args.radius, n_tess=args.n_tess,
+    from plasmonx_b200.spectrum import solve_partitioned
+    # N ranks: one spectrum of N times the frequencies over the same window, dealt
+    # out in blocks of one workload's frequencies per rank, results gathered to rank 0
+    base_f = args.n_freq or {'ag_sphere': 201, 'na_sphere': 61, 'bowtie': 201}.get(args.config, 301)
+    prob = make_problem(args.config, n_freq=base_f * world, radius=args.radius, n_tess=args.n_tess,
                         bem_variant=args.bem_variant, bowtie_edge=args.bowtie_edge)
-    if args.inner_krylov == 0 and args.config == 'bowtie':
-        # the gap-coupled alloy converges slowly: a 256-vector inner basis (re-orthogonalised)
-        # beats restarts every 64 steps by 1.6x (measured sweep 64 / 128 / 256)
-        args.inner_krylov = 256
     prob.tolerance_input = args.tolerance
     prob.tol = args.tolerance * np.sqrt(prob.n_var)
-    F = len(prob.freqs)
     ctx = Context(local)
     solver = Solver(prob, ctx=ctx, store_t=prob.method != 'iterative on the fly')
+    gather_dev = 'cuda:%d' % local if pg is not None and pg.get_backend() == 'nccl' else 'cpu'
+    full_freqs, full_aw = prob.freqs, prob.alpha_w
+    tuning = None
+    if args.inner_krylov == 0 and args.precision.startswith('mixed'):
+        # the inner basis length from a short sweep on a few of the grid's frequencies
+        # (plasmonx_b200.tuning), cached per geometry; not part of the timed region
+        from plasmonx_b200.tuning import Tuner
+        tuner = Tuner()
+        chosen = tuner.settings(solver, args.config, full_freqs, full_aw, precision=args.precision,
+                                mode=prob.method, tol=prob.tol)
+        args.inner_krylov = chosen['inner_krylov']
+        tuning = tuner.records[args.config]
+    gathered = {}
 
     def step():
-        out = solver.solve(precision=args.precision, inner_krylov=args.inner_krylov, inner_tol=args.inner_tol)
+        part = solve_partitioned(solver, full_freqs, full_aw, pg, device=gather_dev, precision=args.precision,
+                                 inner_krylov=args.inner_krylov, inner_tol=args.inner_tol)
+        out = part['local']
         if 'error' in out:
             raise out['error']
+        if part['status'] is not None:
+            gathered.update(n_freq=int(len(part['status'])), status_ok=bool(np.all(part['status'] == 0)))
         return out
 
-    for _ in range(args.warmup):
+    step_out = step()
+    F = len(step_out['results'])          # this rank's block (the whole grid on one rank)
+    if world > 1:
+        # the single-rank legs below (plain FP64 arm, accuracy, CPU, serving) use the rank's block
+        blk = np.arange(rank, len(prob.freqs), world)
+        prob.freqs = prob.freqs[blk]
+        if prob.alpha_w is not None:
+            prob.alpha_w = prob.alpha_w[:, blk]
+        args.no_fp64_compare, args.accuracy_freqs, args.serving_requests = True, 0, 0
+
+    for _ in range(max(0, args.warmup - 1)):
         step()
     barrier(pg, local)
     ctx.profile(True)
@@ -678,10 +793,19 @@ def main():
                 'arnoldi_steps_mean': float(np.mean(o64['steps'][:, 0])), 'status_ok': bool((o64['status'] == 0).all()),
                 'frequencies_timed': int(nf64)}
 
-    # accuracy: sigma_abs against an FP64 refinement solved to 1e-12 relative
-    # residual, on a subset of the frequencies
+    # accuracy: sigma_abs against the oracle's fixtures of this workload (the
+    # reference GMRES restated on the CPU, relative residual 1e-12) when there are
+    # some, else against an FP64 refinement on the device, on a subset of frequencies
     acc = None
-    if args.accuracy_freqs > 0:
+    fixture = oracle_fixture(args, prob) if world == 1 else None
+    if fixture is not None and args.accuracy_freqs > 0:
+        idx = np.asarray(fixture['freq_index'])
+        sref = np.array(fixture['results'])[:, 9]
+        acc = {'freqs': [int(i) for i in idx], 'reference': fixture['reference'],
+               'headline_max_rel_err': float(np.max(np.abs(out['results'][idx, 9] - sref) / np.abs(sref)))}
+        if fp64 is not None and sub is None:
+            fp64['sigma_abs_max_rel_err'] = float(np.max(np.abs(o64['results'][idx, 9] - sref) / np.abs(sref)))
+    elif args.accuracy_freqs > 0:
         idx = np.linspace(0, F - 1, min(args.accuracy_freqs, F)).round().astype(int)
         b = solver.rhs(int(idx[0]), prob.pol_mask)
         sref, ref_status = [], []
@@ -759,14 +883,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         # the CPU baseline runs the reference's algorithm: its step count is the plain
         # FP64 GMRES's of this run when measured
-        sps = fp64['arnoldi_steps_mean'] if fp64 is not None else args.steps_per_solve
-        v, dt, nthr = cpu_sample(prob, args.cpu_matvecs, 0, sps)
-        what = ('%d dense D x products of the oracle (threaded BLAS, %.4f s each)' % (max(args.cpu_matvecs, 20), dt)
-                if is_bem(prob) else
-                '%d on-the-fly A x products of the C restatement (%.2f s each)' % (args.cpu_matvecs, dt))
-        cpu = {'value': v, 'unit': 'freq-solves/s', 'cores': nthr, 'kind': 'port',
-               'sample': what + " x %.1f Arnoldi steps per freq-solve (the reference's GMRES, plain FP64 "
-                                "form of this run)" % sps}
+        sps = fp64['arnoldi_steps_mean'] if fp64 is not None and sub is None else \
+            (args.steps_per_solve or STEPS_PER_SOLVE[args.config])
+        cpu = cpu_reference(prob, sps)
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': 'freq-solves/s', 'n_gpus': world,
                 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
@@ -776,7 +895,10 @@ def main():
                 'data': ('synthetic (seeded geodesic surface, Drude-Lorentz eps)' if is_bem(prob) else
                          'synthetic (seeded fcc lattice, reference default parameters)'),
                 'config': dict(workload_desc(args.config, prob), precision=args.precision,
-                               inner_krylov=args.inner_krylov or 64),
+                               inner_krylov=args.inner_krylov or 64,
+                               **({'partition': 'one spectrum of %d frequencies over the window, dealt round-robin '
+                                                '(%d per rank), results gathered to rank 0' % (len(full_freqs), F),
+                                   'gathered': gathered} if world > 1 else {})),
                 'e2e': {'value': e2e_val, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': int(h2d),
                         'd2h_bytes_per_step': int(F * (20 * 8 + 9 * 16 + 4 + 12))},
                 'gpu_launches': int(launches), 'roofline': roof, 'cpu_baseline': cpu,
@@ -785,6 +907,7 @@ def main():
                 'sigma_abs_max_rel_err': None if acc is None else acc['headline_max_rel_err'],
                 'accuracy': acc, 'fp64_plain_gmres': fp64,
                 'speedup_vs_fp64_plain': None if fp64 is None else value / fp64['value'],
+                'tuning': tuning,
                 'arnoldi_steps': {'mean': float(np.mean(np.concatenate(steps_hist))),
                                   'max': int(np.max(np.concatenate(steps_hist)))},
                 'serving': serving}

@@ -274,8 +274,11 @@ plx_status plx_contract(plx_geom *geom, int32_t count, const double *X, double *
  * split-K partials (k-chunks x count x n_var) must fit in it, otherwise the
  * call returns PLX_ERR_ARG.  The first call on a device looks up the array's
  * device address, so make that first call before any stream capture.  All
- * calls share the array: calls whose kernels overlap on the GPU race.  Runs on
- * the context's stream and returns when S is written. */
+ * calls share the array: calls whose kernels overlap on the GPU race.  The
+ * kernels run on the context's own stream, which is not ordered after the
+ * caller's streams: d_X must be completely written on the device before the
+ * call (synchronise the stream that wrote it).  The call synchronises the
+ * context's stream and returns when S is written. */
 plx_status plx_contract_noalloc(plx_geom *geom, int32_t count, const double *d_X, double *d_S);
 
 /* ---- static FQ / FQFMu ---------------------------------------------------- */
@@ -382,6 +385,17 @@ plx_status plx_profile_enable(plx_ctx *ctx, int32_t on);
 /* Reads one category: accumulated time (ms), sections, flops and bytes. */
 plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,
                             double *bytes);
+
+/* ---- failure handling ------------------------------------------------------ */
+
+/* Number of polls after which a pipeline wait inside the tensor-core kernels
+ * (a copy or a matrix product that does not arrive) gives up; 0 restores the
+ * default of 2^22 polls (seconds).  A kernel whose wait runs out lets every
+ * copy and product it has started finish, frees its tensor memory, returns,
+ * and the call reports PLX_ERR_CUDA ("... timed out waiting on its
+ * pipeline"); the context stays usable.  No counterpart in the reference (its
+ * CPU code has no such waits); tests shorten it to exercise that path. */
+plx_status plx_set_wait_limit(plx_ctx *ctx, uint32_t polls);
 
 #ifdef __cplusplus
 }

@@ -38,10 +38,14 @@ def zrot(x, y, c, s):
     return c * x + s * y, c * y - np.conj(s) * x
 
 
-def gmres(matvec, b, tol, restart, max_iter=1, trace=None):
+def gmres(matvec, b, tol, restart, max_iter=1, trace=None, snapshots=None):
     """Solve A x = b.  ``matvec(v)`` returns A v (including the diagonal shift).
 
     Returns (x, n_steps).  ``trace`` (a list) receives the logged residuals.
+    ``snapshots`` (a dict {level: None}) receives, for every absolute residual
+    level, the least-squares iterate of the first step whose logged residual is
+    below it (no true-residual check): the convergence history that shows how
+    far a solution at ``tol`` is from the ones before it.
     """
     n = b.shape[0]
     m = min(restart, n)
@@ -82,6 +86,11 @@ def gmres(matvec, b, tol, restart, max_iter=1, trace=None):
         resid = abs(H[j + 1, m])
         if trace is not None:
             trace.append(resid)
+        if snapshots is not None:
+            for level in snapshots:
+                if snapshots[level] is None and resid < level:
+                    y = solve_triangular(H[:j + 1, :j + 1], H[:j + 1, m], lower=False)
+                    snapshots[level] = x + V[:, :j + 1] @ y
         if resid < tol:
             y = solve_triangular(H[:j + 1, :j + 1], H[:j + 1, m], lower=False)
             x = x + V[:, :j + 1] @ y

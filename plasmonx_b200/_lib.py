@@ -23,7 +23,7 @@ EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
            'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points',
            'plx_static_n_var', 'plx_static_solve', 'plx_principal_axes', 'plx_neighbour_counts',
-           'plx_bem_field_at_points', 'plx_ctx_launches']
+           'plx_bem_field_at_points', 'plx_ctx_launches', 'plx_set_wait_limit']
 STATIC_FF = {'fq': 0, 'fqfmu': 1}
 KERNEL = {'coulomb': 0, 'ohno': 1, 'gaussian': 2}
 STATIC_WHAT = {'energy': 0, 'static': 1}
@@ -116,6 +116,7 @@ def load():
     lib.plx_principal_axes.argtypes = [C.c_int32, _ip, _dp, _dp, _dp]
     lib.plx_profile_enable.argtypes = [vp, C.c_int32]
     lib.plx_profile_read.argtypes = [vp, C.c_int32, _dp, C.POINTER(C.c_int64), _dp, _dp]
+    lib.plx_set_wait_limit.argtypes = [vp, C.c_uint32]
     _lib = lib
     return lib
 

@@ -591,6 +591,10 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
                         rr.inner_contraction = desc->precision == PLX_MIXED_BF16X3 ? Contraction::TC3
                                                : desc->precision == PLX_MIXED_BF16 ? Contraction::TC1
                                                                                    : rr.outer_contraction;
+                        // tensor-core inner solves restart on their own residual (one cheap
+                        // product) up to 8 cycles before an FP64 residual; an FP64 inner solve's
+                        // restart product would cost as much as the outer one
+                        rr.max_cycles = rr.inner_contraction == rr.outer_contraction ? 1 : 8;
                         RefineResult rres;
                         solve_refined(g, rr, Bg.p, Xg.p, rres);
                         res.status = rres.status;
@@ -672,6 +676,15 @@ plx_status plx_profile_enable(plx_ctx *ctx, int32_t on) {
     });
 }
 
+plx_status plx_set_wait_limit(plx_ctx *ctx, uint32_t polls) {
+    if (!ctx) return PLX_ERR_ARG;
+    return guarded(ctx, [&] {
+        set_device(ctx);
+        PLX_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->wait_limit = polls ? polls : plx_ctx::kDefaultWaitLimit;
+    });
+}
+
 plx_status plx_profile_read(plx_ctx *ctx, int32_t category, double *ms, int64_t *launches, double *flops,
                             double *bytes) {
     if (!ctx || category < 0 || category >= plx_ctx::kProfCategories) return PLX_ERR_ARG;
@@ -711,7 +724,8 @@ plx_status plx_contract(plx_geom *g, int32_t count, const double *X, double *S, 
         contract_t(g, padded / 2, dX.p, dS.p, kinds[how]);
         PLX_CHECK_CUDA(cudaMemcpyAsync(S, dS.p, (size_t)count * n * 8, cudaMemcpyDeviceToHost, g->ctx->stream));
         PLX_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
-        if (how >= 2 && tc_error(g)) throw Error(PLX_ERR_CUDA, "tensor-core contraction timed out");
+        if (how >= 2 && tc_error(g))
+            throw Error(PLX_ERR_CUDA, "tensor-core contraction timed out waiting on its pipeline");
     });
 }
 

@@ -14,6 +14,9 @@
 // has to start at zero.  All calls on a device share the one array and it
 // keeps the last call's contents: two calls whose kernels overlap on the GPU
 // (different streams, host threads or processes sharing a context) race on it.
+// The kernels run on the context's own stream, which is not ordered after the
+// caller's streams: the caller finishes writing X on the device before the
+// call.  The call waits for its kernels, so S is complete when it returns.
 #include <mutex>
 
 #include "plx_internal.h"
@@ -89,5 +92,12 @@ extern "C" plx_status plx_contract_noalloc(plx_geom *g, int32_t count, const dou
     } catch (const plx::Error &e) {
         ctx->last_error = e.msg;
         return e.code;
+    } catch (const std::exception &e) {
+        // a failed lock or message allocation must not leave the C ABI as an exception
+        try {
+            ctx->last_error = e.what();
+        } catch (...) {
+        }
+        return PLX_ERR_ARG;
     }
 }

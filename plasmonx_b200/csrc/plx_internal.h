@@ -84,6 +84,10 @@ struct plx_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t launches = 0;  // kernels launched by the library since creation
+    // polls of every bounded pipeline wait in the tensor-core kernels before
+    // they give up (plx_set_wait_limit)
+    static constexpr uint32_t kDefaultWaitLimit = 1u << 22;
+    uint32_t wait_limit = kDefaultWaitLimit;
     // contraction profiling (plx_profile_enable)
     bool profile = false;
     std::vector<cudaEvent_t> prof_events;   // pairs (start, stop), reused
@@ -158,8 +162,9 @@ struct plx_geom {
     plx::DevArray<int32_t> d_xcol, d_xtj;         // position of j in J, type of j
     plx::DevArray<double> d_xkt;                  // K_ji
     plx::DevArray<double> d_fold_work;            // [R][fold_rows] output of the folded contraction
-    // k-split partial sums of the tensor-core contraction ([splits][R][n_var])
-    plx::DevArray<double> d_tcpart;
+    // FP32 partial sums of the k-pieces of the tensor-core contraction's split
+    // tiles ([piece][column][256 rows])
+    plx::DevArray<float> d_tcpart;
     plx::DevArray<int> d_tc_err;
     // diagonal of blockdiag(Kop, I) T on the charge rows, frequency independent parts:
     // a_i = sum_j K_ij (T_ij - T_ii), b_i,t = sum_{j of type t} K_ji (T_ij - T_ii)
@@ -278,6 +283,9 @@ struct RefineRequest {
     Contraction outer_contraction = Contraction::FP64;
     bool jacobi = true;      // diagonal right preconditioning of the inner solves
     bool single_pass_gs = true;   // tensor-core inner solves: one classical Gram-Schmidt pass
+    // inner GMRES(inner_m) cycles per outer step: a cycle that ends on the full basis
+    // restarts from the inner residual (inner contraction) before an FP64 residual
+    int max_cycles = 1;
 };
 struct RefineResult {
     std::vector<int32_t> status, inner_steps, outer;

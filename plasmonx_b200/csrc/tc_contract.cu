@@ -18,9 +18,18 @@
 // epilogue.  Operand tiles are 32 elements (64 bytes) deep along k and are
 // loaded by TMA with the 64-byte swizzle that the UMMA descriptors describe;
 // the small stages allow 4-6 of them in flight.
-// Every wait on an mbarrier is bounded; a CTA that gives up records an error
-// code, waits (bounded) for its outstanding loads, frees its tensor memory and
-// returns.
+// Every wait on an mbarrier is bounded.  The pipeline waits use the context's
+// limit (plx_set_wait_limit); a CTA whose wait runs out records an error code
+// and gives up, in this order: the MMA issuer still commits `done`, which
+// arrives only when every MMA it has issued has finished; all threads wait for
+// it, so no MMA reads shared memory or writes tensor memory after that point;
+// the producer then waits for the loads it has issued to land, so no copy
+// writes into shared memory after the CTA exits; then the tensor memory is
+// freed and the CTA returns without storing a result.  These clean-up waits
+// use their own, long limit (kDrainLimit), never the pipeline limit.  If one of
+// them runs out as well (a copy or an MMA that never completes: the hardware
+// has stopped answering) the CTA records that error too and exits anyway; the
+// call then fails and nothing it wrote is used.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -38,7 +47,7 @@ constexpr int kBM = 2 * kUM;      // rows of T per CTA: two accumulators share e
 constexpr int kBK = 32;           // k per stage (64 bytes of BF16: the 64-byte swizzle atom)
 constexpr int kLdAlign = 64;      // k padding of the split operands (zeros)
 constexpr int kUmmaK = 16;        // k per tcgen05.mma (kind::f16)
-constexpr uint32_t kSpinLimit = 1u << 22;   // bounded waits (seconds at most)
+constexpr uint32_t kDrainLimit = 1u << 22;  // clean-up waits after an abort (seconds at most)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -65,10 +74,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: returns false (and records `code`) when the limit is reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
-    for (uint32_t it = 0; it < kSpinLimit; ++it)
+// Bounded wait: returns false when `limit` polls pass, or early when another
+// thread of the CTA has raised `abort`; records `code` in *err on failure.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit, volatile int *abort,
+                                          int *err, int code) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (abort && (it & 255u) == 255u && *abort) return false;
+    }
     if (err) atomicCAS(err, 0, code);
     return false;
 }
@@ -134,17 +147,42 @@ constexpr int tc_stages() {
     return std::min(6, (200 * 1024) / TcSmem<BN, 1>::kStage);
 }
 
+// Work of one launch: T = mtiles x ctiles output tiles (256 rows x BN columns,
+// column tile fastest so that the tiles sharing one row block of the operand run
+// side by side and its second read comes from L2).  The first `full` tiles are
+// computed whole, one CTA each, in full waves over the SMs, and stored as FP64
+// into S; each of the remaining T - full tiles is split over k into q pieces of
+// kper k-tiles, one CTA each, which store FP32 partial sums into P (piece j at
+// P + j * 256 * BN, [column][row]); reduce_pieces adds a tile's pieces in
+// order.  With the pieces filling the last wave, every SM gets the same work
+// (whole tiles plus one piece) instead of a last wave that leaves SMs idle.
+struct TcSched {
+    int ctiles;     // column tiles
+    int full;       // tiles computed whole
+    int q;          // pieces per remaining tile
+    int kper;       // k-tiles per piece
+};
+
 template <int BN, int STAGES, int NPROD>
 __global__ void __launch_bounds__(128, 1)
     tc_contract_kernel(const __grid_constant__ CUtensorMap mapTh, const __grid_constant__ CUtensorMap mapTl,
                        const __grid_constant__ CUtensorMap mapXh, const __grid_constant__ CUtensorMap mapXl,
-                       int M, int R, int ktiles, int kper, double *__restrict__ S, int ldS, int64_t split_stride,
-                       int *__restrict__ err) {
+                       int M, int R, int ktiles, TcSched sc, double *__restrict__ S, int ldS,
+                       float *__restrict__ P, int *__restrict__ err, uint32_t wait_limit) {
     using L = TcSmem<BN, STAGES>;
-    // split over k: this CTA accumulates k-tiles [kt0, kt0 + nk) into its own partial
-    const int kt0 = blockIdx.z * kper;
-    const int nk = min(ktiles, kt0 + kper) - kt0;
-    S += (int64_t)blockIdx.z * split_stride;
+    // this CTA's unit: a whole tile, or one k-piece of a remaining tile
+    int tile, kt0, nk, piece = -1;
+    if ((int)blockIdx.x < sc.full) {
+        tile = blockIdx.x;
+        kt0 = 0;
+        nk = ktiles;
+    } else {
+        piece = blockIdx.x - sc.full;
+        tile = sc.full + piece / sc.q;
+        kt0 = (piece % sc.q) * sc.kper;
+        nk = min(ktiles, kt0 + sc.kper) - kt0;
+    }
+    const int mtile = tile / sc.ctiles;
     // two accumulators of BN columns each (rows m0.. and m0 + 128..)
     constexpr uint32_t kTmemCols = 2 * BN <= 64 ? 64 : (2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -156,8 +194,8 @@ __global__ void __launch_bounds__(128, 1)
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.x * BN;
-    const int m0 = blockIdx.y * kBM;
+    const int n0 = (tile % sc.ctiles) * BN;
+    const int m0 = mtile * kBM;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -185,41 +223,34 @@ __global__ void __launch_bounds__(128, 1)
         return which < 2 ? st + which * L::kA : st + 2 * L::kA + (which - 2) * L::kB;
     };
 
+    int issued = 0;     // loads issued by the producer (thread 0)
     if (threadIdx.x == 0) {
         // ---------------- TMA producer ----------------
-        int issued = 0;
         for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
             if (kt >= STAGES) {
-                if (!mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1, err, 1) || *abort_flag) {
+                if (!mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1, wait_limit, abort_flag, err, 1) || *abort_flag) {
                     *abort_flag = 1;
                     break;
                 }
             }
             mbar_expect_tx(&full[s], (uint32_t)L::kStage);
             const int kx = (kt0 + kt) * kBK;
-            const int ay = (blockIdx.y * ktiles + kt0 + kt) * kBM;     // tile-ordered A
+            const int ay = (mtile * ktiles + kt0 + kt) * kBM;          // tile-ordered A
             tma_load_2d(&mapTh, &full[s], stage_ptr(s, 0), 0, ay);
             tma_load_2d(&mapTl, &full[s], stage_ptr(s, 1), 0, ay);
             tma_load_2d(&mapXh, &full[s], stage_ptr(s, 2), kx, n0);
             tma_load_2d(&mapXl, &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
         }
-        if (*abort_flag) {
-            // let the loads already issued land before the CTA can exit
-            for (int kt = std::max(0, issued - STAGES); kt < issued; ++kt)
-                mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, nullptr, 0);
-        }
     } else if (threadIdx.x == 32) {
         // ---------------- MMA issuer ----------------
         constexpr uint32_t idesc = umma_idesc_bf16(kUM, BN);
         constexpr uint64_t kHalf = (uint64_t)(kUM * kBK * 2) >> 4;   // second 128 rows of an A tile
-        bool ok = true;
-        for (int kt = 0; kt < nk && ok; ++kt) {
+        for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
-            if (!mbar_wait(&full[s], (kt / STAGES) & 1, err, 2) || *abort_flag) {
+            if (!mbar_wait(&full[s], (kt / STAGES) & 1, wait_limit, abort_flag, err, 2) || *abort_flag) {
                 *abort_flag = 1;
-                ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -245,14 +276,26 @@ __global__ void __launch_bounds__(128, 1)
             }
             umma_commit(&empty[s]);
         }
-        if (ok) umma_commit(done);
+        // always: arrives once every MMA issued above has completed (also after
+        // an abort, so that nothing below frees memory an MMA still uses)
+        umma_commit(done);
     }
     __syncwarp();
 
     // ---------------- epilogue: TMEM -> S (FP64) ----------------
-    bool have = mbar_wait(done, 0, err, 3) && !*abort_flag;
-    have = __all_sync(0xffffffffu, have);     // tcgen05.ld below is warp-collective
-    if (!have) *abort_flag = 1;
+    bool fin = mbar_wait(done, 0, wait_limit, nullptr, err, 3);
+    if (!fin) {
+        *abort_flag = 1;
+        fin = mbar_wait(done, 0, kDrainLimit, nullptr, err, 4);
+    }
+    // uniform over the CTA; a thread that raised the flag counts it itself
+    const bool have = !__syncthreads_or(*abort_flag != 0 || !fin);
+    if (!have && threadIdx.x == 0) {
+        // let the loads already issued land before the CTA can exit: the last
+        // phase of each stage (earlier phases completed before it was re-armed)
+        for (int kt = issued > STAGES ? issued - STAGES : 0; kt < issued; ++kt)
+            mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, kDrainLimit, nullptr, err, 5);
+    }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
 #pragma unroll 1
@@ -273,7 +316,12 @@ __global__ void __launch_bounds__(128, 1)
                   "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
+            if (piece >= 0) {
+                // partial of a split tile: [column][256 rows] FP32, every element written
+                float *pp = P + (int64_t)piece * kBM * BN + (h * kUM + warp * 32 + lane);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) pp[(int64_t)(c0 + j) * kBM] = __uint_as_float(v[j]);
+            } else if (row < M) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int c = n0 + c0 + j;
@@ -454,25 +502,35 @@ CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t l
 
 template <int BN, int NPROD>
 void launch_bn(plx_geom *g, int M, int R, const CUtensorMap &th, const CUtensorMap &tl, const CUtensorMap &xh,
-               const CUtensorMap &xl, int ktiles, int splits, int kper, double *S, int *err) {
+               const CUtensorMap &xl, int ktiles, const TcSched &sc, int units, double *S, float *P, int *err) {
     constexpr int ST = tc_stages<BN>();
     using L = TcSmem<BN, ST>;
     auto kern = tc_contract_kernel<BN, ST, NPROD>;
     once_per_device(reinterpret_cast<const void *>(kern), g->ctx->device, [&] {
         PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
     });
-    dim3 grid((R + BN - 1) / BN, (M + kBM - 1) / kBM, splits);
-    kern<<<grid, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, M, R, ktiles, kper, S, M, (int64_t)R * M, err);
+    kern<<<units, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, M, R, ktiles, sc, S, M, P, err,
+                                                    g->ctx->wait_limit);
     g->ctx->launches++;
     PLX_CHECK_CUDA(cudaGetLastError());
 }
 
-// S = sum_z P[z] over the k-split partials, in split order.
-__global__ void reduce_splits(int64_t count, int splits, const double *__restrict__ P, double *__restrict__ S) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
-        double a = P[e];
-        for (int z = 1; z < splits; ++z) a += P[(int64_t)z * count + e];
-        S[e] = a;
+// Remaining tiles: S = the sum of a tile's q FP32 pieces in piece order (FP64
+// sums), for the rows and columns inside the matrix.  One block per (tile,
+// 32-column group); threads over the tile's 256 rows.
+template <int BN>
+__global__ void reduce_pieces(int M, int R, int full, int ctiles, int q, const float *__restrict__ P,
+                              double *__restrict__ S, int ldS) {
+    const int t = blockIdx.x;                       // remaining tile index
+    const int tile = full + t;
+    const int m0 = (tile / ctiles) * kBM, n0 = (tile % ctiles) * BN;
+    const int r = threadIdx.x;                      // 0..255
+    if (m0 + r >= M) return;
+    for (int c = blockIdx.y * 32; c < min(BN, blockIdx.y * 32 + 32); ++c) {
+        if (n0 + c >= R) break;
+        double a = 0.0;
+        for (int p = 0; p < q; ++p) a += (double)P[((int64_t)(t * q + p) * BN + c) * kBM + r];
+        S[(int64_t)(n0 + c) * ldS + m0 + r] = a;
     }
 }
 
@@ -482,22 +540,25 @@ int sm_count(int device) {
     return v > 0 ? v : 1;
 }
 
-// Number of k-splits for `tiles` output tiles: the fewest whose last wave fills
-// at least 90% of the SMs (one CTA per SM), keeping >= 16 k-tiles per split.
-int choose_splits(int tiles, int ktiles, int sms) {
-    int best = 1;
-    double best_eff = 0.0;
-    for (int s = 1; s <= 4; ++s) {
-        if (s > 1 && ktiles / s < 16) break;
-        const int64_t ctas = (int64_t)tiles * s;
-        const double eff = (double)ctas / (double)(((ctas + sms - 1) / sms) * sms);
-        if (eff >= 0.9) return s;
-        if (eff > best_eff + 1e-9) {
-            best_eff = eff;
-            best = s;
-        }
-    }
-    return best;
+// Schedule of `tiles` output tiles of `ktiles` k-tiles on `sms` SMs (one CTA per
+// SM): whole tiles in full waves; the r = tiles mod sms tiles of the last wave
+// are split into q = sms / r pieces (at least 8 k-tiles each) when that lets the
+// pieces fill the wave -- otherwise (r close to sms, or no split possible) they
+// run whole too.
+TcSched make_schedule(int tiles, int ctiles, int ktiles, int sms, int &units) {
+    TcSched sc{ctiles, tiles, 1, ktiles};
+    const int r = tiles % sms;
+    units = tiles;
+    if (r == 0 || (double)r / sms >= 0.9) return sc;
+    int q = std::min(sms / r, ktiles / 8);
+    if (q < 2) return sc;
+    const int kper = (ktiles + q - 1) / q;
+    q = (ktiles + kper - 1) / kper;                 // no empty piece
+    sc.full = tiles - r;
+    sc.q = q;
+    sc.kper = kper;
+    units = sc.full + r * q;
+    return sc;
 }
 
 }  // namespace
@@ -717,33 +778,31 @@ void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, 
     CUtensorMap xl = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
     const int ktiles = (int)(ld / kBK);
     int *err = g->d_tc_err.p;
-    // k-splits against wave quantisation; partials reduced in a fixed order
-    const int tiles = ntile * (int)((M + kBM - 1) / kBM);
-    int splits = choose_splits(tiles, ktiles, sm_count(ctx->device));
-    const int kper = (ktiles + splits - 1) / splits;
-    splits = (ktiles + kper - 1) / kper;
-    double *out = S;
-    if (splits > 1) {
-        const size_t pn = (size_t)splits * R * M;
+    const int mtiles = (M + kBM - 1) / kBM;
+    int units = 0;
+    const TcSched sc = make_schedule(mtiles * ntile, ntile, ktiles, sm_count(ctx->device), units);
+    const int rem = mtiles * ntile - sc.full;
+    float *P = nullptr;
+    if (rem > 0) {
+        const size_t pn = (size_t)rem * sc.q * kBM * bn;
         if (g->d_tcpart.n < pn) g->d_tcpart.alloc(ctx, pn);
-        out = g->d_tcpart.p;
+        P = g->d_tcpart.p;
     }
-#define PLX_TC(BNV)                                                                               \
-    case BNV:                                                                                     \
-        if (nprod == 1) launch_bn<BNV, 1>(g, M, R, th, tl, xh, xl, ktiles, splits, kper, out, err);  \
-        else launch_bn<BNV, 3>(g, M, R, th, tl, xh, xl, ktiles, splits, kper, out, err);             \
+#define PLX_TC(BNV)                                                                              \
+    case BNV:                                                                                    \
+        if (nprod == 1) launch_bn<BNV, 1>(g, M, R, th, tl, xh, xl, ktiles, sc, units, S, P, err); \
+        else launch_bn<BNV, 3>(g, M, R, th, tl, xh, xl, ktiles, sc, units, S, P, err);            \
+        if (rem > 0) {                                                                           \
+            reduce_pieces<BNV><<<dim3(rem, BNV / 32), kBM, 0, ctx->stream>>>(M, R, sc.full, ntile, sc.q, P, S, M); \
+            ctx->launches++;                                                                     \
+        }                                                                                        \
         break;
     switch (bn) {
         PLX_TC(32) PLX_TC(64) PLX_TC(96) PLX_TC(128) PLX_TC(160) PLX_TC(192) PLX_TC(224) PLX_TC(256)
         default: throw Error(PLX_ERR_ARG, "bad column tile");
     }
 #undef PLX_TC
-    if (splits > 1) {
-        const int64_t cnt = (int64_t)R * M;
-        reduce_splits<<<(int)std::min<int64_t>(4096, n_blocks(cnt, 256)), 256, 0, ctx->stream>>>(cnt, splits, out, S);
-        ctx->launches++;
-        PLX_CHECK_CUDA(cudaGetLastError());
-    }
+    PLX_CHECK_CUDA(cudaGetLastError());
 }
 
 int tc_error(plx_geom *g) {
@@ -751,6 +810,8 @@ int tc_error(plx_geom *g) {
     int h = 0;
     PLX_CHECK_CUDA(cudaMemcpyAsync(&h, g->d_tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, g->ctx->stream));
     PLX_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    // reported once: the next call starts clean
+    if (h) PLX_CHECK_CUDA(cudaMemsetAsync(g->d_tc_err.p, 0, sizeof(int), g->ctx->stream));
     return h;
 }
 

@@ -52,6 +52,11 @@ class Context:
     def profile_breakdown(self):
         return {name: self.profile_read(k) for k, name in enumerate(self.PROFILE_CATEGORIES)}
 
+    def set_wait_limit(self, polls=0):
+        """Polls after which a pipeline wait in the tensor-core kernels gives up
+        (0: the default); a wait that runs out makes the call fail cleanly."""
+        self.check(self.lib.plx_set_wait_limit(self.h, int(polls)))
+
     @property
     def bytes_in_use(self):
         return int(self.lib.plx_ctx_bytes_in_use(self.h))

@@ -683,4 +683,7 @@ if __name__ == '__main__':
     if len(sys.argv) > 2 and sys.argv[1] == '--one':
         one(sys.argv[2], sys.argv[3])
     else:
-        main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+        tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PLASMONX_REFERENCE')
+        if not tree:
+            sys.exit('usage: make_golden.py /path/to/plasmonX  (or set PLASMONX_REFERENCE)')
+        main(tree)

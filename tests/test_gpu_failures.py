@@ -5,6 +5,9 @@
   * a non-finite right-hand side handed to the reference-shaped GMRES;
   * a geometry larger than the context's HBM budget is refused with
     PLX_ERR_BUDGET and leaves nothing allocated;
+  * the tensor-core kernel's bounded waits: with the wait limit set to one poll
+    every pipeline wait runs out; the kernel lets its copies and products finish,
+    frees its tensor memory and returns, and the call reports PLX_ERR_CUDA;
   * after each failure the same context solves a clean problem.
 """
 import numpy as np
@@ -70,5 +73,31 @@ def test_budget_refusal_leaves_nothing_allocated():
         small = configs.particle('Na', 'sphere', 6.0, n_freq=2, method='iterative')
         with Solver(small, ctx=c) as sv:
             assert np.all(sv.solve()['status'] == 0)
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize('how', ['bf16x3', 'bf16'])
+def test_tensor_core_wait_limit_runs_out_cleanly(how):
+    """A wait limit of one poll makes the tensor-core kernel's first pipeline wait
+    give up (nothing faults: the loads it issued land, the products finish, the
+    kernel returns); plx_contract reports PLX_ERR_CUDA with the timeout message.
+    At the default limit the same context contracts correctly again."""
+    p = configs.ag_sphere(radius=10.0, n_freq=1, method='iterative')
+    c = Context(0)
+    try:
+        with Solver(p, ctx=c, store_t=True) as sv:
+            rng = np.random.default_rng(21)
+            X = rng.standard_normal((8, sv.n_var))
+            ref = sv.contract(X, 'fp64')
+            c.set_wait_limit(1)
+            with pytest.raises(_lib.PlxError) as e:
+                sv.contract(X, how)
+            assert e.value.code == 2 and 'timed out' in str(e.value)
+            c.set_wait_limit(0)
+            for _ in range(2):
+                S = sv.contract(X, how)
+                err = np.linalg.norm(S - ref, axis=1) / np.linalg.norm(ref, axis=1)
+                assert err.max() < (5e-5 if how == 'bf16x3' else 1e-2), err
     finally:
         c.close()

@@ -41,3 +41,31 @@ def test_noalloc_contraction_matches_allocating_entry_point():
             assert st == 1 and b'1 to 16 columns' in sv.lib.plx_last_error(ctx.h)
     finally:
         ctx.close()
+
+
+def test_noalloc_refuses_partials_beyond_the_scratch():
+    """16 columns of the 7,844-unknown sphere need 20 k-chunks x 16 x 7,844 partial
+    sums, more than the 2^21 doubles of the fixed scratch: refused with status 1 and
+    the limit in the message; a call that fits still matches the allocating path."""
+    import torch
+    p = configs.ag_sphere(radius=20.0, n_freq=1, method='iterative')
+    ctx = Context(0)
+    try:
+        with Solver(p, ctx=ctx, store_t=True) as sv:
+            assert sv.n_var == 7844
+            dX = torch.zeros((16, sv.n_var), dtype=torch.float64, device='cuda:0')
+            dS = torch.zeros((16, sv.n_var), dtype=torch.float64, device='cuda:0')
+            torch.cuda.synchronize()
+            st = sv.lib.plx_contract_noalloc(sv.g, 16, C.c_void_p(dX.data_ptr()), C.c_void_p(dS.data_ptr()))
+            assert st == 1 and b'fixed maximum' in sv.lib.plx_last_error(ctx.h)
+            rng = np.random.default_rng(12)
+            X = rng.standard_normal((6, sv.n_var))
+            ref = sv.contract(X, 'fp64')
+            dX = torch.from_numpy(X).to('cuda:0')
+            dS = torch.full((6, sv.n_var), float('nan'), dtype=torch.float64, device='cuda:0')
+            torch.cuda.synchronize()
+            ctx.check(sv.lib.plx_contract_noalloc(sv.g, 6, C.c_void_p(dX.data_ptr()), C.c_void_p(dS.data_ptr())))
+            S = dS.cpu().numpy()
+            assert np.max(np.linalg.norm(S - ref, axis=1) / np.linalg.norm(ref, axis=1)) < 1e-12
+    finally:
+        ctx.close()
