@@ -319,7 +319,7 @@ def _time_orthogonalisation(n, j, reps=5):
     return (time.perf_counter() - t0) / reps
 
 
-def cpu_reference(prob, steps_per_solve, n_min=20, budget_s=20.0):
+def cpu_reference(prob, steps_per_solve, n_min=20, budget_s=8.0):
     """The reference's per-frequency GMRES on the host cores, timed per part and
     composed into freq-solves/s (extrapolated: a whole spectrum takes hours).
 
