@@ -281,6 +281,51 @@ plx_status plx_contract(plx_geom *geom, int32_t count, const double *X, double *
  * context's stream and returns when S is written. */
 plx_status plx_contract_noalloc(plx_geom *geom, int32_t count, const double *d_X, double *d_S);
 
+/* ---- continuous batching ------------------------------------------------- */
+
+/* A refinement solve (precision PLX_MIXED_BF16X3, PLX_MIXED_BF16 or
+ * PLX_FP64_REFINED; mode PLX_GMRES_MEM or PLX_GMRES_OTF) whose columns come and
+ * go while others are in flight: the per-frequency loops of
+ * algorithm_module.f90:334-465 turned into a serving loop.  A request (a grid
+ * of frequencies and polarisations with its own absolute tolerance) added with
+ * plx_batch_add joins the batch at the next plx_batch_step, which runs ONE outer
+ * refinement step (inner GMRES cycles on the tensor cores, then the FP64
+ * residual) for every active column of every request; plx_batch_poll reports a
+ * request whose columns have all finished and plx_batch_take returns its
+ * results (as plx_solve does for its grid) and frees its columns.  While a
+ * batch is open it owns the geometry's frequency table (plx_set_frequencies is
+ * refused); close the batch before destroying the geometry.  No counterpart in
+ * the reference, whose GMRES calls are serialised (algorithm_module.f90:382-385). */
+typedef struct plx_batch plx_batch;
+/* desc: mode, precision, inner_krylov, inner_tol, max_outer (tol and the other
+ * fields are not used; each request brings its own tolerance). */
+plx_status plx_batch_open(plx_geom *geom, const plx_solve_desc *desc, plx_batch **out);
+/* A request: tag (distinct, >= 0), n_freq frequencies (a.u.), alpha_w as in
+ * plx_set_frequencies (n_types x n_freq complex; eps(w) for BEM; NULL for
+ * wFQ), polarisations pol_mask, absolute residual tolerance tol. */
+plx_status plx_batch_add(plx_batch *b, int64_t tag, int32_t n_freq, const double *omega, const double *alpha_w,
+                         int32_t pol_mask, double tol);
+/* One outer step of every active column; n_active (optional) receives the
+ * number of columns still being solved afterwards.  plx_last_solve_ms of the
+ * geometry then holds the step's device time. */
+plx_status plx_batch_step(plx_batch *b, int32_t *n_active);
+/* One outer step of several batches (one per geometry, all on one context):
+ * every inner Arnoldi step of all of them is ONE grouped tensor-core launch
+ * over their operands, in place of the reference's one frequency per thread
+ * (algorithm_module.f90:224-265, 365-405). */
+plx_status plx_batch_step_group(plx_batch *const *batches, int32_t count, int32_t *n_active);
+/* The tag of the earliest request whose columns have all finished, or -1. */
+plx_status plx_batch_poll(plx_batch *b, int64_t *tag);
+/* Results of a finished request (each output optional): polar_out complex
+ * 3 x 3 x n_freq, results_out n_freq x 20, status_out n_freq, steps_out
+ * 3 x n_freq inner Arnoldi steps; frees its columns.  Returns the first
+ * non-OK status of its frequencies, or PLX_OK. */
+plx_status plx_batch_take(plx_batch *b, int64_t tag, double *polar_out, double *results_out, int32_t *status_out,
+                          int32_t *steps_out);
+/* Columns still being solved. */
+int32_t plx_batch_active(const plx_batch *b);
+void plx_batch_close(plx_batch *b);
+
 /* ---- static FQ / FQFMu ---------------------------------------------------- */
 
 /* The static force fields whose types the w-models extend

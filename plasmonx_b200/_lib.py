@@ -23,7 +23,9 @@ EXPORTS = ['plx_ctx_create', 'plx_ctx_destroy', 'plx_last_error', 'plx_ctx_bytes
            'plx_solve', 'plx_last_solve_ms', 'plx_last_solve_launches', 'plx_profile_enable',
            'plx_profile_read', 'plx_contract', 'plx_contract_noalloc', 'plx_field_at_points',
            'plx_static_n_var', 'plx_static_solve', 'plx_principal_axes', 'plx_neighbour_counts',
-           'plx_bem_field_at_points', 'plx_ctx_launches', 'plx_set_wait_limit']
+           'plx_bem_field_at_points', 'plx_ctx_launches', 'plx_set_wait_limit', 'plx_batch_open', 'plx_batch_add',
+           'plx_batch_step', 'plx_batch_step_group', 'plx_batch_poll', 'plx_batch_take', 'plx_batch_active',
+           'plx_batch_close']
 STATIC_FF = {'fq': 0, 'fqfmu': 1}
 KERNEL = {'coulomb': 0, 'ohno': 1, 'gaussian': 2}
 STATIC_WHAT = {'energy': 0, 'static': 1}
@@ -117,6 +119,16 @@ def load():
     lib.plx_profile_enable.argtypes = [vp, C.c_int32]
     lib.plx_profile_read.argtypes = [vp, C.c_int32, _dp, C.POINTER(C.c_int64), _dp, _dp]
     lib.plx_set_wait_limit.argtypes = [vp, C.c_uint32]
+    lib.plx_batch_open.argtypes = [vp, C.POINTER(SolveDesc), C.POINTER(vp)]
+    lib.plx_batch_add.argtypes = [vp, C.c_int64, C.c_int32, _dp, _dp, C.c_int32, C.c_double]
+    lib.plx_batch_step.argtypes = [vp, _ip]
+    lib.plx_batch_step_group.argtypes = [C.POINTER(vp), C.c_int32, _ip]
+    lib.plx_batch_poll.argtypes = [vp, C.POINTER(C.c_int64)]
+    lib.plx_batch_take.argtypes = [vp, C.c_int64, _dp, _dp, _ip, _ip]
+    lib.plx_batch_active.argtypes = [vp]
+    lib.plx_batch_active.restype = C.c_int32
+    lib.plx_batch_close.argtypes = [vp]
+    lib.plx_batch_close.restype = None
     _lib = lib
     return lib
 

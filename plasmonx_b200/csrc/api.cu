@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "plx_internal.h"
@@ -283,6 +284,7 @@ plx_status plx_set_frequencies(plx_geom *g, int32_t n_freq, const double *omega,
     return guarded(g->ctx, [&] {
         set_device(g->ctx);
         if (n_freq < 1 || !omega) throw Error(PLX_ERR_ARG, "need at least one frequency");
+        if (g->open_batches > 0) throw Error(PLX_ERR_ARG, "the geometry's frequencies belong to its open batch");
         if (g->model == PLX_WFQFMU && !alpha_w) throw Error(PLX_ERR_ARG, "alpha_w is required for wFQFMu");
         if (is_bem(g) && !alpha_w) throw Error(PLX_ERR_ARG, "eps(w) (alpha_w) is required for BEM");
         g->n_freq = n_freq;
@@ -727,6 +729,305 @@ plx_status plx_contract(plx_geom *g, int32_t count, const double *X, double *S, 
         if (how >= 2 && tc_error(g))
             throw Error(PLX_ERR_CUDA, "tensor-core contraction timed out waiting on its pipeline");
     });
+}
+
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// continuous batching: a refinement solve whose columns come and go between
+// outer steps (plx_batch_*)
+// ---------------------------------------------------------------------------
+struct plx_batch {
+    plx_geom *g = nullptr;
+    RefineState st;
+    struct Request {
+        int32_t f0 = 0, n_freq = 0;             // frequency-table range
+        std::vector<int32_t> pols;
+        std::vector<int32_t> slots;             // freq-major, pol-minor
+    };
+    std::map<int64_t, Request> req;
+    std::vector<int64_t> order;                 // tags in arrival order
+};
+
+namespace {
+
+// slots of `k` columns: D[slot[k]] = S[k]
+__global__ void scatter_cols(int n, const int32_t *__restrict__ slot, const double *__restrict__ S,
+                             double *__restrict__ D) {
+    int k = blockIdx.y;
+    const double *s = S + (int64_t)k * 2 * n;
+    double *d = D + (int64_t)slot[k] * 2 * n;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < 2LL * n; r += (int64_t)gridDim.x * blockDim.x)
+        d[r] = s[r];
+}
+
+bool request_finished(const plx_batch *b, const plx_batch::Request &r) {
+    for (int s : r.slots)
+        if (b->st.slots[s].state != RefineState::Slot::FINISHED) return false;
+    return true;
+}
+
+int32_t batch_active(const plx_batch *b) {
+    int32_t a = 0;
+    for (const auto &s : b->st.slots) a += s.state == RefineState::Slot::ACTIVE;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+plx_status plx_batch_open(plx_geom *g, const plx_solve_desc *desc, plx_batch **out) {
+    if (!g || !desc || !out) return PLX_ERR_ARG;
+    *out = nullptr;
+    return guarded(g->ctx, [&] {
+        set_device(g->ctx);
+        if (desc->mode != PLX_GMRES_MEM && desc->mode != PLX_GMRES_OTF)
+            throw Error(PLX_ERR_ARG, "a batch solves by GMRES (on-memory or on the fly)");
+        if (desc->precision < PLX_FP64 || desc->precision > PLX_MIXED_BF16) throw Error(PLX_ERR_ARG, "bad precision");
+        if (desc->precision == PLX_FP64)
+            throw Error(PLX_ERR_ARG, "a batch runs the refinement forms (mixed or FP64 refined)");
+        const bool otf = desc->mode == PLX_GMRES_OTF;
+        if (otf && is_bem(g)) throw Error(PLX_ERR_UNSUPPORTED, "BEM on the fly is not provided");
+        if (!otf && !g->has_T) throw Error(PLX_ERR_ARG, "this mode needs the stored T (store_t at creation)");
+        if (g->open_batches > 0) throw Error(PLX_ERR_ARG, "the geometry already has an open batch");
+        const int n = g->n_var;
+        RefineRequest rr;
+        rr.inner_m = desc->inner_krylov > 0 ? std::min(desc->inner_krylov, n) : std::min(64, n);
+        rr.inner_rel = desc->inner_tol > 0 ? desc->inner_tol : 1e-4;
+        rr.max_outer = desc->max_outer > 0 ? desc->max_outer : 60;
+        rr.outer_contraction = otf ? Contraction::FP64_OTF : Contraction::FP64;
+        rr.inner_contraction = desc->precision == PLX_MIXED_BF16X3 ? Contraction::TC3
+                               : desc->precision == PLX_MIXED_BF16 ? Contraction::TC1
+                                                                   : rr.outer_contraction;
+        rr.max_cycles = rr.inner_contraction == rr.outer_contraction ? 1 : 8;
+        auto *b = new plx_batch();
+        b->g = g;
+        b->st.own(g, rr);
+        // the batch owns the frequency table from here on
+        g->n_freq = 0;
+        g->omega.clear();
+        g->alpha_w.clear();
+        g->open_batches++;
+        *out = b;
+    });
+}
+
+plx_status plx_batch_add(plx_batch *b, int64_t tag, int32_t n_freq, const double *omega, const double *alpha_w,
+                         int32_t pol_mask, double tol) {
+    if (!b || !omega || n_freq < 1) return PLX_ERR_ARG;
+    plx_geom *g = b->g;
+    return guarded(g->ctx, [&] {
+        TraceRange trace_("plx_batch_add");
+        set_device(g->ctx);
+        plx_ctx *ctx = g->ctx;
+        cudaStream_t st = ctx->stream;
+        if (tag < 0 || b->req.count(tag)) throw Error(PLX_ERR_ARG, "request tags are distinct and non-negative");
+        if (g->model == PLX_WFQFMU && !alpha_w) throw Error(PLX_ERR_ARG, "alpha_w is required for wFQFMu");
+        if (is_bem(g) && !alpha_w) throw Error(PLX_ERR_ARG, "eps(w) (alpha_w) is required for BEM");
+        if (!(tol > 0.0)) throw Error(PLX_ERR_ARG, "tolerance must be positive");
+        std::vector<int32_t> pols;
+        for (int p = 0; p < 3; ++p)
+            if (pol_mask & (1 << p)) pols.push_back(p);
+        if (pols.empty()) throw Error(PLX_ERR_ARG, "empty polarisation mask");
+        const int n = g->n_var, np = (int)pols.size(), C = n_freq * np;
+        // append the frequencies to the geometry's tables
+        plx_batch::Request r;
+        r.f0 = g->n_freq;
+        r.n_freq = n_freq;
+        r.pols = pols;
+        const int per = is_bem(g) ? 1 : g->n_types;
+        g->omega.insert(g->omega.end(), omega, omega + n_freq);
+        if (alpha_w)
+            for (size_t e = 0; e < (size_t)per * n_freq; ++e) g->alpha_w.push_back({alpha_w[2 * e], alpha_w[2 * e + 1]});
+        g->n_freq += n_freq;
+        upload_frequency_tables(g);
+        // slots: free ones first, then grown
+        RefineState &S = b->st;
+        int used = 0;
+        for (const auto &s : S.slots) used += s.state != RefineState::Slot::FREE;
+        S.grow(used + C);
+        for (int c = 0, s = 0; c < C; ++c) {
+            while (S.slots[s].state != RefineState::Slot::FREE) ++s;
+            RefineState::Slot &sl = S.slots[s];
+            sl = RefineState::Slot();
+            sl.state = RefineState::Slot::ACTIVE;
+            sl.freq = r.f0 + c / np;
+            sl.pol = pols[c % np];
+            sl.tol = tol;
+            sl.tag = tag;
+            r.slots.push_back(s);
+        }
+        // right-hand sides into the slots; x = 0, r = b
+        std::vector<int32_t> cf(C), cp(C);
+        for (int c = 0; c < C; ++c) {
+            cf[c] = S.slots[r.slots[c]].freq;
+            cp[c] = S.slots[r.slots[c]].pol;
+        }
+        DevArray<int32_t> dF, dP, dS;
+        DevArray<double> Bt, Z;
+        dF.alloc(ctx, C);
+        dP.alloc(ctx, C);
+        dS.alloc(ctx, C);
+        Bt.alloc(ctx, (size_t)C * 2 * n);
+        Z.alloc(ctx, (size_t)C * 2 * n);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(dF.p, cf.data(), C * 4, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(dP.p, cp.data(), C * 4, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(dS.p, r.slots.data(), C * 4, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemsetAsync(Z.p, 0, (size_t)C * 2 * n * 8, st));
+        rhs_batch(g, OpBatch{C, dF.p}, dP.p, Bt.p);
+        const int gr = std::min(n_blocks(2LL * n, 256), 1024);
+        scatter_cols<<<dim3(gr, C), 256, 0, st>>>(n, dS.p, Bt.p, S.ownB.p);
+        scatter_cols<<<dim3(gr, C), 256, 0, st>>>(n, dS.p, Bt.p, S.R.p);
+        scatter_cols<<<dim3(gr, C), 256, 0, st>>>(n, dS.p, Z.p, S.ownX.p);
+        ctx->launches += 3;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        b->req[tag] = std::move(r);
+        b->order.push_back(tag);
+    });
+}
+
+plx_status plx_batch_step(plx_batch *b, int32_t *n_active) {
+    if (!b) return PLX_ERR_ARG;
+    return plx_batch_step_group(&b, 1, n_active);
+}
+
+plx_status plx_batch_step_group(plx_batch *const *batches, int32_t count, int32_t *n_active) {
+    if (!batches || count < 1 || !batches[0]) return PLX_ERR_ARG;
+    plx_ctx *ctx = batches[0]->g->ctx;
+    return guarded(ctx, [&] {
+        TraceRange trace_("plx_batch_step");
+        set_device(ctx);
+        std::vector<RefineState *> states;
+        for (int i = 0; i < count; ++i) {
+            if (!batches[i] || batches[i]->g->ctx != ctx)
+                throw Error(PLX_ERR_ARG, "grouped batches must share one context");
+            for (int k = 0; k < i; ++k)
+                if (batches[k]->g == batches[i]->g) throw Error(PLX_ERR_ARG, "one batch per geometry in a group");
+            states.push_back(&batches[i]->st);
+        }
+        const int64_t l0 = ctx->launches;
+        PLX_CHECK_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+        refine_group_step(states);
+        int32_t a = 0;
+        bool timed_out = false;
+        for (int i = 0; i < count; ++i) {
+            batches[i]->st.update_status();      // finished columns are known right after the step
+            a += batch_active(batches[i]);
+            plx_geom *g = batches[i]->g;
+            if (g->d_tc_err.p && tc_error(g) != 0) timed_out = true;
+        }
+        PLX_CHECK_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+        PLX_CHECK_CUDA(cudaEventSynchronize(ctx->ev1));
+        float ms = 0.f;
+        PLX_CHECK_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        for (int i = 0; i < count; ++i) {
+            batches[i]->g->last_ms = ms;
+            batches[i]->g->last_launches = ctx->launches - l0;
+        }
+        if (timed_out) throw Error(PLX_ERR_CUDA, "tensor-core contraction timed out waiting on its pipeline");
+        if (n_active) *n_active = a;
+    });
+}
+
+plx_status plx_batch_poll(plx_batch *b, int64_t *tag) {
+    if (!b || !tag) return PLX_ERR_ARG;
+    *tag = -1;
+    for (int64_t t : b->order) {
+        auto it = b->req.find(t);
+        if (it != b->req.end() && request_finished(b, it->second)) {
+            *tag = t;
+            break;
+        }
+    }
+    return PLX_OK;
+}
+
+plx_status plx_batch_take(plx_batch *b, int64_t tag, double *polar_out, double *results_out, int32_t *status_out,
+                          int32_t *steps_out) {
+    if (!b) return PLX_ERR_ARG;
+    plx_geom *g = b->g;
+    plx_status first_bad = PLX_OK;
+    plx_status s = guarded(g->ctx, [&] {
+        TraceRange trace_("plx_batch_take");
+        set_device(g->ctx);
+        plx_ctx *ctx = g->ctx;
+        cudaStream_t st = ctx->stream;
+        auto it = b->req.find(tag);
+        if (it == b->req.end()) throw Error(PLX_ERR_ARG, "unknown request tag");
+        plx_batch::Request &r = it->second;
+        if (!request_finished(b, r)) throw Error(PLX_ERR_ARG, "the request is still being solved");
+        const int n = g->n_var, C = (int)r.slots.size(), np = (int)r.pols.size();
+        DevArray<int32_t> dS, dD;
+        DevArray<double> Xg;
+        DevArray<Cplx> dpol;
+        dS.alloc(ctx, C);
+        dD.alloc(ctx, C);
+        Xg.alloc(ctx, (size_t)C * 2 * n);
+        dpol.alloc(ctx, (size_t)C * 3);
+        std::vector<int32_t> dst(C);
+        for (int c = 0; c < C; ++c) dst[c] = c;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(dS.p, r.slots.data(), C * 4, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(dD.p, dst.data(), C * 4, cudaMemcpyHostToDevice, st));
+        copy_cols<<<dim3(std::min(n_blocks(2LL * n, 256), 1024), C), 256, 0, st>>>(n, dS.p, dD.p, b->st.ownX.p, Xg.p);
+        ctx->launches++;
+        polar_batch(g, C, nullptr, Xg.p, dpol.p);
+        std::vector<Cplx> hp((size_t)C * 3);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(hp.data(), dpol.p, hp.size() * sizeof(Cplx), cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        for (int f = 0; f < r.n_freq; ++f) {
+            std::vector<Cplx> P(9, Cplx{0.0, 0.0});
+            int32_t fst = PLX_OK;
+            if (steps_out)
+                for (int p = 0; p < 3; ++p) steps_out[3 * f + p] = 0;
+            for (int k = 0; k < np; ++k) {
+                const int c = f * np + k;
+                const RefineState::Slot &sl = b->st.slots[r.slots[c]];
+                for (int a = 0; a < 3; ++a) P[a + 3 * r.pols[k]] = hp[(size_t)3 * c + a];
+                if (sl.status != PLX_OK && fst == PLX_OK) fst = sl.status;
+                if (steps_out) steps_out[3 * f + r.pols[k]] = sl.inner_steps;
+            }
+            if (polar_out)
+                for (int e = 0; e < 9; ++e) {
+                    polar_out[2 * (9 * (size_t)f + e)] = P[e].re;
+                    polar_out[2 * (9 * (size_t)f + e) + 1] = P[e].im;
+                }
+            if (results_out) results_row(P.data(), g->omega[r.f0 + f], results_out + 20 * (size_t)f);
+            if (status_out) status_out[f] = fst;
+            if (fst != PLX_OK && first_bad == PLX_OK) first_bad = (plx_status)fst;
+        }
+        for (int sidx : r.slots) b->st.slots[sidx] = RefineState::Slot();
+        b->req.erase(it);
+        b->order.erase(std::remove(b->order.begin(), b->order.end(), tag), b->order.end());
+        if (b->req.empty()) {
+            // nothing in flight: the frequency table starts again from empty
+            g->n_freq = 0;
+            g->omega.clear();
+            g->alpha_w.clear();
+        }
+        if (first_bad == PLX_ERR_NOT_CONVERGED) ctx->last_error = "refinement ran out of outer steps";
+        else if (first_bad == PLX_ERR_NAN) ctx->last_error = "non-finite residual in the refinement";
+    });
+    return s != PLX_OK ? s : first_bad;
+}
+
+int32_t plx_batch_active(const plx_batch *b) { return b ? batch_active(b) : 0; }
+
+void plx_batch_close(plx_batch *b) {
+    if (!b) return;
+    plx_geom *g = b->g;
+    try {
+        set_device(g->ctx);
+        PLX_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    } catch (...) {
+    }
+    g->open_batches--;
+    g->n_freq = 0;
+    g->omega.clear();
+    g->alpha_w.clear();
+    delete b;
 }
 
 double plx_last_solve_ms(const plx_geom *g) { return g ? g->last_ms : 0.0; }

@@ -20,6 +20,7 @@
 // kernels only touch active columns.
 #include <algorithm>
 #include <cmath>
+#include <memory>
 
 #include "plx_internal.h"
 
@@ -391,221 +392,273 @@ static void batch_norms(plx_geom *g, int count, const double *V, DevArray<double
     ctx->launches += 2;
 }
 
+// One batched GMRES solve, advanced one Arnoldi step at a time so that the
+// operator application of every step can be shared with other solves (a
+// grouped tensor-core launch over several geometries): begin(), then while
+// wants_product(): pre() -> the caller forms W = A X of the returned batch ->
+// post(); then end().  gmres_batched runs it with its own operator.
 template <typename VT>
-static void gmres_impl(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X, GmresResult &res) {
-    plx_ctx *ctx = g->ctx;
-    cudaStream_t st = ctx->stream;
-    const int n = g->n_var;
-    const int C = (int)rq.freq.size();
-    const int m = std::min(rq.m, n);
-    res.status.assign(C, PLX_OK);
-    res.steps.assign(C, 0);
-    res.trace.assign(rq.record_trace ? (size_t)C * m : 0, 0.0);
-    if (C == 0) return;
-    if (m < 1) throw Error(PLX_ERR_ARG, "GMRES dimension must be positive");
+class GmresRun final : public GmresStepper {
+  public:
+    GmresRun(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X, GmresResult &res)
+        : g_(g), ctx_(g->ctx), st_(g->ctx->stream), rq_(rq), d_B_(d_B), d_X_(d_X), res_(res) {}
 
-    const int nchunk = n_blocks(n, kRows);
-    const int ndot = n_blocks(n, kDotRows);
-    if ((size_t)(m + 1) * sizeof(double2) > 200 * 1024) throw Error(PLX_ERR_ARG, "GMRES dimension above 12800");
-    once_per_device(reinterpret_cast<const void *>(tri_solve), ctx->device, [] {
-        PLX_CHECK_CUDA(cudaFuncSetAttribute(tri_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-        PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    });
-    const int hstride = m + 1;   // rows of an H column (0..m)
-    DevArray<int32_t> d_act, d_freq_act, d_cols;
-    d_act.alloc(ctx, C);
-    d_freq_act.alloc(ctx, C);
-    d_cols.alloc(ctx, C);
-    DevArray<double> Xa, Wa, work, nrm_part, nrm;
-    Xa.alloc(ctx, (size_t)C * 2 * n);
-    Wa.alloc(ctx, (size_t)C * 2 * n);
-    work.alloc(ctx, (size_t)C * 2 * n);
-    nrm_part.alloc(ctx, (size_t)C * nchunk);
-    nrm.alloc(ctx, C);
-    DevArray<double> cs;
-    DevArray<double2> sn, gv, hbuf, part, ybuf;
-    cs.alloc(ctx, (size_t)C * m);
-    sn.alloc(ctx, (size_t)C * m);
-    gv.alloc(ctx, (size_t)C * hstride);
-    hbuf.alloc(ctx, (size_t)C * hstride);
-    ybuf.alloc(ctx, (size_t)C * hstride);
-    std::vector<DevArray<VT>> slabs(m + 1);
-    std::vector<DevArray<double2>> hcols(m);
-    DevArray<VT *> d_slabs;
-    DevArray<double2 *> d_hcols;
-    d_slabs.alloc(ctx, m + 1);
-    d_hcols.alloc(ctx, m);
-    std::vector<VT *> h_slabs(m + 1, nullptr);
-    std::vector<double2 *> h_hcols(m, nullptr);
-    PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, st));
-    DevArray<double> Pinv;
-    const bool jac = rq.jacobi && rq.inner;
-    if (jac) {
-        DevArray<int32_t> d_fall;
-        d_fall.alloc(ctx, C);
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_fall.p, rq.freq.data(), C * 4, cudaMemcpyHostToDevice, st));
-        Pinv.alloc(ctx, (size_t)C * 2 * n);
-        diagonal_inverse(g, OpBatch{C, d_fall.p}, Pinv.p);
+    void begin() {
+        const int n = g_->n_var;
+        C_ = (int)rq_.freq.size();
+        m_ = std::min(rq_.m, n);
+        res_.status.assign(C_, PLX_OK);
+        res_.steps.assign(C_, 0);
+        res_.trace.assign(rq_.record_trace ? (size_t)C_ * m_ : 0, 0.0);
+        if (C_ == 0) return;
+        if (m_ < 1) throw Error(PLX_ERR_ARG, "GMRES dimension must be positive");
+        nchunk_ = n_blocks(n, kRows);
+        ndot_ = n_blocks(n, kDotRows);
+        if ((size_t)(m_ + 1) * sizeof(double2) > 200 * 1024) throw Error(PLX_ERR_ARG, "GMRES dimension above 12800");
+        once_per_device(reinterpret_cast<const void *>(tri_solve), ctx_->device, [] {
+            PLX_CHECK_CUDA(cudaFuncSetAttribute(tri_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+            PLX_CHECK_CUDA(cudaFuncSetAttribute(combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        });
+        hstride_ = m_ + 1;   // rows of an H column (0..m)
+        d_act_.alloc(ctx_, C_);
+        d_freq_act_.alloc(ctx_, C_);
+        d_cols_.alloc(ctx_, C_);
+        Xa_.alloc(ctx_, (size_t)C_ * 2 * n);
+        Wa_.alloc(ctx_, (size_t)C_ * 2 * n);
+        work_.alloc(ctx_, (size_t)C_ * 2 * n);
+        nrm_part_.alloc(ctx_, (size_t)C_ * nchunk_);
+        nrm_.alloc(ctx_, C_);
+        cs_.alloc(ctx_, (size_t)C_ * m_);
+        sn_.alloc(ctx_, (size_t)C_ * m_);
+        gv_.alloc(ctx_, (size_t)C_ * hstride_);
+        hbuf_.alloc(ctx_, (size_t)C_ * hstride_);
+        ybuf_.alloc(ctx_, (size_t)C_ * hstride_);
+        std::vector<DevArray<VT>>(m_ + 1).swap(slabs_);
+        std::vector<DevArray<double2>>(m_).swap(hcols_);
+        d_slabs_.alloc(ctx_, m_ + 1);
+        d_hcols_.alloc(ctx_, m_);
+        h_slabs_.assign(m_ + 1, nullptr);
+        h_hcols_.assign(m_, nullptr);
+        PLX_CHECK_CUDA(cudaMemsetAsync(d_X_, 0, (size_t)C_ * 2 * n * 8, st_));
+        jac_ = rq_.jacobi && rq_.inner;
+        if (jac_) {
+            DevArray<int32_t> d_fall;
+            d_fall.alloc(ctx_, C_);
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_fall.p, rq_.freq.data(), C_ * 4, cudaMemcpyHostToDevice, st_));
+            Pinv_.alloc(ctx_, (size_t)C_ * 2 * n);
+            diagonal_inverse(g_, OpBatch{C_, d_fall.p}, Pinv_.p);
+        }
+        // active list: every column with ||b|| > 0 (the reference returns x = 0 otherwise)
+        act_.resize(C_);
+        for (int c = 0; c < C_; ++c) act_[c] = c;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_act_.p, act_.data(), C_ * 4, cudaMemcpyHostToDevice, st_));
+        batch_norms(g_, C_, d_B_, nrm_part_, nrm_);   // B is [C] in column order == compact order here
+        std::vector<double> bnorm(C_);
+        PLX_CHECK_CUDA(cudaMemcpyAsync(bnorm.data(), nrm_.p, C_ * 8, cudaMemcpyDeviceToHost, st_));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st_));
+        slabs_[0].alloc(ctx_, (size_t)C_ * 2 * n);
+        h_slabs_[0] = slabs_[0].p;
+        start_vectors<VT><<<dim3(grid_rows(2LL * n), C_), 256, 0, st_>>>(n, d_act_.p, nrm_.p, d_B_, slabs_[0].p,
+                                                                      gv_.p, hstride_);
+        ctx_->launches++;
+        act_.clear();
+        for (int c = 0; c < C_; ++c) {
+            if (!std::isfinite(bnorm[c])) {
+                res_.status[c] = PLX_ERR_NAN;
+            } else if (bnorm[c] > 0.0) {
+                act_.push_back(c);
+            }
+        }
+        upload_active();
+        resid_.assign(C_, 0.0);
+        j_ = 0;
     }
 
-    // active list: every column with ||b|| > 0 (the reference returns x = 0 otherwise)
-    std::vector<int32_t> act(C);
-    for (int c = 0; c < C; ++c) act[c] = c;
-    PLX_CHECK_CUDA(cudaMemcpyAsync(d_act.p, act.data(), C * 4, cudaMemcpyHostToDevice, st));
-    batch_norms(g, C, d_B, nrm_part, nrm);   // B is [C] in column order == compact order here
-    std::vector<double> bnorm(C);
-    PLX_CHECK_CUDA(cudaMemcpyAsync(bnorm.data(), nrm.p, C * 8, cudaMemcpyDeviceToHost, st));
-    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
-    slabs[0].alloc(ctx, (size_t)C * 2 * n);
-    h_slabs[0] = slabs[0].p;
-    start_vectors<VT><<<dim3(grid_rows(2LL * n), C), 256, 0, st>>>(n, d_act.p, nrm.p, d_B, slabs[0].p,
-                                                              gv.p, hstride);
-    ctx->launches++;
-    act.clear();
-    for (int c = 0; c < C; ++c) {
-        if (!std::isfinite(bnorm[c])) {
-            res.status[c] = PLX_ERR_NAN;
-        } else if (bnorm[c] > 0.0) {
-            act.push_back(c);
-        }
-    }
-    auto upload_active = [&]() {
-        std::vector<int32_t> fa(act.size());
-        for (size_t k = 0; k < act.size(); ++k) fa[k] = rq.freq[act[k]];
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_act.p, act.data(), act.size() * 4, cudaMemcpyHostToDevice, st));
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_freq_act.p, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, st));
-    };
-    upload_active();
+    bool wants_product() const override { return C_ > 0 && j_ < m_ && !act_.empty(); }
 
-    std::vector<double> resid(C);
-    for (int j = 0; j < m && !act.empty(); ++j) {
-        const int na = (int)act.size();
-        // --- w = A v_j for every active column (one batched operator) -----------
-        gather_cols<VT><<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, h_slabs[j], Xa.p);
-        ctx->launches++;
-        if (jac) {
-            scale_cols<<<dim3(grid_rows(n), na), 256, 0, st>>>(n, d_act.p, Pinv.p, Xa.p, 0);
-            ctx->launches++;
+    // w = A v_j for every active column: the batch the caller multiplies
+    OpInput pre() override {
+        const int n = g_->n_var;
+        const int na = (int)act_.size();
+        gather_cols<VT><<<dim3(grid_rows(2LL * n), na), 256, 0, st_>>>(n, d_act_.p, h_slabs_[j_], Xa_.p);
+        ctx_->launches++;
+        if (jac_) {
+            scale_cols<<<dim3(grid_rows(n), na), 256, 0, st_>>>(n, d_act_.p, Pinv_.p, Xa_.p, 0);
+            ctx_->launches++;
         }
-        OpBatch ob{na, d_freq_act.p};
-        apply_operator(g, ob, Xa.p, Wa.p, work.p, rq.contraction);
-        // --- Arnoldi --------------------------------------------------------------
-        hcols[j].alloc(ctx, (size_t)C * hstride);
-        h_hcols[j] = hcols[j].p;
-        slabs[j + 1].alloc(ctx, (size_t)C * 2 * n);
-        h_slabs[j + 1] = slabs[j + 1].p;
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p + j + 1, &h_slabs[j + 1], sizeof(VT *),
-                                       cudaMemcpyHostToDevice, st));
+        return OpInput{g_, OpBatch{na, d_freq_act_.p}, Xa_.p, Wa_.p, work_.p, rq_.contraction};
+    }
+
+    // the Arnoldi step on W, the least-squares update and the convergence test
+    void post() override {
+        const int n = g_->n_var;
+        const int j = j_;
+        const int na = (int)act_.size();
+        hcols_[j].alloc(ctx_, (size_t)C_ * hstride_);
+        h_hcols_[j] = hcols_[j].p;
+        slabs_[j + 1].alloc(ctx_, (size_t)C_ * 2 * n);
+        h_slabs_[j + 1] = slabs_[j + 1].p;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs_.p + j + 1, &h_slabs_[j + 1], sizeof(VT *), cudaMemcpyHostToDevice, st_));
         if (j == 0)
-            PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs.p, &h_slabs[0], sizeof(VT *), cudaMemcpyHostToDevice, st));
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_hcols.p + j, &h_hcols[j], sizeof(double2 *),
-                                       cudaMemcpyHostToDevice, st));
-        PLX_CHECK_CUDA(cudaMemsetAsync(hcols[j].p, 0, (size_t)C * hstride * 16, st));
-        size_t need = (size_t)na * ndot * (j + 1);
-        if (part.n < need) part.alloc(ctx, std::max(need, part.n * 2));
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_slabs_.p, &h_slabs_[0], sizeof(VT *), cudaMemcpyHostToDevice, st_));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_hcols_.p + j, &h_hcols_[j], sizeof(double2 *), cudaMemcpyHostToDevice, st_));
+        PLX_CHECK_CUDA(cudaMemsetAsync(hcols_[j].p, 0, (size_t)C_ * hstride_ * 16, st_));
+        size_t need = (size_t)na * ndot_ * (j + 1);
+        if (part_.n < need) part_.alloc(ctx_, std::max(need, part_.n * 2));
         auto project = [&](int i0, int i1, int accumulate) {
             int ni = i1 - i0;
-            dots_partial<VT><<<dim3(ndot, na), kThreads, 0, st>>>(n, i0, i1, d_act.p, d_slabs.p, Wa.p, part.p);
-            dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st>>>(ndot, ni, i0, d_act.p, part.p,
-                                                                      hbuf.p, hcols[j].p, hstride,
-                                                                      accumulate);
-            ctx->launches += 2 + combine_chunked(st, n, i0, ni, na, d_act.p, d_slabs.p, hbuf.p, -1.0, Wa.p, 0);
+            dots_partial<VT><<<dim3(ndot_, na), kThreads, 0, st_>>>(n, i0, i1, d_act_.p, d_slabs_.p, Wa_.p, part_.p);
+            dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st_>>>(ndot_, ni, i0, d_act_.p, part_.p, hbuf_.p,
+                                                                       hcols_[j].p, hstride_, accumulate);
+            ctx_->launches += 2 + combine_chunked(st_, n, i0, ni, na, d_act_.p, d_slabs_.p, hbuf_.p, -1.0, Wa_.p, 0);
         };
-        prof_begin(ctx);
-        if (j + 1 < 25 && !rq.inner) {
+        prof_begin(ctx_);
+        if (j + 1 < 25 && !rq_.inner) {
             for (int i = 0; i <= j; ++i) project(i, i + 1, 0);        // modified Gram-Schmidt
         } else {
             project(0, j + 1, 0);                                     // classical GS ...
-            if (!rq.single_pass) project(0, j + 1, 1);                // ... and re-orthogonalise
+            if (!rq_.single_pass) project(0, j + 1, 1);               // ... and re-orthogonalise
         }
-        batch_norms(g, na, Wa.p, nrm_part, nrm);
-        prof_end(ctx, PROF_ORTHO, 0.0, 0.0);
-        prof_begin(ctx);
-        normalize<VT><<<dim3(grid_rows(2LL * n), na), 256, 0, st>>>(n, d_act.p, nrm.p, Wa.p, slabs[j + 1].p,
-                                                               hcols[j].p, hstride, j + 1);
-        givens<<<n_blocks(na, 128), 128, 0, st>>>(na, j, d_act.p, d_hcols.p, hstride, cs.p, sn.p, gv.p,
-                                                 hstride, m, nrm.p);
-        ctx->launches += 2;
-        prof_end(ctx, PROF_LSQ, 0.0, 0.0);
+        batch_norms(g_, na, Wa_.p, nrm_part_, nrm_);
+        prof_end(ctx_, PROF_ORTHO, 0.0, 0.0);
+        prof_begin(ctx_);
+        normalize<VT><<<dim3(grid_rows(2LL * n), na), 256, 0, st_>>>(n, d_act_.p, nrm_.p, Wa_.p, slabs_[j + 1].p,
+                                                                    hcols_[j].p, hstride_, j + 1);
+        givens<<<n_blocks(na, 128), 128, 0, st_>>>(na, j, d_act_.p, d_hcols_.p, hstride_, cs_.p, sn_.p, gv_.p,
+                                                  hstride_, m_, nrm_.p);
+        ctx_->launches += 2;
+        prof_end(ctx_, PROF_LSQ, 0.0, 0.0);
         PLX_CHECK_CUDA(cudaGetLastError());
-        PLX_CHECK_CUDA(cudaMemcpyAsync(resid.data(), nrm.p, na * 8, cudaMemcpyDeviceToHost, st));
-        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(resid_.data(), nrm_.p, na * 8, cudaMemcpyDeviceToHost, st_));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st_));
         // --- convergence test -----------------------------------------------------
         std::vector<int32_t> trig;
-        std::vector<int> trig_k;
         for (int k = 0; k < na; ++k) {
-            int c = act[k];
-            res.steps[c] = j + 1;
-            if (rq.record_trace) res.trace[(size_t)c * m + j] = resid[k];
-            const double tc = rq.tols.empty() ? rq.tol : rq.tols[c];
-            if (!std::isfinite(resid[k])) res.status[c] = PLX_ERR_NAN;
-            else if (resid[k] < tc || (rq.inner && j == m - 1)) trig.push_back(c);
+            int c = act_[k];
+            res_.steps[c] = j + 1;
+            if (rq_.record_trace) res_.trace[(size_t)c * m_ + j] = resid_[k];
+            const double tc = rq_.tols.empty() ? rq_.tol : rq_.tols[c];
+            if (!std::isfinite(resid_[k])) res_.status[c] = PLX_ERR_NAN;
+            else if (resid_[k] < tc || (rq_.inner && j == m_ - 1)) trig.push_back(c);
         }
-        std::vector<char> done(C, 0);
-        for (int c : act)
-            if (res.status[c] == PLX_ERR_NAN) done[c] = 1;
-        if (!trig.empty() && rq.inner) {
+        std::vector<char> done(C_, 0);
+        for (int c : act_)
+            if (res_.status[c] == PLX_ERR_NAN) done[c] = 1;
+        if (!trig.empty() && rq_.inner) {
             // inner solve of a refinement: take the least-squares solution as is
             const int nt = (int)trig.size();
-            PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
-            tri_solve<<<nt, 32, (j + 1) * sizeof(double2), st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p,
-                                                                 hstride, ybuf.p);
-            ctx->launches += 1 + combine_chunked(st, n, 0, j + 1, nt, d_cols.p, d_slabs.p, ybuf.p, 1.0, d_X, 1);
-            if (jac) {
-                scale_cols<<<dim3(grid_rows(n), nt), 256, 0, st>>>(n, d_cols.p, Pinv.p, d_X, 1);
-                ctx->launches++;
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols_.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st_));
+            tri_solve<<<nt, 32, (j + 1) * sizeof(double2), st_>>>(nt, j, d_cols_.p, d_hcols_.p, hstride_, gv_.p,
+                                                                  hstride_, ybuf_.p);
+            ctx_->launches += 1 + combine_chunked(st_, n, 0, j + 1, nt, d_cols_.p, d_slabs_.p, ybuf_.p, 1.0, d_X_, 1);
+            if (jac_) {
+                scale_cols<<<dim3(grid_rows(n), nt), 256, 0, st_>>>(n, d_cols_.p, Pinv_.p, d_X_, 1);
+                ctx_->launches++;
             }
             for (int c : trig) done[c] = 1;
             for (int c : trig)
-                if (resid[std::find(act.begin(), act.end(), c) - act.begin()] >= (rq.tols.empty() ? rq.tol : rq.tols[c]))
-                    res.status[c] = PLX_ERR_NOT_CONVERGED;   // inner dimension used up (not an error)
+                if (resid_[std::find(act_.begin(), act_.end(), c) - act_.begin()] >=
+                    (rq_.tols.empty() ? rq_.tol : rq_.tols[c]))
+                    res_.status[c] = PLX_ERR_NOT_CONVERGED;   // inner dimension used up (not an error)
         } else if (!trig.empty()) {
             const int nt = (int)trig.size();
-            PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st));
-            tri_solve<<<nt, 32, (j + 1) * sizeof(double2), st>>>(nt, j, d_cols.p, d_hcols.p, hstride, gv.p,
-                                                                 hstride, ybuf.p);
-            ctx->launches += combine_chunked(st, n, 0, j + 1, nt, d_cols.p, d_slabs.p, ybuf.p, 1.0, d_X, 1);
-            gather_x<<<dim3(grid_rows(2LL * n), nt), 256, 0, st>>>(n, d_cols.p, d_X, Xa.p);
-            ctx->launches += 2;
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_cols_.p, trig.data(), nt * 4, cudaMemcpyHostToDevice, st_));
+            tri_solve<<<nt, 32, (j + 1) * sizeof(double2), st_>>>(nt, j, d_cols_.p, d_hcols_.p, hstride_, gv_.p,
+                                                                  hstride_, ybuf_.p);
+            ctx_->launches += combine_chunked(st_, n, 0, j + 1, nt, d_cols_.p, d_slabs_.p, ybuf_.p, 1.0, d_X_, 1);
+            gather_x<<<dim3(grid_rows(2LL * n), nt), 256, 0, st_>>>(n, d_cols_.p, d_X_, Xa_.p);
+            ctx_->launches += 2;
             std::vector<int32_t> tf(nt);
-            for (int t = 0; t < nt; ++t) tf[t] = rq.freq[trig[t]];
+            for (int t = 0; t < nt; ++t) tf[t] = rq_.freq[trig[t]];
             DevArray<int32_t> d_tf;
-            d_tf.alloc(ctx, nt);
-            PLX_CHECK_CUDA(cudaMemcpyAsync(d_tf.p, tf.data(), nt * 4, cudaMemcpyHostToDevice, st));
+            d_tf.alloc(ctx_, nt);
+            PLX_CHECK_CUDA(cudaMemcpyAsync(d_tf.p, tf.data(), nt * 4, cudaMemcpyHostToDevice, st_));
             OpBatch tb{nt, d_tf.p};
-            apply_operator(g, tb, Xa.p, Wa.p, work.p, Contraction::FP64 == rq.contraction || Contraction::FP64_OTF == rq.contraction ? rq.contraction : Contraction::FP64);
-            residual<<<dim3(grid_rows(2LL * n), nt), 256, 0, st>>>(n, d_cols.p, d_B, Wa.p);
-            ctx->launches++;
-            batch_norms(g, nt, Wa.p, nrm_part, nrm);
+            apply_operator(g_, tb, Xa_.p, Wa_.p, work_.p,
+                           Contraction::FP64 == rq_.contraction || Contraction::FP64_OTF == rq_.contraction
+                               ? rq_.contraction
+                               : Contraction::FP64);
+            residual<<<dim3(grid_rows(2LL * n), nt), 256, 0, st_>>>(n, d_cols_.p, d_B_, Wa_.p);
+            ctx_->launches++;
+            batch_norms(g_, nt, Wa_.p, nrm_part_, nrm_);
             std::vector<double> tres(nt);
-            PLX_CHECK_CUDA(cudaMemcpyAsync(tres.data(), nrm.p, nt * 8, cudaMemcpyDeviceToHost, st));
-            PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+            PLX_CHECK_CUDA(cudaMemcpyAsync(tres.data(), nrm_.p, nt * 8, cudaMemcpyDeviceToHost, st_));
+            PLX_CHECK_CUDA(cudaStreamSynchronize(st_));
             for (int t = 0; t < nt; ++t)
-                if (tres[t] < rq.tol) done[trig[t]] = 1;
+                if (tres[t] < rq_.tol) done[trig[t]] = 1;
                 else if (!std::isfinite(tres[t])) {
-                    res.status[trig[t]] = PLX_ERR_NAN;
+                    res_.status[trig[t]] = PLX_ERR_NAN;
                     done[trig[t]] = 1;
                 }
         }
         std::vector<int32_t> keep;
-        for (int c : act)
+        for (int c : act_)
             if (!done[c]) keep.push_back(c);
-        if (keep.size() != act.size()) {
-            act.swap(keep);
-            if (!act.empty()) upload_active();
+        if (keep.size() != act_.size()) {
+            act_.swap(keep);
+            if (!act_.empty()) upload_active();
         }
+        ++j_;
     }
-    for (int c : act) res.status[c] = PLX_ERR_NOT_CONVERGED;
-    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+
+    void end() override {
+        for (int c : act_) res_.status[c] = PLX_ERR_NOT_CONVERGED;
+        act_.clear();
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st_));
+    }
+
+  private:
+    void upload_active() {
+        std::vector<int32_t> fa(act_.size());
+        for (size_t k = 0; k < act_.size(); ++k) fa[k] = rq_.freq[act_[k]];
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_act_.p, act_.data(), act_.size() * 4, cudaMemcpyHostToDevice, st_));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(d_freq_act_.p, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, st_));
+    }
+
+    plx_geom *g_;
+    plx_ctx *ctx_;
+    cudaStream_t st_;
+    GmresRequest rq_;
+    const double *d_B_;
+    double *d_X_;
+    GmresResult &res_;
+    int C_ = 0, m_ = 0, j_ = 0, nchunk_ = 0, ndot_ = 0, hstride_ = 0;
+    bool jac_ = false;
+    std::vector<int32_t> act_;
+    std::vector<double> resid_;
+    DevArray<int32_t> d_act_, d_freq_act_, d_cols_;
+    DevArray<double> Xa_, Wa_, work_, nrm_part_, nrm_, cs_, Pinv_;
+    DevArray<double2> sn_, gv_, hbuf_, part_, ybuf_;
+    std::vector<DevArray<VT>> slabs_;
+    std::vector<DevArray<double2>> hcols_;
+    DevArray<VT *> d_slabs_;
+    DevArray<double2 *> d_hcols_;
+    std::vector<VT *> h_slabs_;
+    std::vector<double2 *> h_hcols_;
+};
+
+std::unique_ptr<GmresStepper> make_gmres(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
+                                         GmresResult &res) {
+    if (rq.inner && rq.basis_fp32) {
+        auto r = std::make_unique<GmresRun<float>>(g, rq, d_B, d_X, res);
+        r->begin();
+        return r;
+    }
+    auto r = std::make_unique<GmresRun<double>>(g, rq, d_B, d_X, res);
+    r->begin();
+    return r;
 }
 
 void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
                    GmresResult &res) {
-    if (rq.inner && rq.basis_fp32)
-        gmres_impl<float>(g, rq, d_B, d_X, res);
-    else
-        gmres_impl<double>(g, rq, d_B, d_X, res);
+    auto run = make_gmres(g, rq, d_B, d_X, res);
+    while (run->wants_product()) {
+        OpInput in = run->pre();
+        apply_operator(in.g, in.b, in.X, in.Y, in.work, in.how);
+        run->post();
+    }
+    run->end();
 }
 
 }  // namespace plx

@@ -713,6 +713,42 @@ static void finish_rows(plx_geom *g, const OpBatch &b, const double *S, const do
     PLX_CHECK_CUDA(cudaGetLastError());
 }
 
+// Output of the folded tensor-core contraction of b.count columns: the work
+// array, or for alloys (interface rows after the n operator rows) the
+// geometry's fold buffer.
+static double *folded_output(plx_geom *g, const OpBatch &b, double *work) {
+    const int64_t M = tc_fold_rows(g);
+    if (M <= g->n_var) return work;
+    const size_t need = (size_t)b.count * 2 * M;
+    if (g->d_fold_work.n < need) g->d_fold_work.alloc(g->ctx, need);
+    return g->d_fold_work.p;
+}
+
+// Y = S + D(w) X after the folded contraction S = A0 X (and the interface
+// correction of alloys).
+static void folded_finish(plx_geom *g, const OpBatch &b, const double *S, const double *X, double *Y) {
+    plx_ctx *ctx = g->ctx;
+    const int64_t M = g->fold_rows;
+    prof_begin(ctx);
+    folded_rows<<<dim3(n_blocks(g->n_var, 256), b.count), 256, 0, ctx->stream>>>(
+        g->n_atoms, g->n_types, g->n_var, M, b.count, b.d_freq, g->d_type.p, g->d_dq.p, g->d_frac.p,
+        g->d_inv_alpha.p, S, X, Y);
+    ctx->launches++;
+    if (g->n_xrows > 0) {
+        iface_rows<<<dim3(n_blocks(g->n_xrows, 128), b.count), 128, 0, ctx->stream>>>(
+            g->n_xrows, b.count, g->n_types, g->n_var, M, b.d_freq, g->d_type.p, g->d_xrow.p, g->d_xipos.p,
+            g->d_xrowptr.p, g->d_xcol.p, g->d_xtj.p, g->d_xkt.p, g->d_wratio.p, S, Y);
+        ctx->launches++;
+    }
+    PLX_CHECK_CUDA(cudaGetLastError());
+    prof_end(ctx, PROF_ROWS, 0.0, 0.0);
+}
+
+static double tc_bytes(plx_geom *g, Contraction how, int count) {
+    const double nn = (double)g->n_var;
+    return (how == Contraction::TC3 ? 4.0 : 2.0) * (double)g->fold_rows * (double)g->ldk + 2.0 * 8.0 * nn * 2.0 * count;
+}
+
 void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, double *work,
                     Contraction how) {
     if (b.count == 0) return;
@@ -721,31 +757,11 @@ void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, d
         // matrix and a diagonal pass (no conductance rows per application)
         plx_ctx *ctx = g->ctx;
         const double nn = (double)g->n_var;
-        const int64_t M = tc_fold_rows(g);
-        double *S = work;
-        if (M > g->n_var) {
-            // alloys: the output carries the interface rows after the n operator rows
-            const size_t need = (size_t)b.count * 2 * M;
-            if (g->d_fold_work.n < need) g->d_fold_work.alloc(ctx, need);
-            S = g->d_fold_work.p;
-        }
+        double *S = folded_output(g, b, work);
         prof_begin(ctx);
         tc_contract(g, b.count, X, S, how == Contraction::TC3 ? 3 : 1, true);
-        prof_end(ctx, PROF_TC, 2.0 * nn * nn * 2.0 * b.count,
-                 (how == Contraction::TC3 ? 4.0 : 2.0) * (double)M * (double)g->ldk + 2.0 * 8.0 * nn * 2.0 * b.count);
-        prof_begin(ctx);
-        folded_rows<<<dim3(n_blocks(g->n_var, 256), b.count), 256, 0, ctx->stream>>>(
-            g->n_atoms, g->n_types, g->n_var, M, b.count, b.d_freq, g->d_type.p, g->d_dq.p, g->d_frac.p,
-            g->d_inv_alpha.p, S, X, Y);
-        ctx->launches++;
-        if (g->n_xrows > 0) {
-            iface_rows<<<dim3(n_blocks(g->n_xrows, 128), b.count), 128, 0, ctx->stream>>>(
-                g->n_xrows, b.count, g->n_types, g->n_var, M, b.d_freq, g->d_type.p, g->d_xrow.p, g->d_xipos.p,
-                g->d_xrowptr.p, g->d_xcol.p, g->d_xtj.p, g->d_xkt.p, g->d_wratio.p, S, Y);
-            ctx->launches++;
-        }
-        PLX_CHECK_CUDA(cudaGetLastError());
-        prof_end(ctx, PROF_ROWS, 0.0, 0.0);
+        prof_end(ctx, PROF_TC, 2.0 * nn * nn * 2.0 * b.count, tc_bytes(g, how, b.count));
+        folded_finish(g, b, S, X, Y);
         return;
     }
     contract_t(g, b.count, X, work, how);
@@ -755,6 +771,50 @@ void apply_operator(plx_geom *g, const OpBatch &b, const double *X, double *Y, d
     else
         finish_rows(g, b, work, X, Y);
     prof_end(g->ctx, PROF_ROWS, 0.0, 0.0);
+}
+
+void apply_operator_group(const std::vector<OpInput> &items) {
+    // the folded tensor-core contractions that can share a launch: same context,
+    // same product count, distinct geometries
+    std::vector<size_t> grp;
+    for (size_t i = 0; i < items.size(); ++i) {
+        const OpInput &it = items[i];
+        if (it.b.count == 0 || !(it.how == Contraction::TC3 || it.how == Contraction::TC1) ||
+            !tc_folds_operator(it.g))
+            continue;
+        bool ok = true;
+        for (size_t k : grp)
+            ok = ok && items[k].g != it.g && items[k].g->ctx == it.g->ctx && items[k].how == it.how;
+        if (ok) grp.push_back(i);
+    }
+    if (grp.size() < 2) {
+        for (const OpInput &it : items) apply_operator(it.g, it.b, it.X, it.Y, it.work, it.how);
+        return;
+    }
+    plx_ctx *ctx = items[grp[0]].g->ctx;
+    std::vector<TcItem> ti;
+    std::vector<double *> S;
+    double flops = 0.0, bytes = 0.0;
+    for (size_t k : grp) {
+        const OpInput &it = items[k];
+        S.push_back(folded_output(it.g, it.b, it.work));
+        ti.push_back(TcItem{it.g, it.b.count, it.X, S.back(), it.how == Contraction::TC3 ? 3 : 1, true});
+        const double nn = (double)it.g->n_var;
+        flops += 2.0 * nn * nn * 2.0 * it.b.count;
+        bytes += tc_bytes(it.g, it.how, it.b.count);
+    }
+    prof_begin(ctx);
+    tc_contract_group(ti);
+    prof_end(ctx, PROF_TC, flops, bytes);
+    for (size_t j = 0; j < grp.size(); ++j) {
+        const OpInput &it = items[grp[j]];
+        folded_finish(it.g, it.b, S[j], it.X, it.Y);
+    }
+    for (size_t i = 0; i < items.size(); ++i)
+        if (std::find(grp.begin(), grp.end(), i) == grp.end()) {
+            const OpInput &it = items[i];
+            apply_operator(it.g, it.b, it.X, it.Y, it.work, it.how);
+        }
 }
 
 void rhs_batch(plx_geom *g, const OpBatch &b, const int32_t *d_pol, double *Bout) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
@@ -172,6 +173,8 @@ struct plx_geom {
     // split-K partial sums of the few-column contraction (grown on demand;
     // used only by work ordered on the context's single stream)
     plx::DevArray<double> d_part;
+    // continuous batches open on this geometry (they own its frequency table)
+    int open_batches = 0;
     // timing of the last plx_solve
     double last_ms = 0.0;
     int64_t last_launches = 0;
@@ -216,6 +219,17 @@ void diagonal_inverse(plx_geom *g, const OpBatch &b, double *Pinv);
 // (nprod 3: Th Xh + Th Xl + Tl Xh; nprod 1: Th Xh).  X, S: [count][2][n] FP64.
 void build_t_split(plx_geom *g);
 void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded = false);
+// Several contractions (geometries of one context, same product count) in ONE
+// launch: every CTA finds its contraction and tile in a table of groups.
+struct TcItem {
+    plx_geom *g;
+    int count;
+    const double *X;
+    double *S;
+    int nprod;
+    bool folded;
+};
+void tc_contract_group(const std::vector<TcItem> &items);
 // true when apply_operator contracts with the folded A0 on the tensor cores:
 // every atomistic geometry (T stored or generated; alloys with the interface
 // correction)
@@ -269,6 +283,33 @@ struct GmresResult {
 // B and X are [C][2][n] device arrays; X receives the solutions.
 void gmres_batched(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
                    GmresResult &res);
+// An operator application a solve asks for: Y = A(w) X on the batch b of
+// geometry g, with `work` scratch of the same size as X.
+struct OpInput {
+    plx_geom *g;
+    OpBatch b;
+    const double *X;
+    double *Y;
+    double *work;
+    Contraction how;
+};
+// A batched GMRES advanced one Arnoldi step at a time (make_gmres has run the
+// set-up): while wants_product(): pre() returns the batch to multiply, the
+// caller writes its product to OpInput::Y, then post(); finally end().  B, X
+// and res must outlive the stepper.
+struct GmresStepper {
+    virtual ~GmresStepper() = default;
+    virtual bool wants_product() const = 0;
+    virtual OpInput pre() = 0;
+    virtual void post() = 0;
+    virtual void end() = 0;
+};
+std::unique_ptr<GmresStepper> make_gmres(plx_geom *g, const GmresRequest &rq, const double *d_B, double *d_X,
+                                         GmresResult &res);
+// Several operator applications at once: the tensor-core contractions of
+// folded atomistic geometries that share a context are ONE grouped launch; any
+// other application runs on its own.
+void apply_operator_group(const std::vector<OpInput> &items);
 
 // refine.cu: iterative refinement -- FP64 residuals r = b - A x outside, an
 // inner GMRES of dimension inner_m with `inner` contraction on A d = r to a
@@ -292,6 +333,68 @@ struct RefineResult {
     std::vector<double> residual;     // final ||b - A x||
 };
 void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, double *d_X, RefineResult &res);
+
+// Columns of a refinement in slots [cap][2][n]: right-hand sides B, solutions X
+// and FP64 residuals R, with per-slot bookkeeping.  attach() works on arrays the
+// caller owns (one solve of C columns); own() + grow() keep them in the state
+// (continuous batching: columns come and go between outer steps).
+struct RefineState {
+    struct Slot {
+        enum State { FREE = 0, ACTIVE = 1, FINISHED = 2 } state = FREE;
+        int32_t freq = 0, pol = 0;
+        double tol = 0.0;               // absolute
+        int32_t status = PLX_ERR_NOT_CONVERGED;
+        int32_t outer = 0, inner_steps = 0;
+        double residual = 0.0;
+        int64_t tag = -1;               // request of a continuous batch
+    };
+    plx_geom *g = nullptr;
+    RefineRequest rq;
+    int cap = 0;
+    const double *B = nullptr;
+    double *X = nullptr;
+    DevArray<double> R, ownB, ownX;
+    // scratch of an outer step, cap columns
+    DevArray<double> Ba, Da, AXa, nrm, Dacc, Bc, Wc;
+    DevArray<int32_t> d_idx, d_fa, d_sub, d_fsub;
+    std::vector<Slot> slots;
+    void attach(plx_geom *geom, const RefineRequest &settings, int n_slots, const double *d_B, double *d_X);
+    void own(plx_geom *geom, const RefineRequest &settings);
+    int grow(int need);
+    // residual norms of the ACTIVE slots: converged, non-finite or out of outer
+    // steps become FINISHED with their status
+    void update_status();
+
+  private:
+    void scratch(int n_cols);
+};
+
+// One outer refinement step over a state's ACTIVE slots: begin() (false when
+// none is active), then while advance(&need): the caller computes the inner
+// operator product `need` and calls product_done(); advance() returning false
+// means the step (inner cycles, x += d, FP64 residual) is complete.
+class OuterStep {
+  public:
+    explicit OuterStep(RefineState &s);
+    ~OuterStep();
+    bool begin();
+    bool advance(OpInput *need);
+    void product_done();
+
+  private:
+    RefineState &s_;
+    std::vector<int32_t> act_, fa_, cur_;
+    std::vector<double> tol_k_;
+    GmresRequest in_, rin_;
+    GmresResult ir_;
+    std::unique_ptr<GmresStepper> run_;
+    const double *bc_ = nullptr;
+    int cyc_ = 0;
+    bool done_ = true;
+};
+// One outer step of several states (geometries sharing a context) whose inner
+// Arnoldi steps share one grouped operator application per step.
+void refine_group_step(const std::vector<RefineState *> &states);
 
 // analysis.cu: induced field (3 complex per point) and density (1 complex per
 // point) of one solution x (complex interleaved, n_var) at P points [3][P] bohr

@@ -17,8 +17,17 @@
 // for up to max_cycles cycles before the outer step pays for an FP64 residual:
 // the FP64 product, the expensive one, is then spent once per inner_rel of
 // progress instead of once per inner_m Arnoldi steps.
+//
+// The columns live in slots of a RefineState; an OuterStep advances all of a
+// state's active columns by one outer step and can hand out its inner
+// operator products one Arnoldi step at a time, so that the outer steps of
+// several states (several geometries) share one grouped contraction per step
+// (refine_group_step).  solve_refined runs the outer steps of one state to the
+// end; the continuous-batching entry points (plx_batch_*) run one outer step at
+// a time and add or remove columns between steps.
 #include <algorithm>
 #include <cmath>
+#include <memory>
 
 #include "plx_internal.h"
 
@@ -67,10 +76,11 @@ __global__ void scatter_residual(int n, const int32_t *__restrict__ idx, const d
         r[t] = b[t] - a[t];
 }
 
-// ||v_c||_2 for every column, one block per column (fixed summation order).
-__global__ void column_norms(int n, const double *__restrict__ V, double *__restrict__ out) {
-    int c = blockIdx.x;
-    const double *v = V + (int64_t)c * 2 * n;
+// ||v_idx[k]||_2 for every listed slot, one block per slot (fixed summation order).
+__global__ void column_norms(int n, const int32_t *__restrict__ idx, const double *__restrict__ V,
+                             double *__restrict__ out) {
+    int k = blockIdx.x;
+    const double *v = V + (int64_t)idx[k] * 2 * n;
     double s = 0.0;
     for (int64_t t = threadIdx.x; t < 2LL * n; t += blockDim.x) s += v[t] * v[t];
     __shared__ double red[32];
@@ -80,7 +90,7 @@ __global__ void column_norms(int n, const double *__restrict__ V, double *__rest
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        out[c] = sqrt(t);
+        out[k] = sqrt(t);
     }
 }
 
@@ -88,9 +98,274 @@ int grid_cols(int n) { return std::min(n_blocks(2LL * n, 256), 512); }
 
 }  // namespace
 
-void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, double *d_X, RefineResult &res) {
+// ---------------------------------------------------------------------------
+// RefineState: slots of columns
+// ---------------------------------------------------------------------------
+
+void RefineState::attach(plx_geom *geom, const RefineRequest &settings, int n_slots, const double *d_B, double *d_X) {
+    g = geom;
+    rq = settings;
+    cap = n_slots;
+    B = d_B;
+    X = d_X;
+    R.alloc(g->ctx, (size_t)cap * 2 * g->n_var);
+    scratch(cap);
+    slots.assign(cap, Slot());
+}
+
+void RefineState::own(plx_geom *geom, const RefineRequest &settings) {
+    g = geom;
+    rq = settings;
+    cap = 0;
+    B = nullptr;
+    X = nullptr;
+}
+
+void RefineState::scratch(int n_cols) {
+    plx_ctx *ctx = g->ctx;
+    const size_t count = (size_t)n_cols * 2 * g->n_var;
+    Ba.alloc(ctx, count);
+    Da.alloc(ctx, count);
+    AXa.alloc(ctx, count);
+    if (rq.max_cycles > 1) {
+        Dacc.alloc(ctx, count);
+        Bc.alloc(ctx, count);
+        Wc.alloc(ctx, count);
+        d_sub.alloc(ctx, n_cols);
+        d_fsub.alloc(ctx, n_cols);
+    }
+    nrm.alloc(ctx, n_cols);
+    d_idx.alloc(ctx, n_cols);
+    d_fa.alloc(ctx, n_cols);
+}
+
+int RefineState::grow(int need) {
+    // owned storage only (the continuous-batching state): keeps every slot's data
+    if (need <= cap) return cap;
+    plx_ctx *ctx = g->ctx;
+    const int n = g->n_var;
+    const int ncap = std::max(need, std::max(16, 2 * cap));
+    DevArray<double> nB, nX, nR;
+    nB.alloc(ctx, (size_t)ncap * 2 * n);
+    nX.alloc(ctx, (size_t)ncap * 2 * n);
+    nR.alloc(ctx, (size_t)ncap * 2 * n);
+    if (cap > 0) {
+        const size_t b = (size_t)cap * 2 * n * 8;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(nB.p, ownB.p, b, cudaMemcpyDeviceToDevice, ctx->stream));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(nX.p, ownX.p, b, cudaMemcpyDeviceToDevice, ctx->stream));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(nR.p, R.p, b, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    std::swap(ownB.p, nB.p);
+    std::swap(ownB.n, nB.n);
+    std::swap(ownX.p, nX.p);
+    std::swap(ownX.n, nX.n);
+    std::swap(R.p, nR.p);
+    std::swap(R.n, nR.n);
+    nB.ctx = nX.ctx = nR.ctx = ctx;
+    ownB.ctx = ownX.ctx = R.ctx = ctx;
+    B = ownB.p;
+    X = ownX.p;
+    cap = ncap;
+    slots.resize(cap);
+    scratch(cap);
+    return cap;
+}
+
+void RefineState::update_status() {
     plx_ctx *ctx = g->ctx;
     cudaStream_t st = ctx->stream;
+    const int n = g->n_var;
+    std::vector<int32_t> idx;
+    for (int c = 0; c < cap; ++c)
+        if (slots[c].state == Slot::ACTIVE) idx.push_back(c);
+    if (idx.empty()) return;
+    const int k = (int)idx.size();
+    PLX_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, idx.data(), k * 4, cudaMemcpyHostToDevice, st));
+    column_norms<<<k, 256, 0, st>>>(n, d_idx.p, R.p, nrm.p);
+    ctx->launches++;
+    std::vector<double> rn(k);
+    PLX_CHECK_CUDA(cudaMemcpyAsync(rn.data(), nrm.p, k * 8, cudaMemcpyDeviceToHost, st));
+    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+    for (int t = 0; t < k; ++t) {
+        Slot &s = slots[idx[t]];
+        s.residual = rn[t];
+        if (!std::isfinite(rn[t])) {
+            s.status = PLX_ERR_NAN;
+            s.state = Slot::FINISHED;
+        } else if (rn[t] < s.tol) {
+            s.status = PLX_OK;
+            s.state = Slot::FINISHED;
+        } else if (s.outer >= rq.max_outer) {
+            s.status = PLX_ERR_NOT_CONVERGED;
+            s.state = Slot::FINISHED;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// OuterStep
+// ---------------------------------------------------------------------------
+
+OuterStep::OuterStep(RefineState &s) : s_(s) {}
+OuterStep::~OuterStep() = default;
+
+bool OuterStep::begin() {
+    RefineState &S = s_;
+    plx_geom *g = S.g;
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = g->n_var;
+    S.update_status();
+    act_.clear();
+    for (int c = 0; c < S.cap; ++c)
+        if (S.slots[c].state == RefineState::Slot::ACTIVE) act_.push_back(c);
+    if (act_.empty()) return false;
+    TraceRange trace_("refinement step");
+    const int na = (int)act_.size();
+    in_ = GmresRequest();
+    in_.m = S.rq.inner_m;
+    in_.contraction = S.rq.inner_contraction;
+    in_.inner = true;
+    in_.jacobi = S.rq.jacobi;
+    // a tensor-core inner solve is accurate to ~1e-6 at best: an FP32 basis costs nothing in accuracy
+    in_.basis_fp32 = S.rq.inner_contraction == Contraction::TC3 || S.rq.inner_contraction == Contraction::TC1;
+    // one Gram-Schmidt pass keeps an FP32 basis orthogonal enough up to 64 vectors
+    // (measured); longer inner solves re-orthogonalise
+    in_.single_pass = in_.basis_fp32 && S.rq.single_pass_gs && S.rq.inner_m <= 64;
+    fa_.assign(na, 0);
+    tol_k_.assign(na, 0.0);
+    for (int k = 0; k < na; ++k) {
+        const RefineState::Slot &sl = S.slots[act_[k]];
+        fa_[k] = sl.freq;
+        in_.freq.push_back(sl.freq);
+        in_.pol.push_back(sl.pol);
+        // no point asking the inner solve for more than the outer tolerance
+        tol_k_[k] = std::max(S.rq.inner_rel * sl.residual, 0.5 * sl.tol);
+        in_.tols.push_back(tol_k_[k]);
+    }
+    PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_idx.p, act_.data(), na * 4, cudaMemcpyHostToDevice, st));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_fa.p, fa_.data(), na * 4, cudaMemcpyHostToDevice, st));
+    gather_idx<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, S.d_idx.p, S.R.p, S.Ba.p);
+    ctx->launches++;
+    cur_.resize(na);
+    for (int k = 0; k < na; ++k) cur_[k] = k;
+    cyc_ = 0;
+    bc_ = S.Ba.p;
+    ir_ = GmresResult();
+    run_ = make_gmres(g, in_, S.Ba.p, S.Da.p, ir_);
+    done_ = false;
+    return true;
+}
+
+bool OuterStep::advance(OpInput *need) {
+    RefineState &S = s_;
+    plx_geom *g = S.g;
+    plx_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = g->n_var;
+    const int na = (int)act_.size();
+    while (!done_) {
+        if (run_->wants_product()) {
+            *need = run_->pre();
+            return true;
+        }
+        run_->end();
+        // a cycle ended: count its steps, keep its correction
+        for (size_t t = 0; t < cur_.size(); ++t) S.slots[act_[cur_[t]]].inner_steps += ir_.steps[t];
+        if (S.rq.max_cycles > 1) {
+            if (cyc_ == 0) {
+                PLX_CHECK_CUDA(cudaMemcpyAsync(S.Dacc.p, S.Da.p, (size_t)na * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
+            } else {
+                PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_sub.p, cur_.data(), cur_.size() * 4, cudaMemcpyHostToDevice, st));
+                scatter_add<<<dim3(grid_cols(n), (unsigned)cur_.size()), 256, 0, st>>>(n, S.d_sub.p, S.Da.p,
+                                                                                       S.Dacc.p);
+                ctx->launches++;
+            }
+            // restarts: columns whose cycle ended on the full basis continue from
+            // their inner residual
+            std::vector<int32_t> sub, pos, fsub;
+            for (size_t t = 0; t < cur_.size(); ++t)
+                if (ir_.status[t] == PLX_ERR_NOT_CONVERGED) {
+                    sub.push_back((int32_t)t);
+                    pos.push_back(cur_[t]);
+                    fsub.push_back(fa_[cur_[t]]);
+                }
+            if (!sub.empty() && cyc_ + 1 < S.rq.max_cycles) {
+                const int ns = (int)sub.size();
+                PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_sub.p, sub.data(), ns * 4, cudaMemcpyHostToDevice, st));
+                PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_fsub.p, fsub.data(), ns * 4, cudaMemcpyHostToDevice, st));
+                // Bc = b_cycle[sub] - A d_cycle[sub]   (inner contraction)
+                gather_idx<<<dim3(grid_cols(n), ns), 256, 0, st>>>(n, S.d_sub.p, S.Da.p, S.AXa.p);
+                ctx->launches++;
+                apply_operator(g, OpBatch{ns, S.d_fsub.p}, S.AXa.p, S.Da.p, S.Wc.p, S.rq.inner_contraction);
+                compact_residual<<<dim3(grid_cols(n), ns), 256, 0, st>>>(n, S.d_sub.p, bc_, S.Da.p, S.AXa.p);
+                ctx->launches++;
+                PLX_CHECK_CUDA(cudaMemcpyAsync(S.Bc.p, S.AXa.p, (size_t)ns * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
+                bc_ = S.Bc.p;
+                rin_ = in_;
+                rin_.freq.clear();
+                rin_.pol.clear();
+                rin_.tols.clear();
+                for (int t = 0; t < ns; ++t) {
+                    rin_.freq.push_back(in_.freq[pos[t]]);
+                    rin_.pol.push_back(in_.pol[pos[t]]);
+                    rin_.tols.push_back(tol_k_[pos[t]]);
+                }
+                cur_ = pos;
+                ++cyc_;
+                ir_ = GmresResult();
+                run_ = make_gmres(g, rin_, S.Bc.p, S.Da.p, ir_);
+                continue;
+            }
+            PLX_CHECK_CUDA(cudaMemcpyAsync(S.Da.p, S.Dacc.p, (size_t)na * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
+        }
+        // x += d ; FP64 residual r = b - A x of the active columns
+        PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_idx.p, act_.data(), na * 4, cudaMemcpyHostToDevice, st));
+        PLX_CHECK_CUDA(cudaMemcpyAsync(S.d_fa.p, fa_.data(), na * 4, cudaMemcpyHostToDevice, st));
+        scatter_add<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, S.d_idx.p, S.Da.p, S.X);
+        gather_idx<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, S.d_idx.p, S.X, S.Ba.p);
+        ctx->launches += 2;
+        apply_operator(g, OpBatch{na, S.d_fa.p}, S.Ba.p, S.AXa.p, S.Da.p, S.rq.outer_contraction);
+        scatter_residual<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, S.d_idx.p, S.B, S.AXa.p, S.R.p);
+        ctx->launches++;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        for (int c : act_) S.slots[c].outer += 1;
+        run_.reset();
+        done_ = true;
+    }
+    return false;
+}
+
+void OuterStep::product_done() { run_->post(); }
+
+// ---------------------------------------------------------------------------
+
+void refine_group_step(const std::vector<RefineState *> &states) {
+    std::vector<std::unique_ptr<OuterStep>> steps;
+    for (RefineState *s : states) {
+        auto os = std::make_unique<OuterStep>(*s);
+        if (os->begin()) steps.push_back(std::move(os));
+    }
+    std::vector<OpInput> need;
+    std::vector<OuterStep *> who;
+    for (;;) {
+        need.clear();
+        who.clear();
+        for (auto &os : steps) {
+            OpInput in{};
+            if (os->advance(&in)) {
+                need.push_back(in);
+                who.push_back(os.get());
+            }
+        }
+        if (need.empty()) break;
+        apply_operator_group(need);
+        for (OuterStep *os : who) os->product_done();
+    }
+}
+
+void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, double *d_X, RefineResult &res) {
+    plx_ctx *ctx = g->ctx;
     const int n = g->n_var;
     const int C = (int)rq.freq.size();
     res.status.assign(C, PLX_ERR_NOT_CONVERGED);
@@ -98,134 +373,32 @@ void solve_refined(plx_geom *g, const RefineRequest &rq, const double *d_B, doub
     res.outer.assign(C, 0);
     res.residual.assign(C, 0.0);
     if (C == 0) return;
-    DevArray<double> R, Ba, Da, AXa, nrm, Dacc, Bc, Wc;
-    DevArray<int32_t> d_idx, d_fa, d_sub, d_fsub;
-    R.alloc(ctx, (size_t)C * 2 * n);
-    Ba.alloc(ctx, (size_t)C * 2 * n);
-    Da.alloc(ctx, (size_t)C * 2 * n);
-    AXa.alloc(ctx, (size_t)C * 2 * n);
-    nrm.alloc(ctx, C);
-    d_idx.alloc(ctx, C);
-    d_fa.alloc(ctx, C);
-    const int max_cycles = std::max(1, rq.max_cycles);
-    if (max_cycles > 1) {
-        Dacc.alloc(ctx, (size_t)C * 2 * n);
-        Bc.alloc(ctx, (size_t)C * 2 * n);
-        Wc.alloc(ctx, (size_t)C * 2 * n);
-        d_sub.alloc(ctx, C);
-        d_fsub.alloc(ctx, C);
+    RefineState S;
+    S.attach(g, rq, C, d_B, d_X);
+    for (int c = 0; c < C; ++c) {
+        RefineState::Slot &sl = S.slots[c];
+        sl.state = RefineState::Slot::ACTIVE;
+        sl.freq = rq.freq[c];
+        sl.pol = rq.pol[c];
+        sl.tol = rq.tol;
     }
-    PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, st));
-    PLX_CHECK_CUDA(cudaMemcpyAsync(R.p, d_B, (size_t)C * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
-    std::vector<double> rn(C);
-    std::vector<char> live(C, 1);
-    for (int outer = 0;; ++outer) {
-        TraceRange trace_("refinement step");
-        column_norms<<<C, 256, 0, st>>>(n, R.p, nrm.p);
-        ctx->launches++;
-        PLX_CHECK_CUDA(cudaMemcpyAsync(rn.data(), nrm.p, C * 8, cudaMemcpyDeviceToHost, st));
-        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
-        std::vector<int32_t> act;
-        for (int c = 0; c < C; ++c) {
-            if (!live[c]) continue;
-            res.residual[c] = rn[c];
-            if (!std::isfinite(rn[c])) {
-                res.status[c] = PLX_ERR_NAN;
-                live[c] = 0;
-            } else if (rn[c] < rq.tol) {
-                res.status[c] = PLX_OK;
-                live[c] = 0;
-            } else {
-                act.push_back(c);
-            }
+    PLX_CHECK_CUDA(cudaMemsetAsync(d_X, 0, (size_t)C * 2 * n * 8, ctx->stream));
+    PLX_CHECK_CUDA(cudaMemcpyAsync(S.R.p, d_B, (size_t)C * 2 * n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    for (;;) {
+        OuterStep os(S);
+        if (!os.begin()) break;
+        OpInput need{};
+        while (os.advance(&need)) {
+            apply_operator(need.g, need.b, need.X, need.Y, need.work, need.how);
+            os.product_done();
         }
-        if (act.empty() || outer >= rq.max_outer) break;
-        const int na = (int)act.size();
-        std::vector<int32_t> fa(na);
-        GmresRequest in;
-        in.m = rq.inner_m;
-        in.contraction = rq.inner_contraction;
-        in.inner = true;
-        in.jacobi = rq.jacobi;
-        // a tensor-core inner solve is accurate to ~1e-6 at best: an FP32 basis costs nothing in accuracy
-        in.basis_fp32 = rq.inner_contraction == Contraction::TC3 || rq.inner_contraction == Contraction::TC1;
-        // one Gram-Schmidt pass keeps an FP32 basis orthogonal enough up to 64 vectors
-        // (measured); longer inner solves re-orthogonalise
-        in.single_pass = in.basis_fp32 && rq.single_pass_gs && rq.inner_m <= 64;
-        std::vector<double> tol_k(na);
-        for (int k = 0; k < na; ++k) {
-            int c = act[k];
-            fa[k] = rq.freq[c];
-            in.freq.push_back(rq.freq[c]);
-            in.pol.push_back(rq.pol[c]);
-            // no point asking the inner solve for more than the outer tolerance
-            tol_k[k] = std::max(rq.inner_rel * rn[c], 0.5 * rq.tol);
-            in.tols.push_back(tol_k[k]);
-        }
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_idx.p, act.data(), na * 4, cudaMemcpyHostToDevice, st));
-        PLX_CHECK_CUDA(cudaMemcpyAsync(d_fa.p, fa.data(), na * 4, cudaMemcpyHostToDevice, st));
-        gather_idx<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, d_idx.p, R.p, Ba.p);
-        ctx->launches++;
-        GmresResult ir;
-        gmres_batched(g, in, Ba.p, Da.p, ir);
-        for (int k = 0; k < na; ++k) {
-            res.inner_steps[act[k]] += ir.steps[k];
-            res.outer[act[k]] += 1;
-        }
-        if (max_cycles > 1) {
-            // restarts: columns whose cycle ended on the full basis continue from their
-            // inner residual; cur[] are positions in act of the columns of the last cycle
-            PLX_CHECK_CUDA(cudaMemcpyAsync(Dacc.p, Da.p, (size_t)na * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
-            std::vector<int32_t> cur(na);
-            for (int k = 0; k < na; ++k) cur[k] = k;
-            const double *bc = Ba.p;      // right-hand sides of the last cycle, compact over cur
-            for (int cyc = 1; cyc < max_cycles; ++cyc) {
-                std::vector<int32_t> sub, pos, fsub;
-                for (size_t t = 0; t < cur.size(); ++t)
-                    if (ir.status[t] == PLX_ERR_NOT_CONVERGED) {
-                        sub.push_back((int32_t)t);
-                        pos.push_back(cur[t]);
-                        fsub.push_back(fa[cur[t]]);
-                    }
-                if (sub.empty()) break;
-                const int ns = (int)sub.size();
-                PLX_CHECK_CUDA(cudaMemcpyAsync(d_sub.p, sub.data(), ns * 4, cudaMemcpyHostToDevice, st));
-                PLX_CHECK_CUDA(cudaMemcpyAsync(d_fsub.p, fsub.data(), ns * 4, cudaMemcpyHostToDevice, st));
-                // Bc = b_cycle[sub] - A d_cycle[sub]   (inner contraction)
-                gather_idx<<<dim3(grid_cols(n), ns), 256, 0, st>>>(n, d_sub.p, Da.p, AXa.p);
-                ctx->launches++;
-                apply_operator(g, OpBatch{ns, d_fsub.p}, AXa.p, Da.p, Wc.p, rq.inner_contraction);
-                compact_residual<<<dim3(grid_cols(n), ns), 256, 0, st>>>(n, d_sub.p, bc, Da.p, AXa.p);
-                ctx->launches++;
-                PLX_CHECK_CUDA(cudaMemcpyAsync(Bc.p, AXa.p, (size_t)ns * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
-                bc = Bc.p;
-                GmresRequest rin = in;
-                rin.freq.clear();
-                rin.pol.clear();
-                rin.tols.clear();
-                for (int t = 0; t < ns; ++t) {
-                    rin.freq.push_back(in.freq[pos[t]]);
-                    rin.pol.push_back(in.pol[pos[t]]);
-                    rin.tols.push_back(tol_k[pos[t]]);
-                }
-                ir = GmresResult();
-                gmres_batched(g, rin, Bc.p, Da.p, ir);
-                PLX_CHECK_CUDA(cudaMemcpyAsync(d_sub.p, pos.data(), ns * 4, cudaMemcpyHostToDevice, st));
-                scatter_add<<<dim3(grid_cols(n), ns), 256, 0, st>>>(n, d_sub.p, Da.p, Dacc.p);
-                ctx->launches++;
-                for (int t = 0; t < ns; ++t) res.inner_steps[act[pos[t]]] += ir.steps[t];
-                cur = pos;
-            }
-            PLX_CHECK_CUDA(cudaMemcpyAsync(Da.p, Dacc.p, (size_t)na * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
-        }
-        scatter_add<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, d_idx.p, Da.p, d_X);
-        gather_idx<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, d_idx.p, d_X, Ba.p);
-        ctx->launches += 2;
-        // FP64 residual of the active columns
-        apply_operator(g, OpBatch{na, d_fa.p}, Ba.p, AXa.p, Da.p, rq.outer_contraction);
-        scatter_residual<<<dim3(grid_cols(n), na), 256, 0, st>>>(n, d_idx.p, d_B, AXa.p, R.p);
-        ctx->launches++;
-        PLX_CHECK_CUDA(cudaGetLastError());
+    }
+    for (int c = 0; c < C; ++c) {
+        const RefineState::Slot &sl = S.slots[c];
+        res.status[c] = sl.state == RefineState::Slot::FINISHED ? sl.status : PLX_ERR_NOT_CONVERGED;
+        res.inner_steps[c] = sl.inner_steps;
+        res.outer[c] = sl.outer;
+        res.residual[c] = sl.residual;
     }
     if (g->d_tc_err.p && tc_error(g) != 0)
         throw Error(PLX_ERR_CUDA, "tensor-core contraction timed out waiting on its pipeline");

@@ -34,6 +34,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "pair_tiles.cuh"
 #include "plx_internal.h"
@@ -134,67 +135,75 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                  : "memory");
 }
 
-template <int BN, int STAGES>
-struct TcSmem {
-    static constexpr int kA = kBM * kBK * 2;      // bytes of one A operand tile
-    static constexpr int kB = BN * kBK * 2;       // bytes of one B operand tile
-    static constexpr int kStage = 2 * kA + 2 * kB;
-    static constexpr int kBytes = STAGES * kStage + 1024 /* align */ + 256 /* barriers */;
+// Work of one launch: the output tiles (256 rows x bn columns, column tile
+// fastest so that the tiles sharing one row block of an operand run side by
+// side and its second read comes from L2) of one or several groups -- a group
+// is one contraction S = A X of one geometry.  A group's first `full` tiles are
+// computed whole, one CTA each, and stored as FP64 into S; each of its
+// remaining tiles is split over k into q pieces of kper k-tiles, one CTA each,
+// which store FP32 partial sums into P (piece j at P + j * 256 * bn,
+// [column][row]); reduce_pieces adds a tile's pieces in order.  With the
+// pieces filling the last wave, every SM gets the same work (whole tiles plus
+// one piece) instead of a last wave that leaves SMs idle.  Several groups in one
+// launch run whole tiles only, the groups ordered by decreasing k length, so
+// that the hardware's in-order dispatch of CTAs to free SMs balances them.
+constexpr int kMaxGroups = 6;
+struct TcGroup {
+    int M, R, bn, ktiles;       // rows, real columns, column tile, k-tiles (32 deep)
+    int unit0;                  // first CTA of the group
+    int full, q, kper, ctiles;  // schedule (see above)
+    double *S;                  // [R][M] FP64
+    float *P;                   // pieces of the split tiles
+    int *err;                   // the geometry's error word (first bounded wait that ran out)
+};
+struct TcLaunch {
+    CUtensorMap map[kMaxGroups][4];   // A high, A low, X high, X low
+    TcGroup grp[kMaxGroups];
+    int ngroups;
+    int stages;                 // pipeline depth
+    int bn_max;                 // shared-memory / tensor-memory sizing
+    uint32_t wait_limit;
 };
 
-template <int BN>
-constexpr int tc_stages() {
-    return std::min(6, (200 * 1024) / TcSmem<BN, 1>::kStage);
-}
+__host__ __device__ constexpr int tc_stage_bytes(int bn) { return 2 * (kBM * kBK * 2) + 2 * (bn * kBK * 2); }
 
-// Work of one launch: T = mtiles x ctiles output tiles (256 rows x BN columns,
-// column tile fastest so that the tiles sharing one row block of the operand run
-// side by side and its second read comes from L2).  The first `full` tiles are
-// computed whole, one CTA each, in full waves over the SMs, and stored as FP64
-// into S; each of the remaining T - full tiles is split over k into q pieces of
-// kper k-tiles, one CTA each, which store FP32 partial sums into P (piece j at
-// P + j * 256 * BN, [column][row]); reduce_pieces adds a tile's pieces in
-// order.  With the pieces filling the last wave, every SM gets the same work
-// (whole tiles plus one piece) instead of a last wave that leaves SMs idle.
-struct TcSched {
-    int ctiles;     // column tiles
-    int full;       // tiles computed whole
-    int q;          // pieces per remaining tile
-    int kper;       // k-tiles per piece
-};
-
-template <int BN, int STAGES, int NPROD>
-__global__ void __launch_bounds__(128, 1)
-    tc_contract_kernel(const __grid_constant__ CUtensorMap mapTh, const __grid_constant__ CUtensorMap mapTl,
-                       const __grid_constant__ CUtensorMap mapXh, const __grid_constant__ CUtensorMap mapXl,
-                       int M, int R, int ktiles, TcSched sc, double *__restrict__ S, int ldS,
-                       float *__restrict__ P, int *__restrict__ err, uint32_t wait_limit) {
-    using L = TcSmem<BN, STAGES>;
-    // this CTA's unit: a whole tile, or one k-piece of a remaining tile
+template <int NPROD>
+__global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_constant__ TcLaunch p) {
+    // this CTA's group and unit: a whole tile, or one k-piece of a remaining tile
+    int gi = 0;
+    while (gi + 1 < p.ngroups && (int)blockIdx.x >= p.grp[gi + 1].unit0) ++gi;
+    const TcGroup &G = p.grp[gi];
+    const int u = (int)blockIdx.x - G.unit0;
     int tile, kt0, nk, piece = -1;
-    if ((int)blockIdx.x < sc.full) {
-        tile = blockIdx.x;
+    if (u < G.full) {
+        tile = u;
         kt0 = 0;
-        nk = ktiles;
+        nk = G.ktiles;
     } else {
-        piece = blockIdx.x - sc.full;
-        tile = sc.full + piece / sc.q;
-        kt0 = (piece % sc.q) * sc.kper;
-        nk = min(ktiles, kt0 + sc.kper) - kt0;
+        piece = u - G.full;
+        tile = G.full + piece / G.q;
+        kt0 = (piece % G.q) * G.kper;
+        nk = min(G.ktiles, kt0 + G.kper) - kt0;
     }
-    const int mtile = tile / sc.ctiles;
-    // two accumulators of BN columns each (rows m0.. and m0 + 128..)
-    constexpr uint32_t kTmemCols = 2 * BN <= 64 ? 64 : (2 * BN <= 128 ? 128 : (2 * BN <= 256 ? 256 : 512));
+    const int bn = G.bn, M = G.M, R = G.R, ktiles = G.ktiles;
+    const int STAGES = p.stages;
+    const int kStage = tc_stage_bytes(p.bn_max);
+    const int kA = kBM * kBK * 2;
+    const int mtile = tile / G.ctiles;
+    int *err = G.err;
+    const uint32_t wait_limit = p.wait_limit;
+    // two accumulators of bn columns each (rows m0.. and m0 + 128..)
+    const uint32_t tmem_cols = 2 * p.bn_max <= 64 ? 64 : (2 * p.bn_max <= 128 ? 128 : (2 * p.bn_max <= 256 ? 256 : 512));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * L::kStage);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * kStage);
     uint64_t *empty = full + STAGES;
     uint64_t *done = empty + STAGES;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = (tile % sc.ctiles) * BN;
+    const int n0 = (tile % G.ctiles) * bn;
     const int m0 = mtile * kBM;
 
     if (threadIdx.x == 0) {
@@ -208,7 +217,7 @@ __global__ void __launch_bounds__(128, 1)
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kTmemCols)
+                     "r"(tmem_cols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -218,14 +227,16 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t tmem = *tmem_slot;
 
     auto stage_ptr = [&](int s, int which) -> uint8_t * {
-        // which: 0 Th, 1 Tl, 2 Xh, 3 Xl
-        uint8_t *st = base + s * L::kStage;
-        return which < 2 ? st + which * L::kA : st + 2 * L::kA + (which - 2) * L::kB;
+        // which: 0 A high, 1 A low, 2 X high, 3 X low
+        uint8_t *st = base + s * kStage;
+        return which < 2 ? st + which * kA : st + 2 * kA + (which - 2) * (p.bn_max * kBK * 2);
     };
 
     int issued = 0;     // loads issued by the producer (thread 0)
     if (threadIdx.x == 0) {
         // ---------------- TMA producer ----------------
+        const CUtensorMap *mp = p.map[gi];
+        const uint32_t tx = (uint32_t)(2 * kA + 2 * bn * kBK * 2);
         for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
             if (kt >= STAGES) {
@@ -234,18 +245,18 @@ __global__ void __launch_bounds__(128, 1)
                     break;
                 }
             }
-            mbar_expect_tx(&full[s], (uint32_t)L::kStage);
+            mbar_expect_tx(&full[s], tx);
             const int kx = (kt0 + kt) * kBK;
             const int ay = (mtile * ktiles + kt0 + kt) * kBM;          // tile-ordered A
-            tma_load_2d(&mapTh, &full[s], stage_ptr(s, 0), 0, ay);
-            tma_load_2d(&mapTl, &full[s], stage_ptr(s, 1), 0, ay);
-            tma_load_2d(&mapXh, &full[s], stage_ptr(s, 2), kx, n0);
-            tma_load_2d(&mapXl, &full[s], stage_ptr(s, 3), kx, n0);
+            tma_load_2d(&mp[0], &full[s], stage_ptr(s, 0), 0, ay);
+            tma_load_2d(&mp[1], &full[s], stage_ptr(s, 1), 0, ay);
+            tma_load_2d(&mp[2], &full[s], stage_ptr(s, 2), kx, n0);
+            tma_load_2d(&mp[3], &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
         }
     } else if (threadIdx.x == 32) {
         // ---------------- MMA issuer ----------------
-        constexpr uint32_t idesc = umma_idesc_bf16(kUM, BN);
+        const uint32_t idesc = umma_idesc_bf16(kUM, bn);
         constexpr uint64_t kHalf = (uint64_t)(kUM * kBK * 2) >> 4;   // second 128 rows of an A tile
         for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
@@ -265,7 +276,7 @@ __global__ void __launch_bounds__(128, 1)
                 const uint32_t acc0 = (kt > 0 || kk > 0) ? 1u : 0u;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const uint32_t td = tmem + (uint32_t)(h * BN);
+                    const uint32_t td = tmem + (uint32_t)(h * bn);
                     const uint64_t ho = h * kHalf;
                     umma_bf16(td, dTh + ho + off, dXh + off, idesc, acc0);
                     if (NPROD > 1) {
@@ -282,7 +293,7 @@ __global__ void __launch_bounds__(128, 1)
     }
     __syncwarp();
 
-    // ---------------- epilogue: TMEM -> S (FP64) ----------------
+    // ---------------- epilogue: TMEM -> S (FP64) or the piece's partial (FP32) ----------------
     bool fin = mbar_wait(done, 0, wait_limit, nullptr, err, 3);
     if (!fin) {
         *abort_flag = 1;
@@ -301,10 +312,10 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {
         const int row = m0 + h * kUM + warp * 32 + lane;
-#pragma unroll
-        for (int c0 = 0; c0 < BN; c0 += 32) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < bn; c0 += 32) {
             uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * BN + c0);
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * bn + c0);
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -318,14 +329,14 @@ __global__ void __launch_bounds__(128, 1)
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (piece >= 0) {
                 // partial of a split tile: [column][256 rows] FP32, every element written
-                float *pp = P + (int64_t)piece * kBM * BN + (h * kUM + warp * 32 + lane);
+                float *pp = G.P + (int64_t)piece * kBM * bn + (h * kUM + warp * 32 + lane);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) pp[(int64_t)(c0 + j) * kBM] = __uint_as_float(v[j]);
             } else if (row < M) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int c = n0 + c0 + j;
-                    if (c < R) S[(int64_t)c * ldS + row] = (double)__uint_as_float(v[j]);
+                    if (c < R) G.S[(int64_t)c * M + row] = (double)__uint_as_float(v[j]);
                 }
             }
         }
@@ -334,7 +345,7 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
     }
 }
 
@@ -500,37 +511,21 @@ CUtensorMap make_map(const void *ptr, uint64_t inner, uint64_t outer, uint64_t l
     return m;
 }
 
-template <int BN, int NPROD>
-void launch_bn(plx_geom *g, int M, int R, const CUtensorMap &th, const CUtensorMap &tl, const CUtensorMap &xh,
-               const CUtensorMap &xl, int ktiles, const TcSched &sc, int units, double *S, float *P, int *err) {
-    constexpr int ST = tc_stages<BN>();
-    using L = TcSmem<BN, ST>;
-    auto kern = tc_contract_kernel<BN, ST, NPROD>;
-    once_per_device(reinterpret_cast<const void *>(kern), g->ctx->device, [&] {
-        PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes));
-    });
-    kern<<<units, 128, L::kBytes, g->ctx->stream>>>(th, tl, xh, xl, M, R, ktiles, sc, S, M, P, err,
-                                                    g->ctx->wait_limit);
-    g->ctx->launches++;
-    PLX_CHECK_CUDA(cudaGetLastError());
-}
-
-// Remaining tiles: S = the sum of a tile's q FP32 pieces in piece order (FP64
-// sums), for the rows and columns inside the matrix.  One block per (tile,
-// 32-column group); threads over the tile's 256 rows.
-template <int BN>
-__global__ void reduce_pieces(int M, int R, int full, int ctiles, int q, const float *__restrict__ P,
-                              double *__restrict__ S, int ldS) {
+// Remaining tiles of a group: S = the sum of a tile's q FP32 pieces in piece
+// order (FP64 sums), for the rows and columns inside the matrix.  One block per
+// (tile, 32-column group); threads over the tile's 256 rows.
+__global__ void reduce_pieces(int M, int R, int bn, int full, int ctiles, int q, const float *__restrict__ P,
+                              double *__restrict__ S) {
     const int t = blockIdx.x;                       // remaining tile index
     const int tile = full + t;
-    const int m0 = (tile / ctiles) * kBM, n0 = (tile % ctiles) * BN;
+    const int m0 = (tile / ctiles) * kBM, n0 = (tile % ctiles) * bn;
     const int r = threadIdx.x;                      // 0..255
     if (m0 + r >= M) return;
-    for (int c = blockIdx.y * 32; c < min(BN, blockIdx.y * 32 + 32); ++c) {
+    for (int c = blockIdx.y * 32; c < min(bn, blockIdx.y * 32 + 32); ++c) {
         if (n0 + c >= R) break;
         double a = 0.0;
-        for (int p = 0; p < q; ++p) a += (double)P[((int64_t)(t * q + p) * BN + c) * kBM + r];
-        S[(int64_t)(n0 + c) * ldS + m0 + r] = a;
+        for (int p = 0; p < q; ++p) a += (double)P[((int64_t)(t * q + p) * bn + c) * kBM + r];
+        S[(int64_t)(n0 + c) * M + m0 + r] = a;
     }
 }
 
@@ -540,28 +535,29 @@ int sm_count(int device) {
     return v > 0 ? v : 1;
 }
 
-// Schedule of `tiles` output tiles of `ktiles` k-tiles on `sms` SMs (one CTA per
-// SM): whole tiles in full waves; the r = tiles mod sms tiles of the last wave
-// are split into q = sms / r pieces (at least 8 k-tiles each) when that lets the
-// pieces fill the wave -- otherwise (r close to sms, or no split possible) they
-// run whole too.
-TcSched make_schedule(int tiles, int ctiles, int ktiles, int sms, int &units) {
-    TcSched sc{ctiles, tiles, 1, ktiles};
+// Schedule of one group's `tiles` output tiles of `ktiles` k-tiles on `sms` SMs
+// (one CTA per SM): whole tiles in full waves; the r = tiles mod sms tiles of
+// the last wave are split into q = sms / r pieces (at least 8 k-tiles each)
+// when that lets the pieces fill the wave -- otherwise (r close to sms, or no
+// split possible) they run whole too.  Returns the group's number of CTAs.
+int make_schedule(TcGroup &gp, int tiles, int sms, bool split) {
+    gp.full = tiles;
+    gp.q = 1;
+    gp.kper = gp.ktiles;
     const int r = tiles % sms;
-    units = tiles;
-    if (r == 0 || (double)r / sms >= 0.9) return sc;
-    int q = std::min(sms / r, ktiles / 8);
-    if (q < 2) return sc;
-    const int kper = (ktiles + q - 1) / q;
-    q = (ktiles + kper - 1) / kper;                 // no empty piece
-    sc.full = tiles - r;
-    sc.q = q;
-    sc.kper = kper;
-    units = sc.full + r * q;
-    return sc;
+    if (!split || r == 0 || (double)r / sms >= 0.9) return tiles;
+    int q = std::min(sms / r, gp.ktiles / 8);
+    if (q < 2) return tiles;
+    const int kper = (gp.ktiles + q - 1) / q;
+    q = (gp.ktiles + kper - 1) / kper;              // no empty piece
+    gp.full = tiles - r;
+    gp.q = q;
+    gp.kper = kper;
+    return gp.full + r * q;
 }
 
 }  // namespace
+
 
 void build_t_split(plx_geom *g) {
     if (g->d_Th.p) return;
@@ -746,63 +742,116 @@ int64_t tc_fold_rows(plx_geom *g) {
     return g->fold_rows;
 }
 
-void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded) {
-    if (folded)
-        build_a_split(g);
-    else
-        build_t_split(g);
-    plx_ctx *ctx = g->ctx;
-    const int n = g->n_var;
-    // output rows: n, or the folded operand's rows (n plus interface rows); S is [R][M]
-    const int M = folded ? (int)g->fold_rows : n;
-    const int R = 2 * count;
-    const int64_t ld = g->ldk;
-    // column tiles: as few as possible, each a multiple of 32 columns (<= 256)
-    const int ntile = (R + 255) / 256;
-    int bn = ((R + ntile - 1) / ntile + 31) / 32 * 32;
-    const int Rpad = ntile * bn;
-    size_t need = (size_t)Rpad * ld;
-    if (g->d_Xh.n < need) {
-        g->d_Xh.alloc(ctx, need);
-        g->d_Xl.alloc(ctx, need);
+void tc_contract_group(const std::vector<TcItem> &items) {
+    if (items.empty()) return;
+    if ((int)items.size() > kMaxGroups) {
+        // more contractions than one launch describes: in launches of kMaxGroups
+        for (size_t i0 = 0; i0 < items.size(); i0 += kMaxGroups)
+            tc_contract_group(std::vector<TcItem>(items.begin() + i0,
+                                                  items.begin() + std::min(items.size(), i0 + kMaxGroups)));
+        return;
     }
-    split_bf16<<<std::min<int64_t>(4096, n_blocks((int64_t)Rpad * ld, 256)), 256, 0, ctx->stream>>>(
-        R, n, n, X, Rpad, ld, reinterpret_cast<__nv_bfloat16 *>(g->d_Xh.p),
-        reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
+    plx_ctx *ctx = items[0].g->ctx;
+    const int nprod = items[0].nprod;
+    for (const TcItem &it : items)
+        if (it.g->ctx != ctx || it.nprod != nprod)
+            throw Error(PLX_ERR_ARG, "a grouped contraction needs one context and one product count");
+    for (size_t i = 0; i < items.size(); ++i)
+        for (size_t j = 0; j < i; ++j)
+            if (items[i].g == items[j].g) {
+                // one geometry twice: its column split buffers hold one operand at a time
+                for (const TcItem &it : items) tc_contract_group({it});
+                return;
+            }
+    const bool single = items.size() == 1;
+    // longest k first: the hardware hands CTAs to free SMs in launch order
+    std::vector<int> order(items.size());
+    for (size_t i = 0; i < items.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return items[a].g->n_var > items[b].g->n_var; });
+    TcLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.ngroups = (int)items.size();
+    L.wait_limit = ctx->wait_limit;
+    int units = 0, bn_max = 32;
+    const int sms = sm_count(ctx->device);
+    struct Post {
+        int gi, rem;
+    };
+    std::vector<Post> post;
+    for (int k = 0; k < L.ngroups; ++k) {
+        const TcItem &it = items[order[k]];
+        plx_geom *g = it.g;
+        if (it.folded)
+            build_a_split(g);
+        else
+            build_t_split(g);
+        const int n = g->n_var;
+        // output rows: n, or the folded operand's rows (n plus interface rows); S is [R][M]
+        const int M = it.folded ? (int)g->fold_rows : n;
+        const int R = 2 * it.count;
+        const int64_t ld = g->ldk;
+        // column tiles: as few as possible, each a multiple of 32 columns (<= 256)
+        const int ntile = (R + 255) / 256;
+        const int bn = ((R + ntile - 1) / ntile + 31) / 32 * 32;
+        const int Rpad = ntile * bn;
+        const size_t need = (size_t)Rpad * ld;
+        if (g->d_Xh.n < need) {
+            g->d_Xh.alloc(ctx, need);
+            g->d_Xl.alloc(ctx, need);
+        }
+        split_bf16<<<std::min<int64_t>(4096, n_blocks((int64_t)Rpad * ld, 256)), 256, 0, ctx->stream>>>(
+            R, n, n, it.X, Rpad, ld, reinterpret_cast<__nv_bfloat16 *>(g->d_Xh.p),
+            reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
+        ctx->launches++;
+        // A in tile order: rows of kBK elements, kBM rows per box
+        const uint64_t arows = (uint64_t)((M + kBM - 1) / kBM) * kBM * (uint64_t)(ld / kBK);
+        L.map[k][0] = make_map(it.folded ? g->d_Ah.p : g->d_Th.p, kBK, arows, kBK, kBM);
+        L.map[k][1] = make_map(it.folded ? g->d_Al.p : g->d_Tl.p, kBK, arows, kBK, kBM);
+        L.map[k][2] = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
+        L.map[k][3] = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
+        TcGroup &gp = L.grp[k];
+        gp.M = M;
+        gp.R = R;
+        gp.bn = bn;
+        gp.ktiles = (int)(ld / kBK);
+        gp.ctiles = ntile;
+        gp.unit0 = units;
+        gp.S = it.S;
+        const int mtiles = (M + kBM - 1) / kBM;
+        units += make_schedule(gp, mtiles * ntile, sms, single);
+        const int rem = mtiles * ntile - gp.full;
+        if (rem > 0) {
+            const size_t pn = (size_t)rem * gp.q * kBM * bn;
+            if (g->d_tcpart.n < pn) g->d_tcpart.alloc(ctx, pn);
+            gp.P = g->d_tcpart.p;
+            post.push_back({k, rem});
+        }
+        bn_max = std::max(bn_max, bn);
+        if (!g->d_tc_err.p) throw Error(PLX_ERR_CUDA, "tensor-core error word missing");
+        gp.err = g->d_tc_err.p;
+    }
+    L.bn_max = bn_max;
+    L.stages = std::min(6, (200 * 1024) / tc_stage_bytes(bn_max));
+    const int smem = L.stages * tc_stage_bytes(bn_max) + 1024 /* align */ + 256 /* barriers */;
+    auto kern = nprod == 1 ? tc_contract_kernel<1> : tc_contract_kernel<3>;
+    once_per_device(reinterpret_cast<const void *>(kern), ctx->device, [&] {
+        PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    });
+    kern<<<units, 128, smem, ctx->stream>>>(L);
     ctx->launches++;
-    // A in tile order: rows of kBK elements, kBM rows per box
-    const uint64_t arows = (uint64_t)((M + kBM - 1) / kBM) * kBM * (uint64_t)(ld / kBK);
-    CUtensorMap th = make_map(folded ? g->d_Ah.p : g->d_Th.p, kBK, arows, kBK, kBM);
-    CUtensorMap tl = make_map(folded ? g->d_Al.p : g->d_Tl.p, kBK, arows, kBK, kBM);
-    CUtensorMap xh = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
-    CUtensorMap xl = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
-    const int ktiles = (int)(ld / kBK);
-    int *err = g->d_tc_err.p;
-    const int mtiles = (M + kBM - 1) / kBM;
-    int units = 0;
-    const TcSched sc = make_schedule(mtiles * ntile, ntile, ktiles, sm_count(ctx->device), units);
-    const int rem = mtiles * ntile - sc.full;
-    float *P = nullptr;
-    if (rem > 0) {
-        const size_t pn = (size_t)rem * sc.q * kBM * bn;
-        if (g->d_tcpart.n < pn) g->d_tcpart.alloc(ctx, pn);
-        P = g->d_tcpart.p;
-    }
-#define PLX_TC(BNV)                                                                              \
-    case BNV:                                                                                    \
-        if (nprod == 1) launch_bn<BNV, 1>(g, M, R, th, tl, xh, xl, ktiles, sc, units, S, P, err); \
-        else launch_bn<BNV, 3>(g, M, R, th, tl, xh, xl, ktiles, sc, units, S, P, err);            \
-        if (rem > 0) {                                                                           \
-            reduce_pieces<BNV><<<dim3(rem, BNV / 32), kBM, 0, ctx->stream>>>(M, R, sc.full, ntile, sc.q, P, S, M); \
-            ctx->launches++;                                                                     \
-        }                                                                                        \
-        break;
-    switch (bn) {
-        PLX_TC(32) PLX_TC(64) PLX_TC(96) PLX_TC(128) PLX_TC(160) PLX_TC(192) PLX_TC(224) PLX_TC(256)
-        default: throw Error(PLX_ERR_ARG, "bad column tile");
-    }
-#undef PLX_TC
     PLX_CHECK_CUDA(cudaGetLastError());
+    for (const Post &q : post) {
+        const TcGroup &gp = L.grp[q.gi];
+        reduce_pieces<<<dim3(q.rem, gp.bn / 32), kBM, 0, ctx->stream>>>(gp.M, gp.R, gp.bn, gp.full, gp.ctiles, gp.q,
+                                                                      gp.P, gp.S);
+        ctx->launches++;
+    }
+    PLX_CHECK_CUDA(cudaGetLastError());
+}
+
+void tc_contract(plx_geom *g, int count, const double *X, double *S, int nprod, bool folded) {
+    tc_contract_group({TcItem{g, count, X, S, nprod, folded}});
 }
 
 int tc_error(plx_geom *g) {
