@@ -14,11 +14,15 @@ frequency grid and the solve settings.  The server keeps
   plus the Krylov state of the batch are reserved against the HBM budget;
   idle resident geometries are evicted (least recently used) to make room,
   and a request that does not fit waits until running batches release memory;
-* **continuous batching** — whenever a worker becomes free it takes every
-  queued request for its next geometry that shares the solve settings and
-  solves their frequencies as ONE batch (every Arnoldi step of every
-  frequency of every merged request is one contraction launch), then returns
-  each request its own slice of the results.
+* **continuous batching** -- a refinement request (mixed or FP64-refined) joins
+  its geometry's open batch (``plx_batch_*``) as soon as its worker is between
+  two outer steps, even while earlier requests are in flight; every step is
+  one outer refinement step of all in-flight columns of all the worker's open
+  batches together (``plx_batch_step_group``: every inner Arnoldi step is ONE
+  grouped tensor-core launch over the geometries' operands), and a request
+  leaves with its results as soon as its own columns have converged.  Plain
+  FP64 requests (the reference's unrestarted GMRES) are solved as one batch
+  of the queued requests of a geometry.
 
 Latency is measured per request from its arrival to its results on the host;
 ``run_mix`` replays a seeded Poisson arrival stream and reports p50/p99
@@ -31,7 +35,7 @@ import time
 
 import numpy as np
 
-from .solver import Context, Solver
+from .solver import Batch, Context, Solver
 
 KRYLOV_INNER = 64
 
@@ -124,11 +128,15 @@ class Server:
     while it runs.  Device memory belongs to the worker's context, so evicted
     geometries are freed by their own worker thread."""
 
-    def __init__(self, device=0, hbm_budget=None, workers=2, solver_factory=None, context_factory=None):
+    def __init__(self, device=0, hbm_budget=None, workers=2, solver_factory=None, context_factory=None,
+                 batch_factory=None):
         self.device = device
         self.n_workers = int(workers)
         self.solver_factory = solver_factory or (lambda p, ctx, store_t: Solver(p, ctx=ctx, store_t=store_t))
         self.context_factory = context_factory or (lambda dev: Context(dev))
+        self.batch_factory = batch_factory or (lambda solver, mode, precision: Batch(solver, mode=mode,
+                                                                                   precision=precision))
+        self.steps = []              # (worker, geometries, requests, seconds) per batch step
         if hbm_budget is None:
             hbm_budget = self._free_bytes()
         self.budget = int(hbm_budget)
@@ -255,16 +263,6 @@ class Server:
         return req.n_freq * bin(req.pol_mask).count('1')
 
     # ---- workers --------------------------------------------------------------
-    def _take_batch(self, w):
-        """Next batch of worker w (lock held): the first queued request and every
-        queued request of the same geometry and settings."""
-        q = self.queues[w]
-        head = q[0]
-        batch = [r for r in q if r.key == head.key and r.settings == head.settings]
-        for r in batch:
-            q.remove(r)
-        return batch
-
     def _free_evicted(self, w):
         with self.lock:
             gone, self.evicted[w] = self.evicted[w], []
@@ -284,46 +282,191 @@ class Server:
         except Exception as e:          # device failure: report through the requests
             self.errors.append(e)
             return
+        # continuous batching state of this worker: geometry key -> open batch
+        self._open = getattr(self, '_open', {})
+        self._open[w] = {}
         try:
             while True:
                 self._free_evicted(w)
                 with self.lock:
-                    while not self.queues[w] and not self.evicted[w] and not self.stopping:
+                    while (not self.queues[w] and not self.evicted[w] and not self._in_flight(w)
+                           and not self.stopping):
                         self.lock.wait()
                     if self.evicted[w]:
                         continue
-                    if not self.queues[w]:
-                        break        # stopping, nothing queued
-                    batch = self._take_batch(w)
-                    self.busy[w] = True
-                    res = self.resident[w].get(batch[0].key)
-                    mode = res.mode if res is not None else (batch[0].mode or 'iterative')
-                    _, batch_bytes = footprint(batch[0].problem, mode, batch[0].precision,
-                                               sum(self._cols(r) for r in batch))
-                    self.committed += batch_bytes
-                    if res is not None:
-                        res.busy = True
-                self._run_batch(w, batch, res, mode, ctx)
-                with self.lock:
-                    self.committed -= batch_bytes
-                    self.busy[w] = False
-                    r = self.resident[w].get(batch[0].key)
-                    if r is not None:
-                        r.busy = False
-                        r.last_used = time.perf_counter()
-                    self._dispatch()
-                    self.lock.notify_all()
+                    if not self.queues[w] and not self._in_flight(w):
+                        break        # stopping, nothing queued or in flight
+                    joining = self._take_joining(w)
+                    plain = [] if joining or self._in_flight(w) else self._take_plain(w)
+                if plain:
+                    self._plain_batch(w, plain, ctx)
+                    continue
+                for r in joining:
+                    self._join(w, r, ctx)
+                if self._in_flight(w):
+                    self._step(w)
         finally:
             with self.lock:
                 left = list(self.resident[w].values()) + self.evicted[w]
                 self.resident[w].clear()
                 self.evicted[w] = []
+                opened = list(self._open.get(w, {}).values())
+                self._open[w] = {}
+            for ob in opened:
+                try:
+                    ob['batch'].close()
+                except Exception:
+                    pass
             for r in left:
                 try:
                     r.solver.close()
                 except Exception:
                     pass
             ctx.close()
+
+    # ---- continuous batching (refinement forms) ---------------------------------
+    def _in_flight(self, w):
+        return any(ob['reqs'] for ob in self._open.get(w, {}).values())
+
+    def _take_joining(self, w):
+        """Queued refinement requests that can join this worker's batches now (lock
+        held): every one whose geometry has no open batch or an open batch with its
+        settings; their batch bytes are reserved."""
+        q = self.queues[w]
+        out = []
+        for r in list(q):
+            if r.precision == 'fp64':
+                continue
+            ob = self._open[w].get(r.key)
+            if ob is not None and ob['precision'] != r.precision:
+                continue                  # waits until that batch drains
+            res = self.resident[w].get(r.key)
+            mode = res.mode if res is not None else (r.mode or 'iterative')
+            _, r.batch_bytes = footprint(r.problem, mode, r.precision, self._cols(r))
+            self.committed += r.batch_bytes
+            q.remove(r)
+            out.append(r)
+        return out
+
+    def _join(self, w, r, ctx):
+        """Adds a request to its geometry's batch (building the geometry and
+        opening the batch on first use)."""
+        try:
+            ob = self._open[w].get(r.key)
+            if ob is None:
+                with self.lock:
+                    res = self.resident[w].get(r.key)
+                if res is None:
+                    mode = r.mode or 'iterative'
+                    solver = self.solver_factory(r.problem, ctx, mode != 'iterative on the fly')
+                    res = _Resident(solver, mode, getattr(r, 'geo_bytes', 0))
+                    with self.lock:
+                        self.resident[w][r.key] = res
+                batch = self.batch_factory(res.solver, res.mode, r.precision)
+                ob = {'batch': batch, 'res': res, 'precision': r.precision, 'reqs': {}}
+                with self.lock:
+                    res.busy = True
+                    self._open[w][r.key] = ob
+            res = ob['res']
+            p = r.problem
+            ob['batch'].add(r.id, p.freqs, getattr(p, 'alpha_w', None), r.pol_mask, r.tol)
+            r.mode = res.mode
+            r.t_start = time.perf_counter()
+            r.worker = w
+            ob['reqs'][r.id] = r
+        except Exception as e:
+            self._finish(r, error=e)
+
+    def _step(self, w):
+        """One outer step of every open batch of this worker with columns in flight:
+        a grouped step (one tensor-core launch per inner Arnoldi step over all their
+        geometries), then the finished requests are taken out."""
+        live = [ob for ob in self._open[w].values() if ob['reqs']]
+        batches = [ob['batch'] for ob in live]
+        n_req = sum(len(ob['reqs']) for ob in live)
+        t0 = time.perf_counter()
+        try:
+            if len(batches) == 1:
+                batches[0].step()
+            else:
+                type(batches[0]).step_group(batches)
+        except Exception as e:
+            for ob in live:
+                for r in list(ob['reqs'].values()):
+                    self._finish(r, error=e)
+                ob['reqs'].clear()
+            return
+        with self.lock:
+            self.steps.append((w, len(live), n_req, time.perf_counter() - t0))
+        for ob in live:
+            for r in ob['reqs'].values():
+                r.batch_size = max(r.batch_size, n_req)
+                r.geometries_shared = max(getattr(r, 'geometries_shared', 1), len(live))
+            while True:
+                tag = ob['batch'].poll()
+                if tag is None:
+                    break
+                r = ob['reqs'].pop(tag)
+                try:
+                    r.result = ob['batch'].take(tag)
+                    self._finish(r)
+                except Exception as e:
+                    self._finish(r, error=e)
+        # drained batches close (a request with other settings may be waiting);
+        # their geometries stay resident
+        for key, ob in list(self._open[w].items()):
+            if not ob['reqs']:
+                ob['batch'].close()
+                with self.lock:
+                    del self._open[w][key]
+                    ob['res'].busy = False
+                    ob['res'].last_used = time.perf_counter()
+                    self._dispatch()
+                    self.lock.notify_all()
+
+    def _finish(self, r, error=None):
+        r.error = error if error is not None else r.error
+        r.t_done = time.perf_counter()
+        with self.lock:
+            self.committed -= getattr(r, 'batch_bytes', 0)
+            r.batch_bytes = 0
+            self.batches.append((r.worker, [r.id], r.mode, r.t_done - (r.t_start or r.t_done)))
+            self._dispatch()
+            self.lock.notify_all()
+        r.done.set()
+
+    # ---- plain FP64 requests: one solve per batch of queued requests -------------
+    def _take_plain(self, w):
+        q = self.queues[w]
+        heads = [r for r in q if r.precision == 'fp64']
+        if not heads:
+            return []
+        head = heads[0]
+        batch = [r for r in q if r.key == head.key and r.settings == head.settings]
+        for r in batch:
+            q.remove(r)
+        return batch
+
+    def _plain_batch(self, w, batch, ctx):
+        with self.lock:
+            self.busy[w] = True
+            res = self.resident[w].get(batch[0].key)
+            mode = res.mode if res is not None else (batch[0].mode or 'iterative')
+            _, batch_bytes = footprint(batch[0].problem, mode, batch[0].precision,
+                                       sum(self._cols(r) for r in batch))
+            self.committed += batch_bytes
+            if res is not None:
+                res.busy = True
+        self._run_batch(w, batch, res, mode, ctx)
+        with self.lock:
+            self.committed -= batch_bytes
+            self.busy[w] = False
+            r = self.resident[w].get(batch[0].key)
+            if r is not None:
+                r.busy = False
+                r.last_used = time.perf_counter()
+            self._dispatch()
+            self.lock.notify_all()
 
     def _run_batch(self, w, batch, res, mode, ctx):
         t0 = time.perf_counter()

@@ -236,3 +236,99 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """Continuous batching on one resident geometry (plx_batch): requests --
+    frequency grids with their own tolerance -- join while others are being
+    solved, each step() is one outer refinement step of every active column,
+    and finished requests are taken out with their results.
+
+        b = Batch(solver, precision='mixed_bf16x3')
+        b.add(7, freqs, alpha_w, pol_mask=1, tol=1e-9)
+        while b.active:
+            b.step()                      # or Batch.step_group([b, b2, ...])
+            while (tag := b.poll()) is not None:
+                out = b.take(tag)         # 'results' (F, 20), 'polar', 'status', 'steps'
+
+    While a batch is open it owns the solver's frequency table."""
+
+    def __init__(self, solver, mode=None, precision='mixed_bf16x3', inner_krylov=0, inner_tol=0.0, max_outer=0):
+        self.solver = solver
+        self.ctx = solver.ctx
+        self.lib = solver.lib
+        mode = mode or solver.prob.method
+        if mode == 'inversion':
+            mode = 'iterative'
+        desc = _lib.SolveDesc(_lib.MODE[mode], _lib.PRECISION[precision], 1, 1, 0.0, 0, 0, int(inner_krylov),
+                              float(inner_tol), int(max_outer))
+        h = C.c_void_p()
+        self.ctx.check(self.lib.plx_batch_open(solver.g, C.byref(desc), C.byref(h)))
+        self.h = h
+        self.mode, self.precision = mode, precision
+        self.n_freq = {}
+        self.last_step_ms = 0.0
+
+    def add(self, tag, freqs, alpha_w=None, pol_mask=1, tol=1e-9):
+        freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+        aw = None
+        if alpha_w is not None:
+            aw = np.ascontiguousarray(np.asarray(alpha_w, dtype=np.complex128).T).view(np.float64)
+        self.ctx.check(self.lib.plx_batch_add(self.h, int(tag), len(freqs), ptr(freqs), ptr(aw), int(pol_mask),
+                                              float(tol)))
+        self.n_freq[int(tag)] = len(freqs)
+
+    @property
+    def active(self):
+        return int(self.lib.plx_batch_active(self.h)) if self.h else 0
+
+    def step(self):
+        n = C.c_int32(0)
+        self.ctx.check(self.lib.plx_batch_step(self.h, C.byref(n)))
+        self.last_step_ms = float(self.lib.plx_last_solve_ms(self.solver.g))
+        return n.value
+
+    @staticmethod
+    def step_group(batches):
+        """One outer step of several batches (one per geometry, one context) whose
+        inner Arnoldi steps share one grouped tensor-core launch each."""
+        arr = (C.c_void_p * len(batches))(*[b.h for b in batches])
+        n = C.c_int32(0)
+        b0 = batches[0]
+        b0.ctx.check(b0.lib.plx_batch_step_group(arr, len(batches), C.byref(n)))
+        ms = float(b0.lib.plx_last_solve_ms(b0.solver.g))
+        for b in batches:
+            b.last_step_ms = ms
+        return n.value
+
+    def poll(self):
+        """The tag of the earliest request whose columns have all finished, or None."""
+        t = C.c_int64(-1)
+        self.ctx.check(self.lib.plx_batch_poll(self.h, C.byref(t)))
+        return None if t.value < 0 else int(t.value)
+
+    def take(self, tag):
+        F = self.n_freq[int(tag)]
+        polar = np.zeros((F, 3, 3), dtype=np.complex128)
+        res = np.zeros((F, 20))
+        status = np.zeros(F, dtype=np.int32)
+        steps = np.zeros((F, 3), dtype=np.int32)
+        st = self.lib.plx_batch_take(self.h, int(tag), ptr(polar.view(np.float64)), ptr(res), ptr(status, _lib._ip),
+                                     ptr(steps, _lib._ip))
+        out = {'polar': polar.transpose(0, 2, 1).copy(), 'results': res, 'status': status, 'steps': steps}
+        if st not in (_lib.PLX_OK, 5, 6):      # not converged / non-finite: reported per frequency
+            self.ctx.check(st)
+        del self.n_freq[int(tag)]
+        return out
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.plx_batch_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+

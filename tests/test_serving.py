@@ -1,6 +1,8 @@
 """Scheduling of the serving loop (admission by footprint, resident geometries,
-batching of requests that share a geometry, concurrent workers), exercised with
-a stand-in solver on the CPU; the GPU test of the same loop is test_gpu_serving.py."""
+continuous batching -- requests joining a batch while others are in flight,
+grouped steps over several geometries -- and concurrent workers), exercised with
+a stand-in solver and batch on the CPU; the GPU test of the same loop is
+test_gpu_serving.py."""
 import threading
 import time
 
@@ -47,9 +49,61 @@ class FakeSolver:
         self.closed = True
 
 
+class FakeBatch:
+    """Continuous batch stand-in: a request needs 1 + (its frequency count mod 3)
+    outer steps; a step sleeps `delay`; results[:, 0] = the request's frequencies."""
+
+    def __init__(self, solver, mode, precision, delay=0.02):
+        self.solver, self.mode, self.precision, self.delay = solver, mode, precision, delay
+        self.left, self.freqs, self.done = {}, {}, []
+        self.closed = False
+
+    def add(self, tag, freqs, alpha_w, pol_mask, tol):
+        self.freqs[tag] = np.asarray(freqs)
+        self.left[tag] = 1 + len(freqs) % 3
+
+    @property
+    def active(self):
+        return len(self.left)
+
+    def _advance(self):
+        for t in list(self.left):
+            self.left[t] -= 1
+            if self.left[t] == 0:
+                del self.left[t]
+                self.done.append(t)
+
+    def step(self):
+        FakeBatch.step_group([self])
+
+    @staticmethod
+    def step_group(batches):
+        t0 = time.perf_counter()
+        time.sleep(batches[0].delay)
+        for b in batches:
+            b._advance()
+        with FakeSolver.lock:
+            FakeSolver.log.append(('step', tuple(id(b.solver.problem) for b in batches), t0, time.perf_counter()))
+
+    def poll(self):
+        return self.done[0] if self.done else None
+
+    def take(self, tag):
+        self.done.remove(tag)
+        f = self.freqs.pop(tag)
+        res = np.zeros((len(f), 20))
+        res[:, 0] = f
+        return {'results': res, 'polar': np.zeros((len(f), 3, 3), complex), 'status': np.zeros(len(f), np.int32),
+                'steps': np.zeros((len(f), 3), np.int32)}
+
+    def close(self):
+        self.closed = True
+
+
 def _server(budget, workers=2):
     FakeSolver.log = []
-    return Server(hbm_budget=budget, workers=workers, solver_factory=FakeSolver, context_factory=FakeContext)
+    return Server(hbm_budget=budget, workers=workers, solver_factory=FakeSolver, context_factory=FakeContext,
+                  batch_factory=FakeBatch)
 
 
 def _na(radius=12.0, nf=5):
@@ -67,21 +121,33 @@ def _req(i, p, freqs=None, arrival=0.0):
     return ServeRequest(i, p, arrival=arrival, precision='mixed_bf16x3', pol_mask=1, tol=1.0)
 
 
-def test_requests_on_one_geometry_are_batched_and_sliced():
+def test_requests_join_a_running_batch_and_get_their_own_slice():
     p = _na()
     p.geometry_key = 'na'
     with _server(1 << 40, workers=1) as srv:
-        first = srv.submit(_req(0, p, [1.0, 2.0]))
-        time.sleep(0.01)                          # the first batch is running
+        first = srv.submit(_req(0, p, [1.0, 2.0, 3.0, 4.0, 5.0]))      # three outer steps
+        time.sleep(0.03)                                              # the first batch is running
         later = [srv.submit(_req(k, p, [10.0 * k, 10.0 * k + 1, 10.0 * k + 2])) for k in (1, 2, 3)]
         for r in [first] + later:
             assert r.done.wait(5)
-    assert first.batch_size == 1
-    assert all(r.batch_size == 3 for r in later)        # merged while the worker was busy
     for r in later:
+        assert r.t_start < first.t_done                   # joined while the first was in flight
+        assert r.batch_size >= 2
         np.testing.assert_array_equal(r.result['results'][:, 0], r.problem.freqs)
     builds = [e for e in FakeSolver.log if e[0] == 'build']
     assert len(builds) == 1                               # the geometry stayed resident
+
+
+def test_two_geometries_on_one_worker_share_grouped_steps():
+    a, b = _na(12.0), _na(13.0)
+    with _server(1 << 40, workers=1) as srv:
+        ra = srv.submit(_req(0, a, [1.0, 2.0, 3.0, 4.0, 5.0]))
+        rb = srv.submit(_req(1, b, [6.0, 7.0, 8.0, 9.0, 10.0]))
+        assert ra.done.wait(5) and rb.done.wait(5)
+    grouped = [e for e in FakeSolver.log if e[0] == 'step' and len(e[1]) == 2]
+    assert grouped and set(grouped[0][1]) == {id(ra.problem), id(rb.problem)}
+    assert ra.geometries_shared == 2 and rb.geometries_shared == 2
+    np.testing.assert_array_equal(rb.result['results'][:, 0], rb.problem.freqs)
 
 
 def test_admission_picks_matrix_free_when_t_does_not_fit_and_rejects_too_large():
@@ -117,11 +183,25 @@ def test_two_workers_overlap_different_geometries():
     with _server(1 << 40, workers=2) as srv:
         ra, rb = srv.submit(_req(0, a)), srv.submit(_req(1, b))
         assert ra.done.wait(5) and rb.done.wait(5)
-    solves = [e for e in FakeSolver.log if e[0] == 'solve']
-    assert len(solves) == 2
-    (s0, e0), (s1, e1) = [(x[4], x[5]) for x in solves]
-    assert max(s0, s1) < min(e0, e1)                       # the two solves ran at the same time
     assert ra.worker != rb.worker
+    sa = [(e[2], e[3]) for e in FakeSolver.log if e[0] == 'step' and e[1] == (id(a),)]
+    sb = [(e[2], e[3]) for e in FakeSolver.log if e[0] == 'step' and e[1] == (id(b),)]
+    assert sa and sb
+    # the two workers' steps ran at the same time
+    assert max(sa[0][0], sb[0][0]) < min(sa[-1][1], sb[-1][1])
+
+
+def test_plain_fp64_requests_are_solved_as_one_batch():
+    p = _na()
+    p.geometry_key = 'na64'
+    with _server(1 << 40, workers=1) as srv:
+        rs = [ServeRequest(k, p, precision='fp64', pol_mask=1, tol=1.0) for k in range(3)]
+        for r in rs:
+            srv.submit(r)
+        for r in rs:
+            assert r.done.wait(5) and r.error is None
+    solves = [e for e in FakeSolver.log if e[0] == 'solve']
+    assert 1 <= len(solves) <= 3
 
 
 def test_mix_statistics_and_pool_is_seeded():
