@@ -454,7 +454,16 @@ plx_status plx_complex_inversion(plx_geom *g, int32_t i_freq, double *variables_
         DevArray<double> V;
         V.alloc(g->ctx, 3 * 2 * (size_t)n);
         for (int c = 0; c < 3; ++c) upload_vec(g->ctx, variables_w + 2 * (size_t)n * c, n, V.p + (size_t)c * 2 * n);
-        solve_inversion_cols(g, i_freq, 3, V.p);
+        bool done = false;
+        if (hessenberg_applies(g, 3)) {
+            DevArray<double> Xh;
+            Xh.alloc(g->ctx, 3 * 2 * (size_t)n);
+            done = hessenberg_solve(g, {i_freq}, 3, V.p, Xh.p);
+            if (done)
+                PLX_CHECK_CUDA(cudaMemcpyAsync(V.p, Xh.p, 3 * 2 * (size_t)n * 8, cudaMemcpyDeviceToDevice,
+                                               g->ctx->stream));
+        }
+        if (!done) solve_inversion_cols(g, i_freq, 3, V.p);
         for (int c = 0; c < 3; ++c) download_vec(g->ctx, V.p + (size_t)c * 2 * n, n, variables_w + 2 * (size_t)n * c);
     });
 }
@@ -496,7 +505,7 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
         int fb = desc->freq_block;
         if (fb <= 0) {
             if (desc->mode == PLX_INVERSION) {
-                fb = 1;
+                fb = hessenberg_applies(g, np) ? F : 1;
             } else {
                 uint64_t avail = ctx->budget > ctx->in_use ? ctx->budget - ctx->in_use : 0;
                 // device bytes per complex column: the plain form keeps an FP64 Krylov
@@ -534,8 +543,17 @@ plx_status plx_solve(plx_geom *g, const plx_solve_desc *desc, double *x_out, dou
             PLX_CHECK_CUDA(cudaMemcpyAsync(dP.p, cp.data(), C * 4, cudaMemcpyHostToDevice, st));
             rhs_batch(g, OpBatch{C, dF.p}, dP.p, B.p);
             if (desc->mode == PLX_INVERSION) {
-                PLX_CHECK_CUDA(cudaMemcpyAsync(X.p, B.p, (size_t)C * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
-                for (int a = 0; a < nf; ++a) {
+                // scalar-shift models: every frequency of the block in one launch on the
+                // geometry's Hessenberg form; a singular factor falls back to the LU
+                bool done = false;
+                if (hessenberg_applies(g, np)) {
+                    std::vector<int32_t> fl(nf);
+                    for (int a = 0; a < nf; ++a) fl[a] = f0 + a;
+                    done = hessenberg_solve(g, fl, np, B.p, X.p);
+                }
+                if (!done)
+                    PLX_CHECK_CUDA(cudaMemcpyAsync(X.p, B.p, (size_t)C * 2 * n * 8, cudaMemcpyDeviceToDevice, st));
+                for (int a = 0; a < nf && !done; ++a) {
                     try {
                         solve_inversion_cols(g, f0 + a, np, X.p + (size_t)a * np * 2 * n);
                     } catch (const Error &e) {

@@ -175,6 +175,9 @@ struct plx_geom {
     plx::DevArray<double> d_part;
     // continuous batches open on this geometry (they own its frequency table)
     int open_batches = 0;
+    // Hessenberg reduction A0 = Q H Q^T of the scalar-shift models: reflectors
+    // (column k below row k), their 2 / v^T v, and H row-major
+    plx::DevArray<double> d_hess_v, d_hess_beta, d_hess_rows;
     // timing of the last plx_solve
     double last_ms = 0.0;
     int64_t last_launches = 0;
@@ -241,6 +244,14 @@ int tc_error(plx_geom *g);   // non-zero when a tensor-core CTA gave up waiting
 // inversion.cu
 // d_vars: [count][2][n] right-hand sides in, solutions of A(w_i) x = b out.
 void solve_inversion_cols(plx_geom *g, int i_freq, int count, double *d_vars);
+
+// hessenberg.cu: direct solve of the models whose frequency dependence is a
+// multiple of the identity (one-type wFQ, BEM DPCM): one Hessenberg reduction
+// per geometry, O(n^2) per frequency, every frequency of a call in one launch.
+bool hessenberg_applies(const plx_geom *g, int cols);
+void build_hessenberg(plx_geom *g);
+// B, X: [freqs.size() * cols][2][n]; false when a triangular factor is singular
+bool hessenberg_solve(plx_geom *g, const std::vector<int32_t> &freqs, int cols, const double *B, double *X);
 // C = A B for column-major n_var x n_var FP64 matrices (cuBLAS)
 void bem_dgemm(plx_geom *g, const double *A, const double *B, double *C);
 
