@@ -607,6 +607,10 @@ def run_reference(args):
     rank, world, local, pg = dist_setup()
     if rank != 0:
         return
+    if args.config == 'serving':
+        print(json.dumps({'impl': 'reference', 'unavailable': 'the reference has no request loop; its per-request '
+                                                             'cost is the ag_sphere / na_sphere / bem lines'}))
+        return
     if args.config == 'field_grid':
         from plasmonx_b200 import analysis as A
         prob, n = points_problem(args)
@@ -665,6 +669,51 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+SERVING_METRIC = 'freq-solves/s of a seeded Poisson request mix (p50/p99 latency), batched mixed vs plain FP64'
+
+
+def run_serving(args):
+    """Config 5: the seeded Poisson mix (wFQ Na, wFQFMu Ag/Au spheres and rods, BEM
+    spheres and rods, 20-400 frequencies each) through the serving loop, once with
+    the batched mixed-precision form and once with the plain FP64 GMRES, the same
+    requests in the same order; per-request sigma_abs of the two arms compared."""
+    from plasmonx_b200.serving import Server, request_pool, run_mix
+    n = max(1, args.serving_requests)
+    # warm-up: CUDA context, kernel attributes, allocator pools
+    with Server(device=0, workers=args.serving_workers) as srv:
+        run_mix(srv, request_pool(n_requests=4, rate=args.serving_rate, seed=99, scale='small'))
+    arms, results = {}, {}
+    for prec in ('mixed_bf16x3', 'fp64'):
+        pool = request_pool(n_requests=n, rate=args.serving_rate, seed=7, scale=args.serving_scale, precision=prec)
+        with Clocks(0) as clk:
+            with Server(device=0, workers=args.serving_workers) as srv:
+                st = run_mix(srv, pool)
+        steps = srv.steps
+        st.update({'clocks': clk.summary(), 'outer_steps': len(steps),
+                   'grouped_steps': sum(1 for s in steps if s[1] > 1),
+                   'max_geometries_per_step': max([s[1] for s in steps] or [0]),
+                   'mean_requests_per_step': float(np.mean([s[2] for s in steps])) if steps else 0.0,
+                   'mean_requests_sharing': float(np.mean([r.batch_size for r in pool])),
+                   'modes': sorted({str(r.mode) for r in pool})})
+        arms[prec] = st
+        results[prec] = [None if r.result is None else r.result['results'][:, 9] for r in pool]
+    errs = [float(np.max(np.abs(a - b) / np.abs(b))) for a, b in zip(results['mixed_bf16x3'], results['fp64'])
+            if a is not None and b is not None]
+    mixed = arms['mixed_bf16x3']
+    line = {'metric': SERVING_METRIC, 'value': mixed['throughput'], 'unit': 'freq-solves/s', 'n_gpus': 1,
+            'steps': 1, 'warmup': 1, 'ms_per_step': mixed['wall_s'] * 1000.0, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'bf16x3 (fp32 acc) + f64 refinement',
+            'data': 'synthetic (seeded request pool, reference default parameters)',
+            'config': {'workload': 'serving mix, %d requests at %g req/s, %s scale' % (n, args.serving_rate,
+                                                                                     args.serving_scale),
+                       'workers': args.serving_workers},
+            'p50_ms': mixed['p50_ms'], 'p99_ms': mixed['p99_ms'],
+            'fp64_plain': arms['fp64'], 'mixed': mixed,
+            'speedup_vs_fp64_plain': mixed['throughput'] / arms['fp64']['throughput'],
+            'sigma_abs_max_rel_err_vs_fp64_plain': max(errs) if errs else None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -673,7 +722,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', default='ag_sphere',
                     choices=['ag_sphere', 'na_sphere', 'bowtie', 'bem_sphere', 'bem_rod', 'fq_water', 'fqfmu_water',
-                             'field_grid'])
+                             'field_grid', 'serving'])
     ap.add_argument('--grid', type=int, default=100, help='grid points per axis of field_grid')
     ap.add_argument('--waters', type=int, default=0, help='water molecules of fq_water / fqfmu_water')
     ap.add_argument('--n-tess', type=int, default=2000, help='BEM tesserae (20 nu^2)')
@@ -699,7 +748,7 @@ def main():
     ap.add_argument('--n-freq', type=int, default=None, help='fewer frequencies (profiling runs only)')
     ap.add_argument('--serving-requests', type=int, default=24, help='requests in the serving leg (0: skip)')
     ap.add_argument('--serving-rate', type=float, default=20.0, help='Poisson arrival rate, requests/s')
-    ap.add_argument('--serving-scale', default='small', choices=['small', 'full'])
+    ap.add_argument('--serving-scale', default='small', choices=['small', 'medium', 'full'])
     ap.add_argument('--serving-workers', type=int, default=2)
     args = ap.parse_args()
     if args.impl == 'reference':
@@ -708,6 +757,8 @@ def main():
         return run_static(args)
     if args.config == 'field_grid':
         return run_points(args)
+    if args.config == 'serving':
+        return run_serving(args)
 
     rank, world, local, pg = dist_setup()
     from plasmonx_b200.solver import Context, Solver

@@ -535,8 +535,9 @@ def poisson_arrivals(n, rate, seed):
 def request_pool(n_requests=24, rate=20.0, seed=7, scale='small', precision='mixed_bf16x3'):
     """Seeded serving mix: wFQ Na spheres, wFQFMu Ag/Au spheres and rods, BEM spheres
     and rods, each with 20-400 frequencies in its material's window (the 'full' scale:
-    Na 500-20k atoms, Ag/Au 1k-30k atoms, BEM 1k-10k tesserae); 'small' keeps the same
-    kinds at 500-4k atoms / tesserae and 20-100 frequencies so a run takes seconds.
+    Na 500-20k atoms, Ag/Au 1k-30k atoms, BEM 1k-10k tesserae); 'medium' keeps the same
+    kinds at up to 8k atoms, 6k tesserae and 200 frequencies; 'small' at 500-4k atoms /
+    tesserae and 20-100 frequencies so a run takes seconds.
     Geometries repeat across requests (a third of the requests reuse an earlier
     geometry), which is what resident geometries and batching serve."""
     from . import configs
@@ -545,6 +546,8 @@ def request_pool(n_requests=24, rate=20.0, seed=7, scale='small', precision='mix
     arrivals = poisson_arrivals(n_requests, rate, seed)
     if scale == 'full':
         na_r, fmu_atoms, bem_t, fr = (13.0, 46.0), (1000, 30000), (1000, 10000), (20, 400)
+    elif scale == 'medium':
+        na_r, fmu_atoms, bem_t, fr = (13.0, 32.0), (1000, 8000), (1000, 6000), (20, 200)
     else:
         na_r, fmu_atoms, bem_t, fr = (13.0, 22.0), (500, 4000), (500, 4000), (20, 100)
     cache = []
