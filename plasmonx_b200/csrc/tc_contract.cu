@@ -186,13 +186,15 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
         nk = min(G.ktiles, kt0 + G.kper) - kt0;
     }
     const int bn = G.bn, M = G.M, R = G.R, ktiles = G.ktiles;
+    const int bnp = (bn + 31) & ~31;     // TMEM columns of one accumulator (32-aligned)
     const int STAGES = p.stages;
     const int kStage = tc_stage_bytes(p.bn_max);
     const int kA = kBM * kBK * 2;
     const int mtile = tile / G.ctiles;
     int *err = G.err;
     const uint32_t wait_limit = p.wait_limit;
-    // two accumulators of bn columns each (rows m0.. and m0 + 128..)
+    // two accumulators of bn columns each (rows m0.. and m0 + 128..), at TMEM
+    // columns 0 and bnp; bn_max is a multiple of 32
     const uint32_t tmem_cols = 2 * p.bn_max <= 64 ? 64 : (2 * p.bn_max <= 128 ? 128 : (2 * p.bn_max <= 256 ? 256 : 512));
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -276,7 +278,7 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
                 const uint32_t acc0 = (kt > 0 || kk > 0) ? 1u : 0u;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const uint32_t td = tmem + (uint32_t)(h * bn);
+                    const uint32_t td = tmem + (uint32_t)(h * bnp);
                     const uint64_t ho = h * kHalf;
                     umma_bf16(td, dTh + ho + off, dXh + off, idesc, acc0);
                     if (NPROD > 1) {
@@ -315,28 +317,42 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
 #pragma unroll 1
         for (int c0 = 0; c0 < bn; c0 += 32) {
             uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * bn + c0);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
-                  "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
-                  "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
+            const int nc = min(32, bn - c0);           // 32, or 16 for the last chunk
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * bnp + c0);
+            if (nc == 32) {
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+            } else {
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15])
+                    : "r"(taddr));
+#pragma unroll
+                for (int j = 16; j < 32; ++j) v[j] = 0u;
+            }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (piece >= 0) {
                 // partial of a split tile: [column][256 rows] FP32, every element written
                 float *pp = G.P + (int64_t)piece * kBM * bn + (h * kUM + warp * 32 + lane);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) pp[(int64_t)(c0 + j) * kBM] = __uint_as_float(v[j]);
+                for (int j = 0; j < 32; ++j)
+                    if (j < nc) pp[(int64_t)(c0 + j) * kBM] = __uint_as_float(v[j]);
             } else if (row < M) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int c = n0 + c0 + j;
-                    if (c < R) G.S[(int64_t)c * M + row] = (double)__uint_as_float(v[j]);
+                    if (j < nc && c < R) G.S[(int64_t)c * M + row] = (double)__uint_as_float(v[j]);
                 }
             }
         }
@@ -791,9 +807,10 @@ void tc_contract_group(const std::vector<TcItem> &items) {
         const int M = it.folded ? (int)g->fold_rows : n;
         const int R = 2 * it.count;
         const int64_t ld = g->ldk;
-        // column tiles: as few as possible, each a multiple of 32 columns (<= 256)
+        // column tiles: as few as possible, each a multiple of 16 columns (<= 256, the
+        // MMA's N granularity, which keeps the padding of a tile under 16 columns)
         const int ntile = (R + 255) / 256;
-        const int bn = ((R + ntile - 1) / ntile + 31) / 32 * 32;
+        const int bn = ((R + ntile - 1) / ntile + 15) / 16 * 16;
         const int Rpad = ntile * bn;
         const size_t need = (size_t)Rpad * ld;
         if (g->d_Xh.n < need) {
@@ -827,7 +844,7 @@ void tc_contract_group(const std::vector<TcItem> &items) {
             gp.P = g->d_tcpart.p;
             post.push_back({k, rem});
         }
-        bn_max = std::max(bn_max, bn);
+        bn_max = std::max(bn_max, (bn + 31) / 32 * 32);
         if (!g->d_tc_err.p) throw Error(PLX_ERR_CUDA, "tensor-core error word missing");
         gp.err = g->d_tc_err.p;
     }
@@ -843,7 +860,7 @@ void tc_contract_group(const std::vector<TcItem> &items) {
     PLX_CHECK_CUDA(cudaGetLastError());
     for (const Post &q : post) {
         const TcGroup &gp = L.grp[q.gi];
-        reduce_pieces<<<dim3(q.rem, gp.bn / 32), kBM, 0, ctx->stream>>>(gp.M, gp.R, gp.bn, gp.full, gp.ctiles, gp.q,
+        reduce_pieces<<<dim3(q.rem, (gp.bn + 31) / 32), kBM, 0, ctx->stream>>>(gp.M, gp.R, gp.bn, gp.full, gp.ctiles, gp.q,
                                                                       gp.P, gp.S);
         ctx->launches++;
     }
