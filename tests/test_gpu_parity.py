@@ -119,17 +119,19 @@ def test_solve_matches_oracle(ctx, name):
     scale = np.abs(ref['results']).max(axis=0) + 1e-300
     err = np.abs(out['results'] - ref['results']) / scale
     if method == 'inversion':
-        # two FP64 LU solves of the same A(w) agree to ~cond(A) eps in the solution
-        # (held to 50 eps cond per frequency); a result column that is small at some
-        # frequencies (Im alpha of graphene at its lowest frequency, cond 1.4e4)
-        # carries that error relative to the whole solution, so the results are held
-        # to 1e-9 of their column scale
+        # two backward-stable FP64 solves of the same A(w) (the oracle's LU; here LU,
+        # or for one-type wFQ and BEM DPCM the shifted Hessenberg solve) agree to
+        # ~cond(A) eps in the solution (held to 50 eps cond per frequency); the
+        # results are held to 1e-10 of their column scale, or where cond(A(w)) makes
+        # that unattainable (graphene at its lowest frequency, cond 1.4e4) to
+        # 100 eps cond(A(w)) at that frequency
         x, xr = out['x'], np.asarray(ref['x'])
         dx = np.linalg.norm((x - xr).reshape(len(x), -1), axis=1) / np.linalg.norm(xr.reshape(len(x), -1), axis=1)
         op = model.Operator(s)
         cond = np.array([np.linalg.cond(op.matrix(i)) for i in range(len(x))])
         assert np.all(dx <= 50 * 2.22e-16 * cond)
-        assert err.max() < 1e-9
+        bar = np.maximum(1e-10, 100 * 2.22e-16 * cond)[:, None]
+        assert np.all(err <= bar), (err.max(axis=1), bar[:, 0])
     else:
         # same algorithm at the same (loose) tolerance; differences are round-off
         # amplified by the Krylov recurrence, bounded by the tolerance itself.
@@ -148,8 +150,8 @@ def test_solve_matches_oracle(ctx, name):
 @pytest.mark.parametrize('mode', ['iterative', 'iterative on the fly'])
 def test_tight_gmres_matches_lu(ctx, name, mode):
     """sigma_abs of the FP64 GPU solves at tight tolerances against the oracle LU:
-    the reference's (unrestarted) GMRES at a 1e-11 relative residual within 1e-9,
-    and the FP64 refinement (restarted, explicit FP64 residuals) at 1e-12 within 1e-10.
+    the reference's (unrestarted) GMRES and the FP64 refinement (restarted,
+    explicit FP64 residuals), both at a 1e-12 relative residual, within 1e-10.
     (The explicit FP64 residual of the sodium operator bottoms out near 1e-13 of |b|,
     since the charge rows difference neighbouring potentials: 1e-13 is not reliably
     attainable there, while the answer is already accurate to ~2e-13.)"""
@@ -162,10 +164,10 @@ def test_tight_gmres_matches_lu(ctx, name, mode):
     with Solver(p, ctx=ctx, store_t=True) as sv:
         sv.set_frequencies(p.freqs[freqs], None if p.alpha_w is None else p.alpha_w[:, freqs])
         nb = np.linalg.norm(sv.rhs(0, 7)[:, 0])
-        plain = sv.solve(mode=mode, tol=1e-11 * nb, max_krylov=p.n_var)
+        plain = sv.solve(mode=mode, tol=1e-12 * nb, max_krylov=p.n_var)
         refined = sv.solve(mode=mode, precision='fp64_refined', tol=1e-12 * nb, inner_krylov=p.n_var,
                            inner_tol=1e-13, max_outer=10)
-    for out, bar in ((plain, 1e-9), (refined, 1e-10)):
+    for out, bar in ((plain, 1e-10), (refined, 1e-10)):
         assert (out['status'] == 0).all(), out['status']
         sig = out['results'][:, 9:12]
         assert np.max(np.abs(sig - sref)[mask] / np.abs(sref)[mask]) < bar
