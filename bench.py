@@ -92,8 +92,10 @@ PEAKS_FALLBACK = {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustain
 # spectrum, measured on B200; used to turn the CPU arm's timed products and
 # orthogonalisations into freq-solves/s.
 STEPS_PER_SOLVE = {'ag_sphere': 335.6, 'na_sphere': 60.0, 'bowtie': 600.0, 'bem_sphere': 60.0, 'bem_rod': 60.0}
-# measured DRAM bytes / algorithmic bytes of the tensor-core contraction (ncu, small case)
-TRAFFIC_RATIO = 1.004
+# measured DRAM bytes / operand bytes of the tensor-core contraction: ncu of the first two
+# launches of a 21,560-unknown sphere at 402 columns (two column tiles that share each
+# operand tile through L2): 1.972 GB read + 0.065 GB written per launch, operand 1.877 GB
+TRAFFIC_RATIO = (1.972 + 0.065) / 1.877
 
 
 def peaks():
@@ -781,7 +783,10 @@ def main():
         # the inner basis length from a short sweep on a few of the grid's frequencies
         # (plasmonx_b200.tuning), cached per geometry; not part of the timed region
         from plasmonx_b200.tuning import Tuner
-        tuner = Tuner(n_probe=min(48, len(full_freqs)))
+        # the probe is the whole grid (up to 256 frequencies): the balance between the
+        # contraction (cheaper per column as columns grow) and the orthogonalisation
+        # (linear in columns and basis length) depends on the column count
+        tuner = Tuner(n_probe=min(256, len(full_freqs)))
         chosen = tuner.settings(solver, args.config, full_freqs, full_aw, precision=args.precision,
                                 mode=prob.method, tol=prob.tol)
         args.inner_krylov = chosen['inner_krylov']
@@ -902,10 +907,16 @@ def main():
 
     pk, pk_kind = peaks()
     n = prob.n_var
+    tc_operand = 4.0 * (-(-n // 256) * 256) * (-(-n // 64) * 64)
     avg_ms = prof['ms'] / max(1, prof['launches'])
     bytes_per = prof['bytes'] / max(1, prof['launches'])
     flops_per = prof['flops'] / max(1, prof['launches'])
-    if args.precision == 'fp64':
+    if prof['launches'] == 0:
+        # direct inversion: no contraction to bound (the shifted Hessenberg solves are
+        # latency-bound per CTA; the LU path is cuSOLVER's)
+        roof = {'kernel': 'none timed (direct inversion mode)', 'bound': None, 'achieved': None, 'peak': None,
+                'unit': None, 'frac': None, 'traffic': None}
+    elif args.precision == 'fp64':
         roof = {'kernel': 'T contraction (FP64, CUDA cores)', 'bound': 'hbm',
                 'achieved': bytes_per / (avg_ms / 1000.0) / 1e9, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
                 'peak_kind': pk_kind, 'flops_per_launch': flops_per, 'bytes_per_launch': bytes_per,
@@ -922,10 +933,13 @@ def main():
                 'achieved_hbm_gbs': bytes_per / (avg_ms / 1000.0) / 1e9,
                 # DRAM bytes per launch: the ncu capture of the 7,844-unknown case read its
                 # operand 1.004 times (X tiles come from L2); traffic grows with the operand
-                'traffic': bytes_per * TRAFFIC_RATIO, 'traffic_unit': 'bytes per launch',
-                'traffic_source': 'ncu dram__bytes of a 7,844-unknown capture, scaled by operand bytes',
+                'traffic': tc_operand * TRAFFIC_RATIO, 'traffic_unit': 'bytes per launch',
+                'traffic_source': 'ncu dram__bytes (read + write) of a 21,560-unknown, 402-column capture per '
+                                  'operand byte (1.086), times this launch\'s operand bytes (BF16 high + low, '
+                                  'padded tiles)',
                 'note': 'achieved counts one product (algorithmic); the tensor pipe executes %d' % nprod}
-    roof['frac'] = roof['achieved'] / roof['peak']
+    if roof['achieved'] is not None:
+        roof['frac'] = roof['achieved'] / roof['peak']
 
     # serving leg: a seeded Poisson mix of spectrum requests through the request loop
     serving = None
