@@ -68,10 +68,11 @@ def gmres(matvec, b, tol, restart, max_iter=1, trace=None, snapshots=None):
                 H[i, j] = np.vdot(V[:, i], w)
                 w = w - H[i, j] * V[:, i]
         else:
+            # V^H w as conj(w^H V): the same sums without copying the conjugated basis
             Vj = V[:, :j + 1]
-            h = Vj.conj().T @ w
+            h = (w.conj() @ Vj).conj()
             w = w - Vj @ h
-            t = Vj.conj().T @ w
+            t = (w.conj() @ Vj).conj()
             w = w - Vj @ t
             H[:j + 1, j] = h + t
         H[j + 1, j] = np.linalg.norm(w)
