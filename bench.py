@@ -108,12 +108,12 @@ def peaks():
 
 
 def make_problem(name, n_freq=None, method='iterative', polarization='x', radius=None, n_tess=2000,
-                 bem_variant='dpcm', bowtie_edge=80.0):
+                 bem_variant='dpcm', bowtie_edge=80.0, bem_green='approximate'):
     from plasmonx_b200 import configs
     if name in ('bem_sphere', 'bem_rod'):
         from plasmonx_b200.bem import bem_surface
         return bem_surface(n_tess, variant=bem_variant, shape=name[4:], n_freq=n_freq or 301, method=method,
-                           tolerance=1e-9, polarization=polarization, gmres_dim=1000)
+                           tolerance=1e-9, polarization=polarization, gmres_dim=1000, green=bem_green)
     if name == 'ag_sphere':
         return configs.ag_sphere(radius=radius or 35.0, n_freq=n_freq or 201, method=method, tolerance=1e-9,
                                  polarization=polarization, gmres_dim=1000)
@@ -730,6 +730,7 @@ def main():
     ap.add_argument('--n-tess', type=int, default=2000, help='BEM tesserae (20 nu^2)')
     ap.add_argument('--bowtie-edge', type=float, default=80.0, help='prism edge (A): 80 gives 5,850 atoms, 180 ~30k')
     ap.add_argument('--bem-variant', default='dpcm', choices=['dpcm', 'iefpcm'])
+    ap.add_argument('--bem-green', default='approximate', choices=['approximate', 'accurate'])
     ap.add_argument('--precision', default='mixed_bf16x3')
     ap.add_argument('--tolerance', type=float, default=1e-12, help='input tolerance (times sqrt(n_var))')
     ap.add_argument('--no-fp64-compare', action='store_true')
@@ -769,7 +770,7 @@ def main():
     # out in blocks of one workload's frequencies per rank, results gathered to rank 0
     base_f = args.n_freq or {'ag_sphere': 201, 'na_sphere': 61, 'bowtie': 201}.get(args.config, 301)
     prob = make_problem(args.config, n_freq=base_f * world, radius=args.radius, n_tess=args.n_tess,
-                        bem_variant=args.bem_variant, bowtie_edge=args.bowtie_edge)
+                        bem_variant=args.bem_variant, bowtie_edge=args.bowtie_edge, bem_green=args.bem_green)
     prob.tolerance_input = args.tolerance
     prob.tol = args.tolerance * np.sqrt(prob.n_var)
     if args.mode:
