@@ -791,6 +791,8 @@ def main():
         chosen = tuner.settings(solver, args.config, full_freqs, full_aw, precision=args.precision,
                                 mode=prob.method, tol=prob.tol)
         args.inner_krylov = chosen['inner_krylov']
+        if not args.inner_tol:
+            args.inner_tol = chosen['inner_tol']
         tuning = tuner.records[args.config]
     gathered = {}
 

@@ -12,6 +12,10 @@ geometry, not on the hardware alone:
                 whole grid does not fit the device budget, then blocks of 64,
                 32, 16 or 8.
 
+and the inner solve's relative tolerance (1e-3, 1e-4, 1e-5 around the best
+basis): a looser inner solve costs more FP64 residuals, a tighter one more
+inner steps.
+
 ``Tuner.settings(solver, key)`` runs a short sweep once per resident geometry
 -- the candidate settings on a few frequencies spread over the grid, each timed
 by the library's own CUDA events -- and caches the fastest (device time per
@@ -21,13 +25,15 @@ it.  The sweep's records are kept for the report.
 import numpy as np
 
 INNER_CANDIDATES = (64, 128, 256)
+INNER_TOL_CANDIDATES = (1e-3, 1e-5)       # tried around the default 1e-4 for the best basis
 BLOCK_CANDIDATES = (0, 64, 32, 16, 8)
 
 
 class Tuner:
-    def __init__(self, n_probe=6, inner_candidates=INNER_CANDIDATES):
+    def __init__(self, n_probe=6, inner_candidates=INNER_CANDIDATES, inner_tol_candidates=INNER_TOL_CANDIDATES):
         self.n_probe = int(n_probe)
         self.inner_candidates = tuple(inner_candidates)
+        self.inner_tol_candidates = tuple(inner_tol_candidates)
         self.cache = {}
         self.records = {}
 
@@ -49,18 +55,25 @@ class Tuner:
             block = next((b for b in BLOCK_CANDIDATES if (b == 0 or b < F) and fits(b)), 8)
         sweep = []
         solver.set_frequencies(np.asarray(freqs)[idx], None if alpha_w is None else np.asarray(alpha_w)[:, idx])
+        def trial(m, itol):
+            out = solver.solve(mode=mode, precision=precision, pol_mask=pol_mask, tol=tol, inner_krylov=m,
+                               inner_tol=itol)
+            ok = 'error' not in out and bool(np.all(out['status'] == 0))
+            per = out['device_ms'] / max(1, len(idx)) if ok else float('inf')
+            sweep.append({'inner_krylov': m, 'inner_tol': itol or 1e-4, 'ms_per_freq_solve': per, 'ok': ok})
+
         try:
             for m in self.inner_candidates:
-                m_eff = min(m, int(solver.n_var))
-                out = solver.solve(mode=mode, precision=precision, pol_mask=pol_mask, tol=tol, inner_krylov=m_eff)
-                ok = 'error' not in out and bool(np.all(out['status'] == 0))
-                per = out['device_ms'] / max(1, len(idx)) if ok else float('inf')
-                sweep.append({'inner_krylov': m_eff, 'ms_per_freq_solve': per, 'ok': ok})
+                trial(min(m, int(solver.n_var)), 0.0)
+            m_best = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))['inner_krylov']
+            for itol in self.inner_tol_candidates:
+                trial(m_best, itol)
         finally:
             solver.set_frequencies(freqs, alpha_w)
         best = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))
-        chosen = {'inner_krylov': best['inner_krylov'] if np.isfinite(best['ms_per_freq_solve']) else 64,
-                  'freq_block': block}
+        good = np.isfinite(best['ms_per_freq_solve'])
+        chosen = {'inner_krylov': best['inner_krylov'] if good else 64,
+                  'inner_tol': best['inner_tol'] if good else 1e-4, 'freq_block': block}
         self.cache[key] = chosen
         self.records[key] = {'probe_freqs': [int(i) for i in idx], 'sweep': sweep, 'chosen': chosen}
         return chosen
