@@ -974,7 +974,7 @@ def main():
                 'data': ('synthetic (seeded geodesic surface, Drude-Lorentz eps)' if is_bem(prob) else
                          'synthetic (seeded fcc lattice, reference default parameters)'),
                 'config': dict(workload_desc(args.config, prob), precision=args.precision,
-                               inner_krylov=args.inner_krylov or 64,
+                               inner_krylov=args.inner_krylov or 64, inner_tol=args.inner_tol or 1e-4,
                                **({'partition': 'one spectrum of %d frequencies over the window, dealt round-robin '
                                                 '(%d per rank), results gathered to rank 0' % (len(full_freqs), F),
                                    'gathered': gathered} if world > 1 else {})),
