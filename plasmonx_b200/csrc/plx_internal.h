@@ -419,6 +419,12 @@ void bem_field_at_points(plx_ctx *ctx, int n, const double *centres, const doubl
 void neighbour_counts(plx_ctx *ctx, int n, int nt, const double *coord_ang, const int32_t *atom_type,
                       const int32_t *type_z, const double *r0, int32_t *nb_out, int32_t *n_nb_out);
 
+// cholesky.cu: dense FP64 Cholesky of an n x n column-major SPD matrix (lower
+// triangle) in place; returns 0 or the 1-based column of a non-positive pivot;
+// and the solves L L^T X = B for nrhs columns in place
+int cholesky_factor(plx_ctx *ctx, int n, double *A);
+void cholesky_solve(plx_ctx *ctx, int n, const double *L, int nrhs, double *B);
+
 // static_fq.cu: static FQ / FQFMu solves and the principal-axis rotation
 int64_t static_n_var(const plx_static_desc *d);
 void static_solve(plx_ctx *ctx, const plx_static_desc *d, int what, double *variables, double *energy,

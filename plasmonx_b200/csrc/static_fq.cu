@@ -506,24 +506,12 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int mode, int
                                          Rr.p, variables, energy, polar);
     }
     prof_begin(ctx);
-    cusolverDnHandle_t h = solver_handle(ctx);
-    int lwork = 0;
-    if (cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nr, Kr.p, nr, &lwork) != CUSOLVER_STATUS_SUCCESS)
-        throw Error(PLX_ERR_CUDA, "cusolverDnDpotrf_bufferSize failed");
-    work.alloc(ctx, std::max(lwork, 1));
-    info.alloc(ctx, 1);
-    if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, nr, Kr.p, nr, work.p, lwork, info.p) != CUSOLVER_STATUS_SUCCESS)
-        throw Error(PLX_ERR_CUDA, "cusolverDnDpotrf failed");
-    int hinfo = 0;
-    PLX_CHECK_CUDA(cudaMemcpyAsync(&hinfo, info.p, 4, cudaMemcpyDeviceToHost, st));
-    PLX_CHECK_CUDA(cudaStreamSynchronize(st));
-    if (hinfo != 0) {
+    // hand-written blocked Cholesky (cholesky.cu) in place of dpotrf / dpotrs
+    if (cholesky_factor(ctx, nr, Kr.p) != 0) {
         prof_end(ctx, kProfStaticFactor, 0.0, 0.0);
         return false;  // not positive definite: the caller factors the full system
     }
-    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, nr, ncols, Kr.p, nr, Br.p, nr, info.p) != CUSOLVER_STATUS_SUCCESS)
-        throw Error(PLX_ERR_CUDA, "cusolverDnDpotrs failed");
-    check_info(ctx, info, "DPOTRS of the reduced static matrix");
+    cholesky_solve(ctx, nr, Kr.p, ncols, Br.p);
     prof_end(ctx, kProfStaticFactor, dr * dr * dr / 3.0 + 2.0 * dr * dr * ncols, 8.0 * dr * dr);
     return finish_eliminated(ctx, s, N, nr, nrhs, d_keep.p, d_lo, d_hi, K.p, B.p, Bt.p, Br.p, Rr.p, variables,
                              energy, polar);
