@@ -201,8 +201,58 @@ void lu_solve(plx_ctx *ctx, int n, double *A, int nrhs, double *B, const char *w
     check_info(ctx, info, what);
 }
 
+// Z[:, j] = K Y[:, j] for nrhs <= 3 columns (K N x N column-major), in
+// kGemvChunks column chunks (partials Zp[chunk][j][r], then summed in chunk
+// order): one thread per row and chunk, K read once (coalesced), Y broadcast.
+constexpr int kGemvChunks = 16;
+__global__ void dense_gemv_part(int N, int nrhs, const double *__restrict__ K, const double *__restrict__ Y,
+                                double *__restrict__ Zp) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    const int per = (N + kGemvChunks - 1) / kGemvChunks;
+    const int c0 = blockIdx.y * per, c1 = min(N, c0 + per);
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int c = c0; c < c1; ++c) {
+        const double k = K[(int64_t)c * N + r];
+        for (int j = 0; j < nrhs; ++j) acc[j] = fma(k, Y[c + (int64_t)N * j], acc[j]);
+    }
+    for (int j = 0; j < nrhs; ++j) Zp[((int64_t)blockIdx.y * nrhs + j) * N + r] = acc[j];
+}
+
+__global__ void dense_gemv_sum(int N, int nrhs, const double *__restrict__ Zp, double *__restrict__ Z) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)N * nrhs) return;
+    double s = 0.0;
+    for (int q = 0; q < kGemvChunks; ++q) s += Zp[(int64_t)q * nrhs * N + e];
+    Z[e] = s;
+}
+
+// C[i + m j] = sum_p A[p + lda i] B[p + ldb j], one block per output (fixed order).
+__global__ void small_gemm_tn(int m, int n, const double *__restrict__ A, int lda, const double *__restrict__ B,
+                              int ldb, double *__restrict__ C) {
+    const int i = blockIdx.x % m, j = blockIdx.x / m;
+    double s = 0.0;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) s += A[p + (int64_t)lda * i] * B[p + (int64_t)ldb * j];
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        C[blockIdx.x] = t;
+    }
+}
+
 // C (m x k) = A^T B with A (n x m, lda) and B (n x k, ldb), column-major
 void gemm_tn(plx_ctx *ctx, int m, int k, int n, const double *A, int lda, const double *B, int ldb, double *C) {
+    if (m * k <= 64) {
+        // a few outputs (the 3 x 3 polarizability): block reductions
+        small_gemm_tn<<<m * k, 256, 0, ctx->stream>>>(m, n, A, lda, B, ldb, C);
+        ctx->launches++;
+        PLX_CHECK_CUDA(cudaGetLastError());
+        return;
+    }
     const double one = 1.0, zero = 0.0;
     if (cublasDgemm(blas_handle(ctx), CUBLAS_OP_T, CUBLAS_OP_N, m, k, n, &one, A, lda, B, ldb, &zero, C, m) !=
         CUBLAS_STATUS_SUCCESS)
@@ -532,11 +582,13 @@ bool finish_eliminated(plx_ctx *ctx, const StaticDims &s, int N, int nr, int nrh
     V.alloc(ctx, (size_t)nv * nrhs);
     PLX_CHECK_CUDA(cudaMemsetAsync(Y.p, 0, (size_t)N * nrhs * 8, st));
     scatter_kept<<<dim3(n_blocks(nr, 128), nrhs), 128, 0, st>>>(nr, nrhs, N, d_keep, Br, Y.p);
+    if (nrhs > 3) throw Error(PLX_ERR_ARG, "at most three static right-hand sides");
     {
-        const double one = 1.0, zero = 0.0;  // Z = (H K H) y
-        if (cublasDgemm(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_N, N, nrhs, N, &one, K, N, Y.p, N, &zero, Z.p,
-                        N) != CUBLAS_STATUS_SUCCESS)
-            throw Error(PLX_ERR_CUDA, "cublasDgemm failed");
+        DevArray<double> Zp;                                               // Z = (H K H) y
+        Zp.alloc(ctx, (size_t)kGemvChunks * nrhs * N);
+        dense_gemv_part<<<dim3(n_blocks(N, 128), kGemvChunks), 128, 0, st>>>(N, nrhs, K, Y.p, Zp.p);
+        dense_gemv_sum<<<n_blocks((int64_t)N * nrhs, 256), 256, 0, st>>>(N, nrhs, Zp.p, Z.p);
+        ctx->launches += 2;
     }
     multipliers<<<n_blocks((int64_t)m * nrhs, 128), 128, 0, st>>>(m, nrhs, N, n, nv, d_lo, d_hi, Bt, Z.p, V.p);
     reflect_rows<<<n_blocks((int64_t)m * nrhs, 128), 128, 0, st>>>(m, nrhs, N, d_lo, d_hi, Y.p);
@@ -549,9 +601,14 @@ bool finish_eliminated(plx_ctx *ctx, const StaticDims &s, int N, int nr, int nrh
         PLX_CHECK_CUDA(cudaMemcpy2DAsync(V.p + n + m, (size_t)nv * 8, Y.p + n, (size_t)N * 8, (size_t)(N - n) * 8,
                                          nrhs, cudaMemcpyDeviceToDevice, st));
     if (energy) {
-        double dot = 0.0;  // the constraint rows' right-hand side is zero
-        if (cublasDdot(blas_handle(ctx), N, Y.p, 1, B, 1, &dot) != CUBLAS_STATUS_SUCCESS)
-            throw Error(PLX_ERR_CUDA, "cublasDdot failed");
+        // the constraint rows' right-hand side is zero: y . b over the N rows
+        DevArray<double> dd;
+        dd.alloc(ctx, 1);
+        small_gemm_tn<<<1, 256, 0, st>>>(1, N, Y.p, N, B, N, dd.p);
+        ctx->launches++;
+        double dot = 0.0;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(&dot, dd.p, 8, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
         *energy = -0.5 * dot;
     }
     if (variables)
