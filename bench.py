@@ -943,6 +943,9 @@ def main():
                 'note': 'achieved counts one product (algorithmic); the tensor pipe executes %d' % nprod}
     if roof['achieved'] is not None:
         roof['frac'] = roof['achieved'] / roof['peak']
+        if 'issued_tensor_tflops' in roof:
+            # the BF16 products the tensor pipe executes (3 per algorithmic product for bf16x3)
+            roof['issued_frac'] = roof['issued_tensor_tflops'] / roof['peak']
 
     # serving leg: a seeded Poisson mix of spectrum requests through the request loop
     serving = None
