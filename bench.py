@@ -955,10 +955,14 @@ def main():
                             scale=args.serving_scale, precision=args.precision)
         with Server(device=local, workers=args.serving_workers) as srv:
             serving = run_mix(srv, pool)
+        steps = srv.steps
         serving.update({'rate_per_s': args.serving_rate, 'scale': args.serving_scale,
                         'workers': args.serving_workers, 'precision': args.precision,
                         'modes': sorted({str(r.mode) for r in pool}),
-                        'mean_batch_requests': float(np.mean([r.batch_size for r in pool])),
+                        'mean_requests_sharing_a_step': float(np.mean([r.batch_size for r in pool])),
+                        'outer_steps': len(steps),
+                        'grouped_steps': sum(1 for st_ in steps if st_[1] > 1),
+                        'max_geometries_per_step': max([st_[1] for st_ in steps] or [0]),
                         'p99_ms_max_over_ranks': allmax(pg, serving['p99_ms'], local)})
 
     cpu = None
