@@ -77,16 +77,13 @@ __global__ void gather_cols(int n, const int32_t *__restrict__ act, const VT *__
 }
 
 // Partial complex dots conj(V_i[c]) . W[k] for i in [i0, i1) over one chunk of
-// kDotRows rows.  Every thread keeps kDotPT entries of W in registers and
-// accumulates the dots of 16 basis vectors at a time (independent loads, no
-// reduction inside the loop); a warp then reduces its 16 complex partials with
-// one exchange of halves per level (31 shuffles per component for all 16, where
-// 16 separate warp sums take 80), lane l ending with vector l % 16, and a
-// fixed-order sum over the warps follows.  Single-vector projections (modified
-// Gram-Schmidt) take the same path with one active vector.
+// kDotRows rows: every thread keeps kDotPT entries of W in registers and all
+// eight warps work on every basis vector (warp reduction, then a fixed-order
+// sum over the warps), so the kernel is bandwidth-bound for any number of
+// basis vectors, including the single-vector projections of modified
+// Gram-Schmidt.
 constexpr int kDotPT = 4;
 constexpr int kDotRows = kThreads * kDotPT;
-constexpr int kDotV = 16;            // basis vectors per pass
 
 template <typename VT>
 __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
@@ -94,7 +91,7 @@ __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
                                                          VT *const *__restrict__ slabs,
                                                          const double *__restrict__ W,
                                                          double2 *__restrict__ part) {
-    __shared__ double red_re[kThreads / 32][kDotV], red_im[kThreads / 32][kDotV];
+    __shared__ double2 red[kThreads / 32][32];
     const int k = blockIdx.y, c = act[k];
     const int r0 = blockIdx.x * kDotRows;
     const double *wr = W + (int64_t)k * 2 * n;
@@ -107,56 +104,32 @@ __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ni = i1 - i0;
-    for (int g0 = 0; g0 < ni; g0 += kDotV) {
-        const int gn = min(kDotV, ni - g0);
-        double are[kDotV], aim[kDotV];
+    for (int g0 = 0; g0 < ni; g0 += 32) {
+        const int gn = min(32, ni - g0);
+        for (int t = 0; t < gn; ++t) {
+            const VT *v = slabs[i0 + g0 + t] + (int64_t)c * 2 * n;
+            double re = 0.0, im = 0.0;
 #pragma unroll
-        for (int t = 0; t < kDotV; ++t) {
-            are[t] = 0.0;
-            aim[t] = 0.0;
-            if (t < gn) {
-                const VT *v = slabs[i0 + g0 + t] + (int64_t)c * 2 * n;
-#pragma unroll
-                for (int q = 0; q < kDotPT; ++q) {
-                    int r = r0 + threadIdx.x + kThreads * q;
-                    if (r < n) {
-                        double vr = (double)v[r], vi = (double)v[n + r];
-                        are[t] += vr * wre[q] + vi * wim[q];      // conj(v) * w
-                        aim[t] += vr * wim[q] - vi * wre[q];
-                    }
+            for (int q = 0; q < kDotPT; ++q) {
+                int r = r0 + threadIdx.x + kThreads * q;
+                if (r < n) {
+                    double vr = (double)v[r], vi = (double)v[n + r];
+                    re += vr * wre[q] + vi * wim[q];      // conj(v) * w
+                    im += vr * wim[q] - vi * wre[q];
                 }
             }
-        }
-        // lanes l and l ^ 16 first add their 16 values, then halves are exchanged
-#pragma unroll
-        for (int t = 0; t < kDotV; ++t) {
-            are[t] += __shfl_xor_sync(0xffffffffu, are[t], 16);
-            aim[t] += __shfl_xor_sync(0xffffffffu, aim[t], 16);
-        }
-#pragma unroll
-        for (int off = kDotV / 2; off >= 1; off >>= 1) {
-            const bool up = (lane & off) != 0;
-#pragma unroll
-            for (int t = 0; t < off; ++t) {
-                const double sre = up ? are[t] : are[t + off], kre = up ? are[t + off] : are[t];
-                const double sim = up ? aim[t] : aim[t + off], kim = up ? aim[t + off] : aim[t];
-                are[t] = kre + __shfl_xor_sync(0xffffffffu, sre, off);
-                aim[t] = kim + __shfl_xor_sync(0xffffffffu, sim, off);
-            }
-        }
-        // lane l holds the warp's dot of vector g0 + (l & 15)
-        if (lane < kDotV) {
-            red_re[warp][lane] = are[0];
-            red_im[warp][lane] = aim[0];
+            re = warp_sum(re);
+            im = warp_sum(im);
+            if (lane == 0) red[warp][t] = make_double2(re, im);
         }
         __syncthreads();
         if (threadIdx.x < gn) {
-            double2 sum = make_double2(0.0, 0.0);
+            double2 s = make_double2(0.0, 0.0);
             for (int w = 0; w < kThreads / 32; ++w) {
-                sum.x += red_re[w][threadIdx.x];
-                sum.y += red_im[w][threadIdx.x];
+                s.x += red[w][threadIdx.x].x;
+                s.y += red[w][threadIdx.x].y;
             }
-            part[((int64_t)k * gridDim.x + blockIdx.x) * ni + g0 + threadIdx.x] = sum;
+            part[((int64_t)k * gridDim.x + blockIdx.x) * ni + g0 + threadIdx.x] = s;
         }
         __syncthreads();
     }
