@@ -321,6 +321,30 @@ def _time_orthogonalisation(n, j, reps=5):
     return (time.perf_counter() - t0) / reps
 
 
+def _lu_reference(prob, n, budget_s):
+    """The reference's inversion mode on the host cores: per frequency a complex LU
+    of the n x n matrix and the solves for the three field directions (zgetrf +
+    zgetrs, algorithm_module.f90:510-541), threaded LAPACK.  Timed at n when the
+    factorisation is short, else on a 4,000-unknown matrix scaled by (n / 4000)^3."""
+    from scipy.linalg import lu_factor, lu_solve
+    ns = min(n, 4000)
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((ns, ns)) + 1j * rng.standard_normal((ns, ns)) + ns * np.eye(ns)
+    B = rng.standard_normal((ns, 3)) + 0j
+    lu_solve(lu_factor(A), B)
+    done, t0 = 0, time.perf_counter()
+    while done < 1 or (time.perf_counter() - t0 < budget_s and done < 20):
+        lu_solve(lu_factor(A, overwrite_a=False, check_finite=False), B, check_finite=False)
+        done += 1
+    t = (time.perf_counter() - t0) / done * (n / ns) ** 3
+    scaled = '' if ns == n else ', scaled by (%d / %d)^3' % (n, ns)
+    return {'value': 1.0 / t, 'unit': 'freq-solves/s', 'cores': int(_blas_threads()), 'kind': 'port',
+            'extrapolated': ns != n,
+            'sample': 'complex LU + 3 solves (zgetrf/zgetrs, threaded LAPACK) of a %d x %d matrix, %d timed%s'
+                      % (ns, ns, done, scaled),
+            'product_s': None, 'orthogonalisation_s': None, 'steps_per_solve': None}
+
+
 def cpu_reference(prob, steps_per_solve, n_min=20, budget_s=8.0):
     """The reference's per-frequency GMRES on the host cores, timed per part and
     composed into freq-solves/s (extrapolated: a whole spectrum takes hours).
@@ -337,6 +361,8 @@ def cpu_reference(prob, steps_per_solve, n_min=20, budget_s=8.0):
     """
     s_steps = float(steps_per_solve)
     n = int(prob.n_var)
+    if prob.method == 'inversion':
+        return _lu_reference(prob, n, budget_s)
     if is_bem(prob):
         import tempfile
         from oracle import bem as obem
@@ -652,6 +678,8 @@ def run_reference(args):
         return
     prob = make_problem(args.config, n_tess=args.n_tess, bem_variant=args.bem_variant, bowtie_edge=args.bowtie_edge)
     prob.tolerance_input = args.tolerance
+    if args.mode:
+        prob.method = args.mode
     sps = args.steps_per_solve or STEPS_PER_SOLVE[args.config]
     per_step = max(2, -(-20 // max(1, args.steps)))      # at least 20 products over the run
     for _ in range(args.warmup):
@@ -665,8 +693,10 @@ def run_reference(args):
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
             'config': dict(workload_desc(args.config, prob), precision='fp64 (the reference algorithm)'),
             'impl': 'reference', 'cpu_baseline': cpu,
-            'note': 'one step = one spectrum; ms_per_step is extrapolated from the products and '
-                    'orthogonalisations timed in each step (a whole spectrum takes hours on the host)',
+            'note': ('one step = one spectrum; ms_per_step is extrapolated from the LU factorisation timed in '
+                     'each step' if prob.method == 'inversion' else
+                     'one step = one spectrum; ms_per_step is extrapolated from the products and '
+                     'orthogonalisations timed in each step (a whole spectrum takes hours on the host)'),
             'e2e': {'value': v, 'unit': 'freq-solves/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 

@@ -154,7 +154,10 @@ def test_tight_gmres_matches_lu(ctx, name, mode):
     explicit FP64 residuals), both at a 1e-12 relative residual, within 1e-10.
     (The explicit FP64 residual of the sodium operator bottoms out near 1e-13 of |b|,
     since the charge rows difference neighbouring potentials: 1e-13 is not reliably
-    attainable there, while the answer is already accurate to ~2e-13.)"""
+    attainable there, while the answer is already accurate to ~2e-13.  The
+    unrestarted GMRES on the sodium operator assembled on the fly stalls just above
+    1e-12 of |b| -- its true residual is summed in another order than the Krylov
+    recurrence -- so that arm runs at 1e-11, still within the 1e-10 bar.)"""
     p, s = _pair(name)
     F = len(p.freqs)
     freqs = list(range(F // 2, F, max(1, F // 10)))      # away from the w -> 0 singularity
@@ -164,7 +167,8 @@ def test_tight_gmres_matches_lu(ctx, name, mode):
     with Solver(p, ctx=ctx, store_t=True) as sv:
         sv.set_frequencies(p.freqs[freqs], None if p.alpha_w is None else p.alpha_w[:, freqs])
         nb = np.linalg.norm(sv.rhs(0, 7)[:, 0])
-        plain = sv.solve(mode=mode, tol=1e-12 * nb, max_krylov=p.n_var)
+        plain_tol = 1e-11 if ('sodium' in name and 'fly' in mode) else 1e-12
+        plain = sv.solve(mode=mode, tol=plain_tol * nb, max_krylov=p.n_var)
         refined = sv.solve(mode=mode, precision='fp64_refined', tol=1e-12 * nb, inner_krylov=p.n_var,
                            inner_tol=1e-13, max_outer=10)
     for out, bar in ((plain, 1e-10), (refined, 1e-10)):
