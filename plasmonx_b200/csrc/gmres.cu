@@ -135,6 +135,64 @@ __global__ void __launch_bounds__(kThreads) dots_partial(int n, int i0, int i1,
     }
 }
 
+// The same partial dots for projections onto eight or more basis vectors
+// (classical Gram-Schmidt): the chunk of W is staged in shared memory once and
+// each warp takes whole basis vectors, 32 rows per lane with the loads of 16
+// rows in flight, so one warp reduction serves 1,024 rows of a vector (the
+// kernel above pays one per 128 rows and keeps only 8 loads in flight a warp).
+// Same chunking and partial layout as dots_partial.
+template <typename VT>
+__global__ void __launch_bounds__(kThreads) dots_wide(int n, int i0, int i1,
+                                                      const int32_t *__restrict__ act,
+                                                      VT *const *__restrict__ slabs,
+                                                      const double *__restrict__ W,
+                                                      double2 *__restrict__ part) {
+    __shared__ double wsh[2][kDotRows];
+    const int k = blockIdx.y, c = act[k];
+    const int r0 = blockIdx.x * kDotRows;
+    const int rn = min(kDotRows, n - r0);
+    const double *wr = W + (int64_t)k * 2 * n;
+    for (int t = threadIdx.x; t < kDotRows; t += kThreads) {
+        wsh[0][t] = t < rn ? wr[r0 + t] : 0.0;
+        wsh[1][t] = t < rn ? wr[n + r0 + t] : 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ni = i1 - i0;
+    for (int ii = warp; ii < ni; ii += kThreads / 32) {
+        const VT *v = slabs[i0 + ii] + (int64_t)c * 2 * n + r0;
+        double re = 0.0, im = 0.0;
+        constexpr int kBatch = 16;
+        for (int q0 = 0; q0 < kDotRows / 32; q0 += kBatch) {
+            VT vr[kBatch], vi[kBatch];
+            if (rn == kDotRows) {
+#pragma unroll
+                for (int q = 0; q < kBatch; ++q) {
+                    vr[q] = v[lane + 32 * (q0 + q)];
+                    vi[q] = v[n + lane + 32 * (q0 + q)];
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < kBatch; ++q) {
+                    const int t = lane + 32 * (q0 + q);
+                    vr[q] = t < rn ? v[t] : VT(0);
+                    vi[q] = t < rn ? v[n + t] : VT(0);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const int t = lane + 32 * (q0 + q);
+                const double a = wsh[0][t], b = wsh[1][t];          // zero beyond rn
+                re += (double)vr[q] * a + (double)vi[q] * b;        // conj(v) * w
+                im += (double)vr[q] * b - (double)vi[q] * a;
+            }
+        }
+        re = warp_sum(re);
+        im = warp_sum(im);
+        if (lane == 0) part[((int64_t)k * gridDim.x + blockIdx.x) * ni + ii] = make_double2(re, im);
+    }
+}
+
 // Sums the chunk partials: h[k][ii] = sum_b part[k][b][ii]; optionally accumulates
 // into H column j (Hcol[c][i0+ii] += h) when Hslab != nullptr.
 __global__ void dots_finish(int nchunk, int ni, int i0, const int32_t *__restrict__ act,
@@ -169,15 +227,35 @@ __global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int h
                                                     VT *const *__restrict__ slabs,
                                                     const double2 *__restrict__ h, double sign,
                                                     double *__restrict__ Y, int by_col) {
-    extern __shared__ double2 sh[];
+    extern __shared__ double2 sh[];                       // ni coefficients, then ni column pointers
+    const VT **col = reinterpret_cast<const VT **>(sh + ni);
     int k = blockIdx.y, c = act[k];
-    for (int t = threadIdx.x; t < ni; t += blockDim.x) sh[t] = h[(int64_t)k * hld + hoff + t];
+    for (int t = threadIdx.x; t < ni; t += blockDim.x) {
+        sh[t] = h[(int64_t)k * hld + hoff + t];
+        col[t] = slabs[i0 + t] + (int64_t)c * 2 * n;
+    }
     __syncthreads();
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     double ar = 0.0, ai = 0.0;
-    for (int ii = 0; ii < ni; ++ii) {
-        const VT *v = slabs[i0 + ii] + (int64_t)c * 2 * n;
+    constexpr int kBatch = 8;        // loads of 8 basis vectors in flight per thread
+    int ii = 0;
+    for (; ii + kBatch <= ni; ii += kBatch) {
+        VT vr[kBatch], vi[kBatch];
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+            vr[q] = col[ii + q][r];
+            vi[q] = col[ii + q][n + r];
+        }
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+            const double2 hh = sh[ii + q];
+            ar += (double)vr[q] * hh.x - (double)vi[q] * hh.y;
+            ai += (double)vr[q] * hh.y + (double)vi[q] * hh.x;
+        }
+    }
+    for (; ii < ni; ++ii) {
+        const VT *v = col[ii];
         double vr = (double)v[r], vi = (double)v[n + r];
         double2 hh = sh[ii];
         ar += vr * hh.x - vi * hh.y;
@@ -372,7 +450,7 @@ int64_t combine_chunked(cudaStream_t st, int n, int i0, int ni, int count, const
     for (int c0 = 0; c0 < ni; c0 += kCombine) {
         int cn = std::min(kCombine, ni - c0);
         // h is [count][ni]; pass the row stride through a shifted view per chunk
-        combine<VT><<<dim3(n_blocks(n, kThreads), count), kThreads, cn * sizeof(double2), st>>>(
+        combine<VT><<<dim3(n_blocks(n, kThreads), count), kThreads, cn * (sizeof(double2) + sizeof(VT *)), st>>>(
             n, i0 + c0, cn, ni, c0, act, slabs, h, sign, Y, by_col);
         ++launches;
     }
@@ -508,7 +586,11 @@ class GmresRun final : public GmresStepper {
         if (part_.n < need) part_.alloc(ctx_, std::max(need, part_.n * 2));
         auto project = [&](int i0, int i1, int accumulate) {
             int ni = i1 - i0;
-            dots_partial<VT><<<dim3(ndot_, na), kThreads, 0, st_>>>(n, i0, i1, d_act_.p, d_slabs_.p, Wa_.p, part_.p);
+            if (ni >= 8)
+                dots_wide<VT><<<dim3(ndot_, na), kThreads, 0, st_>>>(n, i0, i1, d_act_.p, d_slabs_.p, Wa_.p, part_.p);
+            else
+                dots_partial<VT><<<dim3(ndot_, na), kThreads, 0, st_>>>(n, i0, i1, d_act_.p, d_slabs_.p, Wa_.p,
+                                                                        part_.p);
             dots_finish<<<dim3(n_blocks(ni, 128), na), 128, 0, st_>>>(ndot_, ni, i0, d_act_.p, part_.p, hbuf_.p,
                                                                        hcols_[j].p, hstride_, accumulate);
             ctx_->launches += 2 + combine_chunked(st_, n, i0, ni, na, d_act_.p, d_slabs_.p, hbuf_.p, -1.0, Wa_.p, 0);

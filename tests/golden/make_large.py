@@ -2,11 +2,10 @@
 
     python tests/golden/make_large.py [case ...] [--threads N]
 
-Solves, on the CPU, five frequencies of two benchmark systems with the
-oracle's restatement of the reference GMRES (``oracle/gmres.py``,
-``src/solvers/gmres_module.f90:30-228``) whose products are the C port of the
-reference's on-the-fly matrix-vector product (``oracle/pairs.c``,
-``src/matrix/matrix_module.f90:727-1125`` plus ``new_gmres_diagonal_shift``):
+Solves, on the CPU, five frequencies of two benchmark systems with products
+from the C port of the reference's on-the-fly matrix-vector product
+(``oracle/pairs.c``, ``src/matrix/matrix_module.f90:727-1125`` plus
+``new_gmres_diagonal_shift``):
 
   ag_sphere_r35    wFQFMu silver sphere, fcc a = 4.086 A, R = 35 A:
                    10,473 atoms, 41,892 unknowns, 201 frequencies 3.0-4.5 eV
@@ -14,16 +13,21 @@ reference's on-the-fly matrix-vector product (``oracle/pairs.c``,
                    80 A and thickness 20 A, gap 10 A: 5,850 atoms, 23,400
                    unknowns, 201 frequencies 2.0-4.5 eV
 
-at frequency indices 0, 50, 100, 150 and 200, x polarisation, to an absolute
-tolerance of 1e-12 ||b|| (the reference's test is absolute; the level is
-chosen far below the 1e-10 parity bar).  The geometry is the seeded generator
-the benchmark uses (``plasmonx_b200.configs``); it reaches the oracle through
-the keyword file, as every other oracle fixture does.  For each frequency the
-fixture stores the 20 results of the reference's results row
-(``target_module.f90:1989-2054``), alpha_xx, the Arnoldi step count, the true
-relative residual of the solution, and the x-polarised sigma_abs of the
-iterates whose logged residual first fell below 1e-8 ||b|| and 1e-10 ||b||,
-which bound how far the stored value can still move.
+at frequency indices 0, 50, 100, 150 and 200, x polarisation.  The reference
+GMRES alone (unrestarted, ``oracle/gmres.py``) does not reach a relative
+residual of 1e-12 within 4,000 Krylov vectors on these systems, so the solution
+is refined in FP64: x = 0, r = b; repeat { solve A d = r with the reference
+GMRES to 1e-5 ||r|| (at most 1,500 vectors); x += d; r = b - A x by the FP64
+product } until ||r|| <= 1e-12 ||b|| or the residual stops falling.  Every
+residual is an explicit product of the C port, so the fixture is the solution
+of the same FP64 system the reference assembles, to the attained residual,
+which is stored with the sigma_abs of every refinement pass (the change
+between the last two passes bounds how far the stored value can still move).
+The geometry is the seeded generator the benchmark uses
+(``plasmonx_b200.configs``); it reaches the oracle through the keyword file,
+as every other oracle fixture does.  For each frequency the fixture stores the
+20 results of the reference's results row (``target_module.f90:1989-2054``),
+alpha_xx, the Krylov vectors used, and the refinement history.
 
 Output: ``tests/golden/large/<case>.json``, written after every frequency.
 Run time on 8 cores: about 1.5 s per product for the sphere, 0.5 s for the
@@ -48,8 +52,10 @@ from oracle.gmres import gmres  # noqa: E402
 from plasmonx_b200 import configs  # noqa: E402
 
 FREQ_INDEX = [0, 50, 100, 150, 200]
-REL_TOL = 1e-12
-SNAP = (1e-8, 1e-10)
+REL_TOL = 1e-12          # target relative residual of the refinement
+INNER_REL = 1e-5         # inner GMRES: relative to the current residual
+INNER_DIM = 1500
+MAX_OUTER = 8
 
 
 def build(case):
@@ -70,6 +76,41 @@ def signature(s):
             'coord_abs_sum': float(np.sum(np.abs(s.coord)))}
 
 
+def refine(matvec, b, log=None):
+    """FP64 iterative refinement around the reference GMRES (module docstring).
+
+    Returns (x, its relative residual, history): per pass the Krylov vectors
+    used and the relative residual ||b - A x|| / ||b|| after it."""
+    nb = float(np.linalg.norm(b))
+    x = np.zeros_like(b)
+    r = b.copy()
+    hist = []
+    best = (np.inf, x)
+    for _ in range(MAX_OUTER):
+        nr = float(np.linalg.norm(r))
+        d, steps = gmres(matvec, r, INNER_REL * nr, INNER_DIM, best_effort=True)
+        x_new = x + d
+        r_new = b - matvec(x_new)
+        rel = float(np.linalg.norm(r_new)) / nb
+        hist.append({'krylov': int(steps), 'rel_residual': rel})
+        if log is not None:
+            log(hist[-1], x_new)
+        if rel >= best[0]:
+            break                       # the residual stopped falling: keep the best pass
+        x, r = x_new, r_new
+        best = (rel, x)
+        if rel <= REL_TOL:
+            break
+    return best[1], best[0], hist
+
+
+def _sigma(s, x, i):
+    X = np.zeros((s.n_var, 3), dtype=np.complex128)
+    X[:, 0] = x
+    P = model.polar(s, X)
+    return P, model.results_row(P, s.freqs[i])
+
+
 def run(case, threads):
     text, s = build(case)
     out_dir = os.path.join(HERE, 'large')
@@ -79,34 +120,31 @@ def run(case, threads):
     K = model.k_matrix(s)
     Kbar = K - np.diag(K.sum(axis=1))
     rec = {'case': case, 'geometry': signature(s), 'freq_index': [], 'omega': [], 'results': [],
-           'alpha_xx': [], 'steps': [], 'true_rel_residual': [], 'rel_tol': REL_TOL,
-           'sigma_abs_snapshots': {('%g' % lv): [] for lv in SNAP}, 'seconds': [], 'threads': op.n_threads}
+           'alpha_xx': [], 'krylov_total': [], 'true_rel_residual': [], 'rel_tol': REL_TOL,
+           'method': 'FP64 refinement around the reference GMRES (inner 1e-5, explicit FP64 residuals)',
+           'refinement': [], 'seconds': [], 'threads': op.n_threads}
     for i in FREQ_INDEX:
         t0 = time.time()
         b = model.rhs(s, i, Kbar=Kbar, K=K)[:, 0]
-        nb = float(np.linalg.norm(b))
-        snaps = {lv * nb: None for lv in SNAP}
-        x, steps = gmres(lambda v: op.matvec(i, v), b, REL_TOL * nb, 4000, snapshots=snaps)
-        res = float(np.linalg.norm(b - op.matvec(i, x)) / nb)
-        X = np.zeros((s.n_var, 3), dtype=np.complex128)
-        X[:, 0] = x
-        P = model.polar(s, X)
-        row = model.results_row(P, s.freqs[i])
-        for lv, xs in zip(SNAP, snaps.values()):
-            Xs = np.zeros_like(X)
-            Xs[:, 0] = xs
-            rec['sigma_abs_snapshots']['%g' % lv].append(float(model.results_row(model.polar(s, Xs), s.freqs[i])[9]))
+
+        def log(h, xp):
+            h['sigma_abs'] = float(_sigma(s, xp, i)[1][9])
+            print('  %s freq %d pass: %d vectors, residual %.2e, sigma_abs %.12e (%.0f s)' %
+                  (case, i, h['krylov'], h['rel_residual'], h['sigma_abs'], time.time() - t0), flush=True)
+        x, res, hist = refine(lambda v: op.matvec(i, v), b, log)
+        P, row = _sigma(s, x, i)
         rec['freq_index'].append(i)
         rec['omega'].append(float(s.freqs[i]))
         rec['results'].append([float(v) for v in row])
         rec['alpha_xx'].append([float(P[0, 0].real), float(P[0, 0].imag)])
-        rec['steps'].append(int(steps))
+        rec['krylov_total'].append(int(sum(h['krylov'] for h in hist)))
         rec['true_rel_residual'].append(res)
+        rec['refinement'].append(hist)
         rec['seconds'].append(round(time.time() - t0, 1))
         with open(path, 'w') as f:
             json.dump(rec, f, indent=1)
-        print('%s freq %d: %d steps, residual %.2e, sigma_abs %.12e, %.0f s' %
-              (case, i, steps, res, row[9], time.time() - t0), flush=True)
+        print('%s freq %d: residual %.2e, sigma_abs %.12e, %.0f s' % (case, i, res, row[9], time.time() - t0),
+              flush=True)
 
 
 if __name__ == '__main__':
