@@ -716,7 +716,7 @@ def run_serving(args):
     with Server(device=0, workers=args.serving_workers) as srv:
         run_mix(srv, request_pool(n_requests=4, rate=args.serving_rate, seed=99, scale='small'))
     arms, results = {}, {}
-    for prec in ('mixed_bf16x3', 'fp64'):
+    for prec in (('mixed_bf16x3', 'fp64') if args.serving_arms == 'both' else ('mixed_bf16x3',)):
         pool = request_pool(n_requests=n, rate=args.serving_rate, seed=7, scale=args.serving_scale, precision=prec)
         with Clocks(0) as clk:
             with Server(device=0, workers=args.serving_workers) as srv:
@@ -728,10 +728,13 @@ def run_serving(args):
                    'mean_requests_per_step': float(np.mean([s[2] for s in steps])) if steps else 0.0,
                    'mean_requests_sharing': float(np.mean([r.batch_size for r in pool])),
                    'modes': sorted({str(r.mode) for r in pool})})
+        # a request counts as solved when every one of its frequencies converged
+        ok = [r.result is not None and bool(np.all(r.result['status'] == 0)) for r in pool]
+        st['unconverged'] = int(sum(1 for r, g in zip(pool, ok) if r.result is not None and not g))
         arms[prec] = st
-        results[prec] = [None if r.result is None else r.result['results'][:, 9] for r in pool]
+        results[prec] = [r.result['results'][:, 9] if g else None for r, g in zip(pool, ok)]
     errs = [float(np.max(np.abs(a - b) / np.abs(b))) for a, b in zip(results['mixed_bf16x3'], results['fp64'])
-            if a is not None and b is not None]
+            if a is not None and b is not None] if 'fp64' in results else []
     mixed = arms['mixed_bf16x3']
     line = {'metric': SERVING_METRIC, 'value': mixed['throughput'], 'unit': 'freq-solves/s', 'n_gpus': 1,
             'steps': 1, 'warmup': 1, 'ms_per_step': mixed['wall_s'] * 1000.0, 'higher_is_better': True,
@@ -741,9 +744,12 @@ def run_serving(args):
                                                                                      args.serving_scale),
                        'workers': args.serving_workers},
             'p50_ms': mixed['p50_ms'], 'p99_ms': mixed['p99_ms'],
-            'fp64_plain': arms['fp64'], 'mixed': mixed,
-            'speedup_vs_fp64_plain': mixed['throughput'] / arms['fp64']['throughput'],
-            'sigma_abs_max_rel_err_vs_fp64_plain': max(errs) if errs else None}
+            'fp64_plain': arms.get('fp64', 'not run (--serving-arms mixed): the unrestarted FP64 GMRES of '
+                                           'the 30k-atom requests takes hours per request'),
+            'mixed': mixed,
+            'speedup_vs_fp64_plain': mixed['throughput'] / arms['fp64']['throughput'] if 'fp64' in arms else None,
+            'sigma_abs_max_rel_err_vs_fp64_plain': max(errs) if errs else None,
+            'requests_compared': len(errs)}
     print(json.dumps(line), flush=True)
 
 
@@ -781,6 +787,8 @@ def main():
     ap.add_argument('--radius', type=float, default=None, help='sphere radius in A: a smaller ag_sphere (profiling runs only), or the field_grid sphere (default 20)')
     ap.add_argument('--n-freq', type=int, default=None, help='fewer frequencies (profiling runs only)')
     ap.add_argument('--serving-requests', type=int, default=24, help='requests in the serving leg (0: skip)')
+    ap.add_argument('--serving-arms', default='both', choices=['both', 'mixed'],
+                    help='config serving: run the plain FP64 arm too (both) or the mixed arm alone')
     ap.add_argument('--serving-rate', type=float, default=20.0, help='Poisson arrival rate, requests/s')
     ap.add_argument('--serving-scale', default='small', choices=['small', 'medium', 'full'])
     ap.add_argument('--serving-workers', type=int, default=2)
@@ -879,6 +887,10 @@ def main():
             # FP64 Krylov basis for all frequencies would not fit); throughput per frequency
             sub = np.linspace(0, F - 1, args.fp64_freqs).round().astype(int)
             solver.set_frequencies(prob.freqs[sub], None if prob.alpha_w is None else prob.alpha_w[:, sub])
+        if not args.fp64_krylov and args.config == 'bowtie':
+            # the gap-coupled alloy needs up to ~1,500 Arnoldi steps at this tolerance;
+            # the input's dimension (1,000) leaves frequencies unconverged
+            args.fp64_krylov = 2500
         o64 = solver.solve(precision='fp64', max_krylov=args.fp64_krylov or None)
         if sub is not None:
             solver.set_frequencies(prob.freqs, prob.alpha_w)

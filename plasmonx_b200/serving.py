@@ -228,7 +228,7 @@ class Server:
         p = req.problem
         modes = ['iterative'] if _is_bem(p) else ['iterative', 'iterative on the fly']
         for mode in modes:
-            geo, batch = footprint(p, mode, req.precision, self._cols(req))
+            geo, batch = footprint(p, mode, req.precision, self._block_cols(p, mode, req.precision, self._cols(req)))
             short = self.committed + geo + batch - self.budget
             if short > 0 and short > self.freeing:
                 self._evict(short - self.freeing)
@@ -240,7 +240,8 @@ class Server:
                 return w
             if self.committed + geo + batch <= self.budget + self.freeing:
                 return None          # room is being freed: wait for it
-        geo, batch = footprint(p, modes[-1], req.precision, self._cols(req))
+        geo, batch = footprint(p, modes[-1], req.precision,
+                               self._block_cols(p, modes[-1], req.precision, self._cols(req)))
         if geo + batch > self.budget:
             return 'reject'          # would not fit even on an empty device
         return None
@@ -261,6 +262,18 @@ class Server:
     @staticmethod
     def _cols(req):
         return req.n_freq * bin(req.pol_mask).count('1')
+
+    def _block_cols(self, problem, mode, precision, cols):
+        """Columns a batch holds on the device at once.  The mixed form keeps a
+        short inner basis, so a whole batch runs as one block; the plain FP64 GMRES
+        keeps its unrestarted basis (up to the GMRES dimension) per column, so a
+        batch whose basis would pass a quarter of the budget runs in frequency blocks
+        of that size, one after the other (the reference solves one frequency at a
+        time)."""
+        if precision.startswith('mixed'):
+            return cols
+        per_col = footprint(problem, mode, precision, 1)[1]
+        return max(1, min(cols, int(self.budget // (4 * per_col))))
 
     # ---- workers --------------------------------------------------------------
     def _free_evicted(self, w):
@@ -452,8 +465,9 @@ class Server:
             self.busy[w] = True
             res = self.resident[w].get(batch[0].key)
             mode = res.mode if res is not None else (batch[0].mode or 'iterative')
+            cols = sum(self._cols(r) for r in batch)
             _, batch_bytes = footprint(batch[0].problem, mode, batch[0].precision,
-                                       sum(self._cols(r) for r in batch))
+                                       self._block_cols(batch[0].problem, mode, batch[0].precision, cols))
             self.committed += batch_bytes
             if res is not None:
                 res.busy = True
@@ -485,7 +499,11 @@ class Server:
             aw = [r.problem.alpha_w for r in batch]
             alpha_w = None if aw[0] is None else np.concatenate([np.asarray(a) for a in aw], axis=1)
             res.solver.set_frequencies(freqs, alpha_w)
-            out = res.solver.solve(mode=res.mode, precision=head.precision, pol_mask=head.pol_mask, tol=head.tol)
+            pols = bin(head.pol_mask).count('1')
+            cols = len(freqs) * pols
+            blk = self._block_cols(head.problem, res.mode, head.precision, cols)
+            out = res.solver.solve(mode=res.mode, precision=head.precision, pol_mask=head.pol_mask, tol=head.tol,
+                                   freq_block=0 if blk >= cols else max(1, blk // pols))
             if 'error' in out:
                 raise out['error']
             off = 0
@@ -524,7 +542,9 @@ def run_mix(server, requests, time_scale=1.0):
     return {'requests': len(requests), 'p50_ms': float(np.percentile(lat, 50)),
             'p99_ms': float(np.percentile(lat, 99)), 'mean_ms': float(lat.mean()),
             'throughput': solves / (t1 - t0), 'unit': 'freq-solves/s', 'wall_s': t1 - t0,
-            'batches': len(server.batches), 'errors': sum(r.error is not None for r in requests)}
+            'batches': len(server.batches), 'errors': sum(r.error is not None for r in requests),
+            'error_kinds': dict(collections.Counter('%s: %s' % (type(r.error).__name__, str(r.error)[:80])
+                                                    for r in requests if r.error is not None))}
 
 
 def poisson_arrivals(n, rate, seed):

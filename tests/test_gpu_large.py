@@ -11,7 +11,9 @@ loops, refined in FP64 with explicit residuals to a relative residual near
 
 The device solves the same frequencies, x polarisation:
   * plain FP64 GMRES (the drop-in: unrestarted, the reference's algorithm) at
-    1e-10 of ||b||: sigma_abs within PLAIN_BAR (relative) of the oracle;
+    5e-11 of ||b||: sigma_abs within 1e-10 (relative) of the oracle (at 1e-10
+    of ||b|| one sphere frequency lands at 1.06e-10; at 1e-11 the unrestarted
+    recurrence stalls on four of the five before its true residual gets there);
   * the FP64 refinement (restarted FP64 GMRES, explicit FP64 residuals) at
     1e-11 of ||b||: within 1e-10;
   * mixed BF16x3 tensor-core refinement at the workload's own tolerance
@@ -63,7 +65,7 @@ def ctx():
     c.close()
 
 
-PLAIN_REL = 1e-10
+PLAIN_REL = 5e-11
 PLAIN_BAR = 1e-10
 
 

@@ -34,14 +34,14 @@ class FakeSolver:
     def set_frequencies(self, freqs, alpha_w=None):
         self.freqs = np.asarray(freqs)
 
-    def solve(self, mode=None, precision=None, pol_mask=None, tol=None):
+    def solve(self, mode=None, precision=None, pol_mask=None, tol=None, freq_block=0):
         t0 = time.perf_counter()
         time.sleep(self.delay)
         F = len(self.freqs)
         res = np.zeros((F, 20))
         res[:, 0] = self.freqs
         with FakeSolver.lock:
-            FakeSolver.log.append(('solve', id(self.problem), mode, F, t0, time.perf_counter()))
+            FakeSolver.log.append(('solve', id(self.problem), mode, F, t0, time.perf_counter(), freq_block))
         return {'results': res, 'polar': np.zeros((F, 3, 3), complex), 'status': np.zeros(F, np.int32),
                 'steps': np.zeros((F, 3), np.int32)}
 
@@ -213,3 +213,20 @@ def test_mix_statistics_and_pool_is_seeded():
         st = run_mix(srv, pool1)
     assert st['requests'] == 6 and st['errors'] == 0
     assert st['p50_ms'] <= st['p99_ms'] and st['throughput'] > 0
+
+
+def test_plain_fp64_batch_runs_in_blocks_that_fit():
+    """An unrestarted FP64 basis for every frequency would not fit: the plain arm
+    solves the batch in frequency blocks of at most a quarter of the budget."""
+    p = _na(nf=20)
+    p.geometry_key = 'na64-blocks'
+    geo, per_col = footprint(p, 'iterative', 'fp64', 1)
+    budget = geo + 4 * 5 * per_col                    # room for blocks of about 5 columns
+    block = budget // (4 * per_col)
+    with _server(budget, workers=1) as srv:
+        r = ServeRequest(0, p, precision='fp64', pol_mask=1, tol=1.0)
+        srv.submit(r)
+        assert r.done.wait(5) and r.error is None, r.error
+    solves = [e for e in FakeSolver.log if e[0] == 'solve' and e[1] == id(p)]
+    assert len(solves) == 1 and solves[0][6] == block < r.n_freq
+    assert r.result['results'].shape[0] == r.n_freq
