@@ -273,8 +273,7 @@ plx_status plx_contract(plx_geom *geom, int32_t count, const double *X, double *
  * GPU that loads the library, held until exit); 1 <= count <= 16 and the
  * split-K partials (k-chunks x count x n_var) must fit in it, otherwise the
  * call returns PLX_ERR_ARG.  The first call on a device looks up the array's
- * device address, so make that first call before any stream capture.  All
- * calls share the array: calls whose kernels overlap on the GPU race.  The
+ * device address.  All calls share the array: calls whose kernels overlap on the GPU race.  The
  * kernels run on the context's own stream, which is not ordered after the
  * caller's streams: d_X must be completely written on the device before the
  * call (synchronise the stream that wrote it).  The call synchronises the
