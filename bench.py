@@ -722,7 +722,9 @@ def run_serving(args):
             with Server(device=0, workers=args.serving_workers) as srv:
                 st = run_mix(srv, pool)
         steps = srv.steps
-        st.update({'clocks': clk.summary(), 'outer_steps': len(steps),
+        st.update({'clocks': clk.summary(), 'outer_steps': len(steps), 'budget_bytes': srv.budget,
+                   'min_device_free_bytes': None if srv.min_free is None else srv.min_free[0],
+                   'committed_at_min_free': None if srv.min_free is None else srv.min_free[1],
                    'grouped_steps': sum(1 for s in steps if s[1] > 1),
                    'max_geometries_per_step': max([s[1] for s in steps] or [0]),
                    'mean_requests_per_step': float(np.mean([s[2] for s in steps])) if steps else 0.0,

@@ -375,7 +375,9 @@ typedef struct {
                                    that does not apply; 1 LU of the full system (the
                                    reference's form); 2 as 0 with the Cholesky factor in
                                    single precision and double-precision iterative
-                                   refinement (LAPACK dsposv's algorithm) */
+                                   refinement (LAPACK dsposv's algorithm); 3 as 0 with
+                                   the reduced system factored by the library's own
+                                   blocked Cholesky kernels instead of cuSOLVER's */
 } plx_static_desc;
 
 /* n_var of a static problem, or -1 for an invalid description. */

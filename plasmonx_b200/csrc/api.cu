@@ -20,6 +20,16 @@ void *plx::dev_alloc(plx_ctx *ctx, size_t bytes) {
                                         " of " + std::to_string(ctx->budget) + " in use)");
     void *p = nullptr;
     cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+    if (e == cudaErrorMemoryAllocation) {
+        // the stream-ordered pool keeps freed blocks (release threshold: never), so
+        // blocks of other sizes can hold the memory a new size needs: wait for this
+        // stream's frees, hand every unused block back to the device, retry once
+        cudaGetLastError();
+        cudaStreamSynchronize(ctx->stream);
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocAsync(&p, bytes, ctx->stream);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         throw Error(PLX_ERR_NOMEM, "cudaMallocAsync(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
@@ -156,6 +166,10 @@ void plx_ctx_destroy(plx_ctx *ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    // the pool keeps freed blocks for reuse; a closed context's blocks go back to
+    // the device, so that what it held is free for other contexts and processes
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     delete ctx;
 }
 

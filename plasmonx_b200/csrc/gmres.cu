@@ -221,6 +221,14 @@ __global__ void dots_finish(int nchunk, int ni, int i0, const int32_t *__restric
 
 // W[k] -= sum_{ii} V_{i0+ii}[c] h[k][ii]   (sign = -1), or X[c] += ... (sign = +1,
 // target indexed by column instead of compact position when by_col != 0).
+// Each thread owns kCombineRows rows (strided by the block), so that a block
+// streams kCombineRows x 256 contiguous rows of every basis vector; the loads of
+// a batch of basis vectors are issued before their products are summed (the
+// per-row sum runs over ii in ascending order whatever the batching).
+#ifndef PLX_COMBINE_ROWS
+#define PLX_COMBINE_ROWS 1
+#endif
+constexpr int kCombineRows = PLX_COMBINE_ROWS;
 template <typename VT>
 __global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int hld, int hoff,
                                                     const int32_t *__restrict__ act,
@@ -235,35 +243,58 @@ __global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int h
         col[t] = slabs[i0 + t] + (int64_t)c * 2 * n;
     }
     __syncthreads();
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    double ar = 0.0, ai = 0.0;
-    constexpr int kBatch = 8;        // loads of 8 basis vectors in flight per thread
+    constexpr int RW = kCombineRows;
+    const int rbase = blockIdx.x * (kThreads * RW) + threadIdx.x;
+    if (rbase >= n) return;
+    int rr[RW];
+    bool in[RW];
+#pragma unroll
+    for (int u = 0; u < RW; ++u) {
+        rr[u] = rbase + kThreads * u;
+        in[u] = rr[u] < n;
+        if (!in[u]) rr[u] = rbase;          // a valid row; its sum is not stored
+    }
+    double ar[RW], ai[RW];
+#pragma unroll
+    for (int u = 0; u < RW; ++u) ar[u] = ai[u] = 0.0;
+    constexpr int kBatch = RW == 1 ? 8 : 4;   // basis vectors whose loads are in flight together
     int ii = 0;
     for (; ii + kBatch <= ni; ii += kBatch) {
-        VT vr[kBatch], vi[kBatch];
+        VT vr[kBatch][RW], vi[kBatch][RW];
 #pragma unroll
-        for (int q = 0; q < kBatch; ++q) {
-            vr[q] = col[ii + q][r];
-            vi[q] = col[ii + q][n + r];
-        }
+        for (int q = 0; q < kBatch; ++q)
+#pragma unroll
+            for (int u = 0; u < RW; ++u) {
+                vr[q][u] = col[ii + q][rr[u]];
+                vi[q][u] = col[ii + q][n + rr[u]];
+            }
 #pragma unroll
         for (int q = 0; q < kBatch; ++q) {
             const double2 hh = sh[ii + q];
-            ar += (double)vr[q] * hh.x - (double)vi[q] * hh.y;
-            ai += (double)vr[q] * hh.y + (double)vi[q] * hh.x;
+#pragma unroll
+            for (int u = 0; u < RW; ++u) {
+                ar[u] += (double)vr[q][u] * hh.x - (double)vi[q][u] * hh.y;
+                ai[u] += (double)vr[q][u] * hh.y + (double)vi[q][u] * hh.x;
+            }
         }
     }
     for (; ii < ni; ++ii) {
         const VT *v = col[ii];
-        double vr = (double)v[r], vi = (double)v[n + r];
-        double2 hh = sh[ii];
-        ar += vr * hh.x - vi * hh.y;
-        ai += vr * hh.y + vi * hh.x;
+        const double2 hh = sh[ii];
+#pragma unroll
+        for (int u = 0; u < RW; ++u) {
+            const double vr = (double)v[rr[u]], vi = (double)v[n + rr[u]];
+            ar[u] += vr * hh.x - vi * hh.y;
+            ai[u] += vr * hh.y + vi * hh.x;
+        }
     }
     double *y = Y + (int64_t)(by_col ? c : k) * 2 * n;
-    y[r] += sign * ar;
-    y[n + r] += sign * ai;
+#pragma unroll
+    for (int u = 0; u < RW; ++u) {
+        if (!in[u]) continue;
+        y[rr[u]] += sign * ar[u];
+        y[n + rr[u]] += sign * ai[u];
+    }
 }
 
 // ||W[k]||_2 (dznrm2): partial sums of squares per chunk.
@@ -450,7 +481,8 @@ int64_t combine_chunked(cudaStream_t st, int n, int i0, int ni, int count, const
     for (int c0 = 0; c0 < ni; c0 += kCombine) {
         int cn = std::min(kCombine, ni - c0);
         // h is [count][ni]; pass the row stride through a shifted view per chunk
-        combine<VT><<<dim3(n_blocks(n, kThreads), count), kThreads, cn * (sizeof(double2) + sizeof(VT *)), st>>>(
+        combine<VT><<<dim3(n_blocks(n, kThreads * kCombineRows), count), kThreads,
+                      cn * (sizeof(double2) + sizeof(VT *)), st>>>(
             n, i0 + c0, cn, ni, c0, act, slabs, h, sign, Y, by_col);
         ++launches;
     }

@@ -24,7 +24,10 @@
 //     breaks down, or when asked, the full system is factored by pivoted LU
 //     (dgetrf / dgetrs).  On request the reduced system is factored in single
 //     precision and refined in double (mixed_cholesky); measured on B200 it
-//     does not beat the double-precision factor at these sizes;
+//     does not beat the double-precision factor at these sizes.  Also on
+//     request, the reduced system is factored by the hand-written blocked
+//     Cholesky of cholesky.cu (correct, but measured far slower than dpotrf:
+//     96 ms against 5 ms at 6,000 unknowns);
 //   * the ground-state energy -1/2 x.b (calculate_energy_fq, fq_module.f90:358-374)
 //     and the FQ static polarizability
 //     R^T J^-1 R - (L^T J^-1 R)^T (L^T J^-1 L)^-1 (L^T J^-1 R), J the charge
@@ -556,12 +559,35 @@ bool solve_eliminated(plx_ctx *ctx, const StaticDims &s, int what, int mode, int
                                          Rr.p, variables, energy, polar);
     }
     prof_begin(ctx);
-    // hand-written blocked Cholesky (cholesky.cu) in place of dpotrf / dpotrs
-    if (cholesky_factor(ctx, nr, Kr.p) != 0) {
-        prof_end(ctx, kProfStaticFactor, 0.0, 0.0);
-        return false;  // not positive definite: the caller factors the full system
+    if (mode == 3) {
+        // the hand-written blocked Cholesky (cholesky.cu)
+        if (cholesky_factor(ctx, nr, Kr.p) != 0) {
+            prof_end(ctx, kProfStaticFactor, 0.0, 0.0);
+            return false;  // not positive definite: the caller factors the full system
+        }
+        cholesky_solve(ctx, nr, Kr.p, ncols, Br.p);
+    } else {
+        cusolverDnHandle_t h = solver_handle(ctx);
+        DevArray<double> work;
+        DevArray<int32_t> info;
+        int lwork = 0;
+        if (cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, nr, Kr.p, nr, &lwork) != CUSOLVER_STATUS_SUCCESS)
+            throw Error(PLX_ERR_CUDA, "cusolverDnDpotrf_bufferSize failed");
+        work.alloc(ctx, std::max(lwork, 1));
+        info.alloc(ctx, 1);
+        if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, nr, Kr.p, nr, work.p, lwork, info.p) != CUSOLVER_STATUS_SUCCESS)
+            throw Error(PLX_ERR_CUDA, "cusolverDnDpotrf failed");
+        int hinfo = 0;
+        PLX_CHECK_CUDA(cudaMemcpyAsync(&hinfo, info.p, 4, cudaMemcpyDeviceToHost, st));
+        PLX_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (hinfo != 0) {
+            prof_end(ctx, kProfStaticFactor, 0.0, 0.0);
+            return false;  // not positive definite: the caller factors the full system
+        }
+        if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, nr, ncols, Kr.p, nr, Br.p, nr, info.p) != CUSOLVER_STATUS_SUCCESS)
+            throw Error(PLX_ERR_CUDA, "cusolverDnDpotrs failed");
+        check_info(ctx, info, "DPOTRS of the reduced static matrix");
     }
-    cholesky_solve(ctx, nr, Kr.p, ncols, Br.p);
     prof_end(ctx, kProfStaticFactor, dr * dr * dr / 3.0 + 2.0 * dr * dr * ncols, 8.0 * dr * dr);
     return finish_eliminated(ctx, s, N, nr, nrhs, d_keep.p, d_lo, d_hi, K.p, B.p, Bt.p, Br.p, Rr.p, variables,
                              energy, polar);
@@ -638,6 +664,7 @@ void static_solve(plx_ctx *ctx, const plx_static_desc *d, int what, double *vari
     if (d->kernel < PLX_KERNEL_COULOMB || d->kernel > PLX_KERNEL_GAUSSIAN)
         throw Error(PLX_ERR_ARG, "unknown charge kernel");
     if (what != PLX_GROUND_STATE && what != PLX_STATIC_FIELD) throw Error(PLX_ERR_ARG, "unknown static solve");
+    if (d->factorization < 0 || d->factorization > 3) throw Error(PLX_ERR_ARG, "unknown static factorization");
     const bool fmu = d->forcefield == PLX_STATIC_FQFMU;
     if (fmu && (!d->alpha || !d->r_q || !d->r_mu)) throw Error(PLX_ERR_ARG, "FQFMu needs alpha, r_q and r_mu");
     if (d->kernel == PLX_KERNEL_GAUSSIAN && !d->r_q) throw Error(PLX_ERR_ARG, "the Gaussian kernel needs r_q");

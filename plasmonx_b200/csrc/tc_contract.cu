@@ -49,7 +49,10 @@ constexpr int kBK = 32;           // k per stage (64 bytes of BF16: the 64-byte 
 constexpr int kLdAlign = 64;      // k padding of the split operands (zeros)
 constexpr int kUmmaK = 16;        // k per tcgen05.mma (kind::f16)
 constexpr uint32_t kDrainLimit = 1u << 22;  // clean-up waits after an abort (seconds at most)
-constexpr int kPrefetch = 8;      // A tiles requested into L2 this many stages before their loads
+#ifndef PLX_TC_PREFETCH
+#define PLX_TC_PREFETCH 8
+#endif
+constexpr int kPrefetch = PLX_TC_PREFETCH;   // A tiles requested into L2 this many stages before their loads (0: none)
 constexpr int kSmemBudget = 227 * 1024 - 1024 - 256;   // pipeline stages (after alignment and barriers)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -273,7 +276,7 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
             tma_load_2d(&mp[2], &full[s], stage_ptr(s, 2), kx, n0);
             tma_load_2d(&mp[3], &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
-            if (kt + kPrefetch < nk) {
+            if (kPrefetch > 0 && kt + kPrefetch < nk) {
                 tma_prefetch_l2(&mp[0], 0, ay + kPrefetch * kBM);
                 tma_prefetch_l2(&mp[1], 0, ay + kPrefetch * kBM);
             }

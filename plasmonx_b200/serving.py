@@ -152,14 +152,18 @@ class Server:
         self.batches = []            # (worker, request ids, mode, seconds)
         self.threads = []
         self.errors = []
+        self.min_free = None         # (device free bytes, committed bytes) at the fullest step
 
     def _free_bytes(self):
+        free = self._device_free()
+        return 64 << 30 if free is None else int(0.8 * free)
+
+    def _device_free(self):
         try:
             import torch
-            free, _ = torch.cuda.mem_get_info(self.device)
-            return int(0.85 * free)
+            return int(torch.cuda.mem_get_info(self.device)[0])
         except Exception:
-            return 64 << 30
+            return None
 
     # ---- lifecycle ------------------------------------------------------------
     def start(self):
@@ -411,6 +415,9 @@ class Server:
             return
         with self.lock:
             self.steps.append((w, len(live), n_req, time.perf_counter() - t0))
+            free = self._device_free()
+            if free is not None and (self.min_free is None or free < self.min_free[0]):
+                self.min_free = (free, self.committed)
         for ob in live:
             for r in ob['reqs'].values():
                 r.batch_size = max(r.batch_size, n_req)

@@ -29,7 +29,7 @@ from .outputs import fortran_f
 from .solver import Context
 
 
-FACTORIZATION = {'auto': 0, 'lu': 1, 'cholesky_mixed': 2}
+FACTORIZATION = {'auto': 0, 'lu': 1, 'cholesky_mixed': 2, 'cholesky_blocked': 3}
 
 
 def atoms_per_molecule(mol_index):
@@ -79,7 +79,7 @@ class StaticProblem:
         self.what = what
         self.method = method
         if factorization not in FACTORIZATION:
-            raise ValueError("factorization must be 'auto', 'lu' or 'cholesky_mixed'")
+            raise ValueError("factorization must be 'auto', 'lu', 'cholesky_mixed' or 'cholesky_blocked'")
         # 'auto': charge constraints eliminated, the rest factored by a double-precision
         # Cholesky (LU of the full system where that does not apply); 'cholesky_mixed':
         # the same with a single-precision factor refined in double; 'lu': LU of the

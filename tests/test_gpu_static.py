@@ -51,7 +51,7 @@ def _oracle(p):
                       p.rhs_form, p.e0)
 
 
-@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed', 'lu'])
+@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed', 'cholesky_blocked', 'lu'])
 @pytest.mark.parametrize('name', CASES)
 def test_golden_static_matches_oracle_and_log(ctx, name, factorization):
     p = StaticProblem.from_keyword_file(os.path.join(GOLDEN, name, 'input.kw'))
@@ -83,7 +83,7 @@ SYNTH = [(ff, kernel, what, form, e0)
          for what, form, e0 in (('energy', 'field', 0.0), ('static', 'field', 1e-3), ('static', 'potential', 2e-3))]
 
 
-@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed', 'lu'])
+@pytest.mark.parametrize('factorization', ['auto', 'cholesky_mixed', 'cholesky_blocked', 'lu'])
 @pytest.mark.parametrize('ff,kernel,what,form,e0', SYNTH, ids=lambda v: str(v))
 def test_water_clusters_match_oracle(ctx, ff, kernel, what, form, e0, factorization):
     p = water_cluster(40, ff, kernel, what=what, rhs_form=form, e0=e0, seed=7, factorization=factorization)
