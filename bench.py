@@ -733,6 +733,11 @@ def run_serving(args):
         # a request counts as solved when every one of its frequencies converged
         ok = [r.result is not None and bool(np.all(r.result['status'] == 0)) for r in pool]
         st['unconverged'] = int(sum(1 for r, g in zip(pool, ok) if r.result is not None and not g))
+        st['unconverged_requests'] = [
+            {'id': r.id, 'n_var': int(r.problem.n_var), 'n_freq': r.n_freq, 'tol': r.tol,
+             'kind': type(r.problem).__name__ + ('/' + str(getattr(r.problem, 'model', '')) if hasattr(r.problem, 'model') else ''),
+             'mode': str(r.mode), 'statuses': sorted({int(v) for v in np.asarray(r.result['status']).ravel()})}
+            for r, g in zip(pool, ok) if r.result is not None and not g][:20]
         arms[prec] = st
         results[prec] = [r.result['results'][:, 9] if g else None for r, g in zip(pool, ok)]
     errs = [float(np.max(np.abs(a - b) / np.abs(b))) for a, b in zip(results['mixed_bf16x3'], results['fp64'])
@@ -775,7 +780,8 @@ def main():
     ap.add_argument('--no-fp64-compare', action='store_true')
     ap.add_argument('--fp64-freqs', type=int, default=0, help='time the plain FP64 form on this many frequencies')
     ap.add_argument('--fp64-krylov', type=int, default=0, help='Krylov dimension of the plain FP64 arm (0: input)')
-    ap.add_argument('--mode', default=None, choices=[None, 'inversion', 'iterative', 'iterative on the fly'],
+    ap.add_argument('--mode', default=None,
+                    choices=[None, 'inversion', 'iterative', 'iterative on the fly', 'iterative_on_the_fly'],
                     help="solver mode (default: the workload's)")
     ap.add_argument('--inner-krylov', type=int, default=0)
     ap.add_argument('--ref-rel', type=float, default=1e-11)
@@ -795,6 +801,8 @@ def main():
     ap.add_argument('--serving-scale', default='small', choices=['small', 'medium', 'full'])
     ap.add_argument('--serving-workers', type=int, default=2)
     args = ap.parse_args()
+    if args.mode == 'iterative_on_the_fly':
+        args.mode = 'iterative on the fly'      # the same mode, spelt without spaces for shell variables
     if args.impl == 'reference':
         return run_reference(args)
     if args.config in ('fq_water', 'fqfmu_water'):

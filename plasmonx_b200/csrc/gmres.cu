@@ -221,14 +221,12 @@ __global__ void dots_finish(int nchunk, int ni, int i0, const int32_t *__restric
 
 // W[k] -= sum_{ii} V_{i0+ii}[c] h[k][ii]   (sign = -1), or X[c] += ... (sign = +1,
 // target indexed by column instead of compact position when by_col != 0).
-// Each thread owns kCombineRows rows (strided by the block), so that a block
-// streams kCombineRows x 256 contiguous rows of every basis vector; the loads of
-// a batch of basis vectors are issued before their products are summed (the
-// per-row sum runs over ii in ascending order whatever the batching).
-#ifndef PLX_COMBINE_ROWS
-#define PLX_COMBINE_ROWS 1
-#endif
-constexpr int kCombineRows = PLX_COMBINE_ROWS;
+// Each thread owns kCombineRows rows (strided by the block); the loads of a
+// batch of basis vectors are issued before their products are summed (the
+// per-row sum runs over ii in ascending order whatever the batching).  Four
+// rows per thread measured the same as one (0.65 s of orthogonalisation per two
+// spectra of the 41,892-unknown sphere either way), so one it is.
+constexpr int kCombineRows = 1;
 template <typename VT>
 __global__ void __launch_bounds__(kThreads) combine(int n, int i0, int ni, int hld, int hoff,
                                                     const int32_t *__restrict__ act,

@@ -49,10 +49,6 @@ constexpr int kBK = 32;           // k per stage (64 bytes of BF16: the 64-byte 
 constexpr int kLdAlign = 64;      // k padding of the split operands (zeros)
 constexpr int kUmmaK = 16;        // k per tcgen05.mma (kind::f16)
 constexpr uint32_t kDrainLimit = 1u << 22;  // clean-up waits after an abort (seconds at most)
-#ifndef PLX_TC_PREFETCH
-#define PLX_TC_PREFETCH 8
-#endif
-constexpr int kPrefetch = PLX_TC_PREFETCH;   // A tiles requested into L2 this many stages before their loads (0: none)
 constexpr int kSmemBudget = 227 * 1024 - 1024 - 256;   // pipeline stages (after alignment and barriers)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -98,15 +94,6 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *ba
             smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
-}
-
-// Pulls the box of a tensor map at (x, y) into L2 (no shared memory is written,
-// nothing to wait for; boxes beyond the tensor's extent are not fetched).
-__device__ __forceinline__ void tma_prefetch_l2(const CUtensorMap *map, int x, int y) {
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(x), "r"(y)
-                 : "memory");
 }
 
 // UMMA shared-memory descriptor, K-major operand with the 64-byte swizzle:
@@ -253,13 +240,6 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
         // ---------------- TMA producer ----------------
         const CUtensorMap *mp = p.map[gi];
         const uint32_t tx = (uint32_t)(2 * kA + 2 * bn * kBK * 2);
-        // the A tiles come from HBM once each: ask L2 for them kPrefetch stages
-        // before their loads are issued, so that a load waits on L2, not on DRAM
-        const int arow0 = (mtile * ktiles + kt0) * kBM;
-        for (int kt = 0; kt < min(nk, kPrefetch); ++kt) {
-            tma_prefetch_l2(&mp[0], 0, arow0 + kt * kBM);
-            tma_prefetch_l2(&mp[1], 0, arow0 + kt * kBM);
-        }
         for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
             if (kt >= STAGES) {
@@ -276,10 +256,6 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
             tma_load_2d(&mp[2], &full[s], stage_ptr(s, 2), kx, n0);
             tma_load_2d(&mp[3], &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
-            if (kPrefetch > 0 && kt + kPrefetch < nk) {
-                tma_prefetch_l2(&mp[0], 0, ay + kPrefetch * kBM);
-                tma_prefetch_l2(&mp[1], 0, ay + kPrefetch * kBM);
-            }
         }
     } else if (threadIdx.x == 32) {
         // ---------------- MMA issuer ----------------
