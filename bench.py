@@ -733,6 +733,8 @@ def run_serving(args):
         # a request counts as solved when every one of its frequencies converged
         ok = [r.result is not None and bool(np.all(r.result['status'] == 0)) for r in pool]
         st['unconverged'] = int(sum(1 for r, g in zip(pool, ok) if r.result is not None and not g))
+        st['escalated_requests'] = int(sum(1 for r in pool if getattr(r, 'escalated', 0)))
+        st['escalated_freqs'] = int(sum(getattr(r, 'escalated', 0) for r in pool))
         st['unconverged_requests'] = [
             {'id': r.id, 'n_var': int(r.problem.n_var), 'n_freq': r.n_freq, 'tol': r.tol,
              'kind': type(r.problem).__name__ + ('/' + str(getattr(r.problem, 'model', '')) if hasattr(r.problem, 'model') else ''),

@@ -153,6 +153,7 @@ class Server:
         self.threads = []
         self.errors = []
         self.min_free = None         # (device free bytes, committed bytes) at the fullest step
+        self.escalate = True         # unconverged mixed-precision frequencies are solved again in FP64
 
     def _free_bytes(self):
         free = self._device_free()
@@ -429,7 +430,11 @@ class Server:
                 r = ob['reqs'].pop(tag)
                 try:
                     r.result = ob['batch'].take(tag)
-                    self._finish(r)
+                    bad = np.flatnonzero(np.asarray(r.result['status']) != 0)
+                    if bad.size and self.escalate and r.precision.startswith('mixed'):
+                        self._escalate(w, r, bad)
+                    else:
+                        self._finish(r)
                 except Exception as e:
                     self._finish(r, error=e)
         # drained batches close (a request with other settings may be waiting);
@@ -443,6 +448,38 @@ class Server:
                     ob['res'].last_used = time.perf_counter()
                     self._dispatch()
                     self.lock.notify_all()
+
+    def _escalate(self, w, r, bad):
+        """Frequencies of a mixed-precision request that did not converge (the
+        refinement stalls where cond(A(w)) times the tensor-core operator's
+        ~1e-5 error is near one: sodium close to w -> 0) are solved again by the
+        plain FP64 GMRES on the same resident geometry; the request finishes when
+        that follow-up is merged into its result."""
+        import copy
+        p = copy.copy(r.problem)
+        F = len(r.problem.freqs)
+        p.freqs = np.asarray(r.problem.freqs)[bad]
+        for name in ('alpha_w', 'eps'):
+            v = getattr(r.problem, name, None)
+            if v is not None and np.ndim(v) >= 1 and np.shape(v)[-1] == F:
+                setattr(p, name, np.asarray(v)[..., bad])
+        fr = ServeRequest(-1 - r.id, p, arrival=r.arrival, precision='fp64', pol_mask=r.pol_mask, tol=r.tol)
+        fr.key = r.key
+        fr.mode = r.mode
+        fr.worker = w
+        fr.t_submit = time.perf_counter()
+        fr.parent, fr.parent_idx = r, bad
+        r.escalated = int(bad.size)
+        with self.lock:
+            self.queues[w].appendleft(fr)
+            self.lock.notify_all()
+
+    def _merge_followup(self, fr):
+        r, idx = fr.parent, fr.parent_idx
+        if fr.error is None and fr.result is not None:
+            for k in ('results', 'polar', 'status', 'steps'):
+                r.result[k][idx] = fr.result[k]
+        self._finish(r, error=fr.error)
 
     def _finish(self, r, error=None):
         r.error = error if error is not None else r.error
@@ -529,6 +566,8 @@ class Server:
         for r in batch:
             r.t_done = t1
             r.done.set()
+            if getattr(r, 'parent', None) is not None:
+                self._merge_followup(r)
 
 
 def run_mix(server, requests, time_scale=1.0):

@@ -230,3 +230,31 @@ def test_plain_fp64_batch_runs_in_blocks_that_fit():
     solves = [e for e in FakeSolver.log if e[0] == 'solve' and e[1] == id(p)]
     assert len(solves) == 1 and solves[0][6] == block < r.n_freq
     assert r.result['results'].shape[0] == r.n_freq
+
+
+class StallingBatch(FakeBatch):
+    """Reports every other frequency of a request as not converged (status 5)."""
+
+    def take(self, tag):
+        out = FakeBatch.take(self, tag)
+        out['status'][::2] = 5
+        out['results'][::2, 0] = -1.0          # what a stalled refinement leaves behind
+        return out
+
+
+def test_unconverged_mixed_frequencies_are_solved_again_in_fp64():
+    p = _na(nf=7)
+    p.geometry_key = 'na-stall'
+    FakeSolver.log = []
+    srv = Server(hbm_budget=1 << 40, workers=1, solver_factory=FakeSolver, context_factory=FakeContext,
+                 batch_factory=StallingBatch)
+    with srv:
+        r = srv.submit(ServeRequest(0, p, precision='mixed_bf16x3', pol_mask=1, tol=1.0))
+        assert r.done.wait(5) and r.error is None, r.error
+    assert r.escalated == 4
+    assert np.all(r.result['status'] == 0)
+    # the follow-up solved exactly the stalled frequencies on the resident geometry
+    solves = [e for e in FakeSolver.log if e[0] == 'solve']
+    assert len(solves) == 1 and solves[0][3] == 4
+    assert [e for e in FakeSolver.log if e[0] == 'build'] == [('build', id(p), True)]
+    np.testing.assert_array_equal(r.result['results'][:, 0], p.freqs)
