@@ -965,7 +965,7 @@ def main():
 
     pk, pk_kind = peaks()
     n = prob.n_var
-    tc_operand = 4.0 * (-(-n // 256) * 256) * (-(-n // 64) * 64)
+    tc_operand = (2.0 if args.precision == 'mixed_bf16' else 4.0) * (-(-n // 256) * 256) * (-(-n // 64) * 64)
     avg_ms = prof['ms'] / max(1, prof['launches'])
     bytes_per = prof['bytes'] / max(1, prof['launches'])
     flops_per = prof['flops'] / max(1, prof['launches'])

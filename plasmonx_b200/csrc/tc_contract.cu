@@ -239,7 +239,8 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
     if (threadIdx.x == 0) {
         // ---------------- TMA producer ----------------
         const CUtensorMap *mp = p.map[gi];
-        const uint32_t tx = (uint32_t)(2 * kA + 2 * bn * kBK * 2);
+        // one product (NPROD = 1) reads only the high parts: half the operand bytes
+        const uint32_t tx = (uint32_t)(NPROD > 1 ? 2 * kA + 2 * bn * kBK * 2 : kA + bn * kBK * 2);
         for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % STAGES;
             if (kt >= STAGES) {
@@ -252,9 +253,9 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
             const int kx = (kt0 + kt) * kBK;
             const int ay = (mtile * ktiles + kt0 + kt) * kBM;          // tile-ordered A
             tma_load_2d(&mp[0], &full[s], stage_ptr(s, 0), 0, ay);
-            tma_load_2d(&mp[1], &full[s], stage_ptr(s, 1), 0, ay);
+            if (NPROD > 1) tma_load_2d(&mp[1], &full[s], stage_ptr(s, 1), 0, ay);
             tma_load_2d(&mp[2], &full[s], stage_ptr(s, 2), kx, n0);
-            tma_load_2d(&mp[3], &full[s], stage_ptr(s, 3), kx, n0);
+            if (NPROD > 1) tma_load_2d(&mp[3], &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
         }
     } else if (threadIdx.x == 32) {

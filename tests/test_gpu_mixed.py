@@ -59,7 +59,7 @@ def test_contraction_unaligned_size(ctx):
     assert np.max(np.linalg.norm(s3 - ref, axis=1) / np.linalg.norm(ref, axis=1)) < 5e-5
 
 
-@pytest.mark.parametrize('precision,bar', [('mixed_bf16x3', 1e-6), ('fp64_refined', 1e-10)])
+@pytest.mark.parametrize('precision,bar', [('mixed_bf16x3', 1e-6), ('mixed_bf16', 1e-6), ('fp64_refined', 1e-10)])
 def test_refined_solve_matches_lu(ctx, precision, bar):
     p, s = _ag(radius=10.0, n_freq=5)
     ref = osolve.solve(s, method='inversion')
