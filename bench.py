@@ -844,6 +844,7 @@ def main():
         args.inner_krylov = chosen['inner_krylov']
         if not args.inner_tol:
             args.inner_tol = chosen['inner_tol']
+        args.precision = chosen.get('precision', args.precision)
         tuning = tuner.records[args.config]
     gathered = {}
 
@@ -874,6 +875,7 @@ def main():
     dev_ms = []
     launches = 0
     steps_hist = []
+    unconverged_hist = []
     with Clocks(local) as clk:
         barrier(pg, local)
         t0 = time.perf_counter()
@@ -882,6 +884,7 @@ def main():
             dev_ms.append(out['device_ms'])
             launches += out['launches']
             steps_hist.append(out['steps'][:, 0].copy())
+            unconverged_hist.append(int(np.sum(out['status'] != 0)))
         barrier(pg, local)
         wall = time.perf_counter() - t0
     breakdown = ctx.profile_breakdown()
@@ -1053,6 +1056,7 @@ def main():
                 'clocks': clk.summary(), 'wall_s_timed': wall,
                 'device_ms_breakdown': {k: round(v['ms'], 3) for k, v in breakdown.items()},
                 'sigma_abs_max_rel_err': None if acc is None else acc['headline_max_rel_err'],
+                'status_ok': not any(unconverged_hist), 'unconverged_freq_solves': int(sum(unconverged_hist)),
                 'accuracy': acc, 'fp64_plain_gmres': fp64,
                 'speedup_vs_fp64_plain': None if fp64 is None else value / fp64['value'],
                 'tuning': tuning,

@@ -166,7 +166,12 @@ struct TcLaunch {
     uint32_t wait_limit;
 };
 
-__host__ __device__ constexpr int tc_stage_bytes(int bn) { return 2 * (kBM * kBK * 2) + 2 * (bn * kBK * 2); }
+// Bytes of one pipeline stage: the A and X tiles its products read -- high and
+// low parts for three products, the high parts alone for one (whose stages are
+// then half as large and twice as many fit).
+__host__ __device__ constexpr int tc_stage_bytes(int bn, int nprod) {
+    return (nprod > 1 ? 2 : 1) * (kBM * kBK * 2 + bn * kBK * 2);
+}
 
 template <int NPROD>
 __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_constant__ TcLaunch p) {
@@ -189,7 +194,7 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
     const int bn = G.bn, M = G.M, R = G.R, ktiles = G.ktiles;
     const int bnp = (bn + 31) & ~31;     // TMEM columns of one accumulator (32-aligned)
     const int STAGES = p.stages;
-    const int kStage = tc_stage_bytes(p.bn_max);
+    const int kStage = tc_stage_bytes(p.bn_max, NPROD);
     const int kA = kBM * kBK * 2;
     const int mtile = tile / G.ctiles;
     int *err = G.err;
@@ -230,9 +235,10 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
     const uint32_t tmem = *tmem_slot;
 
     auto stage_ptr = [&](int s, int which) -> uint8_t * {
-        // which: 0 A high, 1 A low, 2 X high, 3 X low
+        // which: 0 A high, 1 A low, 2 X high, 3 X low (the low parts only for NPROD > 1)
+        constexpr int parts = NPROD > 1 ? 2 : 1;
         uint8_t *st = base + s * kStage;
-        return which < 2 ? st + which * kA : st + 2 * kA + (which - 2) * (p.bn_max * kBK * 2);
+        return which < 2 ? st + which * kA : st + parts * kA + (which - 2) * (p.bn_max * kBK * 2);
     };
 
     int issued = 0;     // loads issued by the producer (thread 0)
@@ -851,8 +857,8 @@ void tc_contract_group(const std::vector<TcItem> &items) {
         gp.err = g->d_tc_err.p;
     }
     L.bn_max = bn_max;
-    L.stages = std::min(6, kSmemBudget / tc_stage_bytes(bn_max));
-    const int smem = L.stages * tc_stage_bytes(bn_max) + 1024 /* align */ + 256 /* barriers */;
+    L.stages = std::min(8, kSmemBudget / tc_stage_bytes(bn_max, nprod));
+    const int smem = L.stages * tc_stage_bytes(bn_max, nprod) + 1024 /* align */ + 256 /* barriers */;
     auto kern = nprod == 1 ? tc_contract_kernel<1> : tc_contract_kernel<3>;
     once_per_device(reinterpret_cast<const void *>(kern), ctx->device, [&] {
         PLX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));

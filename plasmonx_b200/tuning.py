@@ -12,9 +12,14 @@ geometry, not on the hardware alone:
                 whole grid does not fit the device budget, then blocks of 64,
                 32, 16 or 8.
 
-and the inner solve's relative tolerance (1e-3, 1e-4, 1e-5 around the best
-basis): a looser inner solve costs more FP64 residuals, a tighter one more
-inner steps.
+and, for the best basis, the inner solve's relative tolerance with the
+tensor-core form: BF16x3 (three products, ~1e-5 operator error) at 1e-3, 1e-4
+or 1e-5, or one BF16 product (half the operand bytes per launch, ~2e-3
+operator error) at 1e-2 or 3e-2 -- a looser inner solve costs more FP64
+residuals, a tighter one more inner steps, and the one-product operator pays
+for its cheaper launches with more outer steps, which wins where the
+refinement contracts fast (the silver sphere: 101 against 82 freq-solves/s)
+and loses where it does not (the Ag-Au bow-tie: 20 against 42).
 
 ``Tuner.settings(solver, key)`` runs a short sweep once per resident geometry
 -- the candidate settings on a few frequencies spread over the grid, each timed
@@ -25,21 +30,22 @@ it.  The sweep's records are kept for the report.
 import numpy as np
 
 INNER_CANDIDATES = (64, 128, 256)
-INNER_TOL_CANDIDATES = (1e-3, 1e-5)       # tried around the default 1e-4 for the best basis
+# (tensor-core form, inner tolerance) tried for the best basis beside the default (BF16x3, 1e-4)
+FORM_CANDIDATES = (('mixed_bf16x3', 1e-3), ('mixed_bf16x3', 1e-5), ('mixed_bf16', 1e-2), ('mixed_bf16', 3e-2))
 BLOCK_CANDIDATES = (0, 64, 32, 16, 8)
 
 
 class Tuner:
-    def __init__(self, n_probe=6, inner_candidates=INNER_CANDIDATES, inner_tol_candidates=INNER_TOL_CANDIDATES):
+    def __init__(self, n_probe=6, inner_candidates=INNER_CANDIDATES, form_candidates=FORM_CANDIDATES):
         self.n_probe = int(n_probe)
         self.inner_candidates = tuple(inner_candidates)
-        self.inner_tol_candidates = tuple(inner_tol_candidates)
+        self.form_candidates = tuple(form_candidates)
         self.cache = {}
         self.records = {}
 
     def settings(self, solver, key, freqs, alpha_w=None, precision='mixed_bf16x3', mode=None, pol_mask=1,
                  tol=None, fits=None):
-        """Tuned {'inner_krylov', 'freq_block'} for the geometry `key`.
+        """Tuned {'inner_krylov', 'inner_tol', 'precision', 'freq_block'} for the geometry `key`.
 
         solver  a Solver holding the geometry (its frequency table is restored)
         freqs   the request's grid; alpha_w its (n_types, F) table or None
@@ -55,25 +61,29 @@ class Tuner:
             block = next((b for b in BLOCK_CANDIDATES if (b == 0 or b < F) and fits(b)), 8)
         sweep = []
         solver.set_frequencies(np.asarray(freqs)[idx], None if alpha_w is None else np.asarray(alpha_w)[:, idx])
-        def trial(m, itol):
-            out = solver.solve(mode=mode, precision=precision, pol_mask=pol_mask, tol=tol, inner_krylov=m,
+        def trial(m, itol, prec):
+            out = solver.solve(mode=mode, precision=prec, pol_mask=pol_mask, tol=tol, inner_krylov=m,
                                inner_tol=itol)
             ok = 'error' not in out and bool(np.all(out['status'] == 0))
             per = out['device_ms'] / max(1, len(idx)) if ok else float('inf')
-            sweep.append({'inner_krylov': m, 'inner_tol': itol or 1e-4, 'ms_per_freq_solve': per, 'ok': ok})
+            sweep.append({'inner_krylov': m, 'inner_tol': itol or 1e-4, 'precision': prec,
+                          'ms_per_freq_solve': per, 'ok': ok})
 
+        # from BF16x3 every form is tried; a one-product request keeps its form
+        forms = [(f, t) for f, t in self.form_candidates if precision == 'mixed_bf16x3' or f == precision]
         try:
             for m in self.inner_candidates:
-                trial(min(m, int(solver.n_var)), 0.0)
+                trial(min(m, int(solver.n_var)), 0.0, precision)
             m_best = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))['inner_krylov']
-            for itol in self.inner_tol_candidates:
-                trial(m_best, itol)
+            for prec_, itol in forms:
+                trial(m_best, itol, prec_)
         finally:
             solver.set_frequencies(freqs, alpha_w)
         best = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))
         good = np.isfinite(best['ms_per_freq_solve'])
         chosen = {'inner_krylov': best['inner_krylov'] if good else 64,
-                  'inner_tol': best['inner_tol'] if good else 1e-4, 'freq_block': block}
+                  'inner_tol': best['inner_tol'] if good else 1e-4,
+                  'precision': best['precision'] if good else precision, 'freq_block': block}
         self.cache[key] = chosen
         self.records[key] = {'probe_freqs': [int(i) for i in idx], 'sweep': sweep, 'chosen': chosen}
         return chosen
