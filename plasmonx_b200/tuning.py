@@ -22,6 +22,8 @@ refinement contracts fast (the silver sphere: 101 against 82 freq-solves/s)
 and loses where it does not (the Ag-Au bow-tie: 20 against 42).
 
 ``Tuner.settings(solver, key)`` runs a short sweep once per resident geometry
+(the basis lengths with the default form; every form at the best of them; the
+basis lengths again with the best form)
 -- the candidate settings on a few frequencies spread over the grid, each timed
 by the library's own CUDA events -- and caches the fastest (device time per
 freq-solve) under the geometry's key; later requests on the same geometry reuse
@@ -77,6 +79,13 @@ class Tuner:
             m_best = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))['inner_krylov']
             for prec_, itol in forms:
                 trial(m_best, itol, prec_)
+            # the basis again for the best form, when that is not the one swept first
+            top = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))
+            if top['precision'] != precision or top['inner_tol'] != 1e-4:
+                for m in self.inner_candidates:
+                    m = min(m, int(solver.n_var))
+                    if m != top['inner_krylov']:
+                        trial(m, top['inner_tol'], top['precision'])
         finally:
             solver.set_frequencies(freqs, alpha_w)
         best = min(sweep, key=lambda r: (r['ms_per_freq_solve'], r['inner_krylov']))

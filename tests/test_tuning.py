@@ -34,11 +34,24 @@ def test_tuner_picks_the_fastest_setting_and_restores_the_grid():
     got = t.settings(sv, 'g', freqs)
     assert got['inner_krylov'] == 128 and got['precision'] == 'mixed_bf16' and got['inner_tol'] == 1e-2
     np.testing.assert_array_equal(sv.freqs, freqs)            # the request's grid is back
-    # the basis sweep, then every form at the best basis, each on the probe frequencies
-    assert len(sv.calls) == len(INNER_CANDIDATES) + len(FORM_CANDIDATES)
+    # the basis sweep, every form at the best basis, the other bases with the best form,
+    # each on the probe frequencies
+    n_trials = len(INNER_CANDIDATES) + len(FORM_CANDIDATES) + len(INNER_CANDIDATES) - 1
+    assert len(sv.calls) == n_trials
     assert all(n == 6 for _, n in sv.calls)
     # cached per geometry key
-    assert t.settings(sv, 'g', freqs) is got and len(sv.calls) == len(INNER_CANDIDATES) + len(FORM_CANDIDATES)
+    assert t.settings(sv, 'g', freqs) is got and len(sv.calls) == n_trials
+
+
+def test_tuner_resweeps_the_basis_for_the_best_form():
+    # BF16x3 is fastest at 128, the one-product form at 64
+    def cost(prec, m, itol):
+        if prec == 'mixed_bf16':
+            return {64: 5.0, 128: 7.0, 256: 9.0}[m] if itol == 3e-2 else 20.0
+        return {64: 10.0, 128: 8.0, 256: 9.0}[m]
+    sv = TimedSolver(cost)
+    got = Tuner(n_probe=6).settings(sv, 'r', np.linspace(3.0, 4.5, 50))
+    assert (got['precision'], got['inner_krylov'], got['inner_tol']) == ('mixed_bf16', 64, 3e-2)
 
 
 def test_tuner_skips_settings_that_do_not_converge():
