@@ -831,6 +831,7 @@ def main():
     gather_dev = 'cuda:%d' % local if pg is not None and pg.get_backend() == 'nccl' else 'cpu'
     full_freqs, full_aw = prob.freqs, prob.alpha_w
     tuning = None
+    requested_precision = args.precision          # the serving leg's requests keep it
     if args.inner_krylov == 0 and args.precision.startswith('mixed'):
         # the inner basis length from a short sweep on a few of the grid's frequencies
         # (plasmonx_b200.tuning), cached per geometry; not part of the timed region
@@ -1017,12 +1018,12 @@ def main():
     if args.serving_requests > 0 and args.impl == 'ours':
         from plasmonx_b200.serving import Server, request_pool, run_mix
         pool = request_pool(n_requests=args.serving_requests, rate=args.serving_rate, seed=7 + rank,
-                            scale=args.serving_scale, precision=args.precision)
+                            scale=args.serving_scale, precision=requested_precision)
         with Server(device=local, workers=args.serving_workers) as srv:
             serving = run_mix(srv, pool)
         steps = srv.steps
         serving.update({'rate_per_s': args.serving_rate, 'scale': args.serving_scale,
-                        'workers': args.serving_workers, 'precision': args.precision,
+                        'workers': args.serving_workers, 'precision': requested_precision,
                         'modes': sorted({str(r.mode) for r in pool}),
                         'mean_requests_sharing_a_step': float(np.mean([r.batch_size for r in pool])),
                         'outer_steps': len(steps),
