@@ -88,6 +88,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
     return false;
 }
 
+// Plain bulk copy of `bytes` contiguous bytes into shared memory (addresses
+// 16-byte aligned, size a multiple of 16), completing on `bar`.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *bar, void *dst, int x, int y) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
@@ -153,12 +162,13 @@ struct TcGroup {
     int M, R, bn, ktiles;       // rows, real columns, column tile, k-tiles (32 deep)
     int unit0;                  // first CTA of the group
     int full, q, kper, ctiles;  // schedule (see above)
+    const uint8_t *ah, *al;     // A high / low, tile-ordered and pre-swizzled (16 KB per stage tile)
     double *S;                  // [R][M] FP64
     float *P;                   // pieces of the split tiles
     int *err;                   // the geometry's error word (first bounded wait that ran out)
 };
 struct TcLaunch {
-    CUtensorMap map[kMaxGroups][4];   // A high, A low, X high, X low
+    CUtensorMap map[kMaxGroups][4];   // [2], [3]: X high, X low ([0], [1] unused: A goes by bulk copy)
     TcGroup grp[kMaxGroups];
     int ngroups;
     int stages;                 // pipeline depth
@@ -257,9 +267,9 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
             }
             mbar_expect_tx(&full[s], tx);
             const int kx = (kt0 + kt) * kBK;
-            const int ay = (mtile * ktiles + kt0 + kt) * kBM;          // tile-ordered A
-            tma_load_2d(&mp[0], &full[s], stage_ptr(s, 0), 0, ay);
-            if (NPROD > 1) tma_load_2d(&mp[1], &full[s], stage_ptr(s, 1), 0, ay);
+            const size_t aoff = (size_t)(mtile * ktiles + kt0 + kt) * kA;   // tile-ordered A
+            bulk_load(stage_ptr(s, 0), G.ah + aoff, kA, &full[s]);
+            if (NPROD > 1) bulk_load(stage_ptr(s, 1), G.al + aoff, kA, &full[s]);
             tma_load_2d(&mp[2], &full[s], stage_ptr(s, 2), kx, n0);
             if (NPROD > 1) tma_load_2d(&mp[3], &full[s], stage_ptr(s, 3), kx, n0);
             issued = kt + 1;
@@ -375,10 +385,16 @@ __global__ void __launch_bounds__(128, 1) tc_contract_kernel(const __grid_consta
 
 // The A operand (T, A0 or D^T split in BF16 high/low) is stored in the order
 // the kernel reads it: [m-tile of 256 rows][k-slab of 32][256 rows][32 k], so
-// every TMA box (256 x 32) is one contiguous 16 KB block of HBM.  Rows beyond
-// n and k beyond n are zero.
+// every stage's tile (256 x 32) is one contiguous 16 KB block of HBM, and within
+// the tile already in the shared-memory image the UMMA descriptors read: the
+// 64-byte swizzle, in which the 16-byte chunk c of row r sits at chunk
+// c ^ ((r >> 1) & 3) of its 64-byte row.  A stage's A tile is then one plain
+// bulk copy.  Rows beyond n and k beyond n are zero.
+__device__ __forceinline__ int64_t a_tile_pos(int64_t rr, int64_t kk) {
+    return rr * kBK + ((((kk >> 3) ^ ((rr >> 1) & 3)) << 3) | (kk & 7));
+}
 __device__ __forceinline__ int64_t a_tiled(int64_t r, int64_t k, int64_t ktiles) {
-    return (((r / kBM) * ktiles + k / kBK) * kBM + r % kBM) * kBK + k % kBK;
+    return ((r / kBM) * ktiles + k / kBK) * (int64_t)(kBM * kBK) + a_tile_pos(r % kBM, k % kBK);
 }
 
 __device__ __forceinline__ void split_store(double a, int64_t idx, __nv_bfloat16 *__restrict__ hi,
@@ -397,7 +413,7 @@ __global__ void split_tiled(int n, int64_t ktiles, int64_t total, const double *
         const int64_t kk = e % kBK, rr = (e / kBK) % kBM, tk = e / ((int64_t)kBK * kBM);
         const int64_t r = (tk / ktiles) * kBM + rr, k = (tk % ktiles) * kBK + kk;
         const double a = (r < n && k < n) ? in[r * n + k] : 0.0;
-        split_store(a, e, hi, lo);
+        split_store(a, tk * (int64_t)(kBM * kBK) + a_tile_pos(rr, kk), hi, lo);
     }
 }
 
@@ -418,8 +434,8 @@ __global__ void split_tiled_t(int n, int64_t ktiles, const double *__restrict__ 
         const int rr = e / kBK, kk = e % kBK;
         float x = tile[kk][rr];
         __nv_bfloat16 h = __float2bfloat16_rn(x);
-        hi[base + e] = h;
-        lo[base + e] = __float2bfloat16_rn(x - __bfloat162float(h));
+        hi[base + a_tile_pos(rr, kk)] = h;
+        lo[base + a_tile_pos(rr, kk)] = __float2bfloat16_rn(x - __bfloat162float(h));
     }
 }
 
@@ -433,7 +449,7 @@ __global__ void split_tiled_gen(int N, int n, int fmu, int64_t ktiles, const dou
     for (int e = threadIdx.x; e < kBK * kBM; e += blockDim.x) {
         const int64_t r = r0 + e / kBK, k = k0 + e % kBK;
         const double a = (r < n && k < n) ? plx_t_element(N, fmu != 0, pos, par, r, k) : 0.0;
-        split_store(a, base + e, hi, lo);
+        split_store(a, base + a_tile_pos(e / kBK, e % kBK), hi, lo);
     }
 }
 
@@ -829,13 +845,12 @@ void tc_contract_group(const std::vector<TcItem> &items) {
             R, n, n, it.X, Rpad, ld, reinterpret_cast<__nv_bfloat16 *>(g->d_Xh.p),
             reinterpret_cast<__nv_bfloat16 *>(g->d_Xl.p));
         ctx->launches++;
-        // A in tile order: rows of kBK elements, kBM rows per box
-        const uint64_t arows = (uint64_t)((M + kBM - 1) / kBM) * kBM * (uint64_t)(ld / kBK);
-        L.map[k][0] = make_map(it.folded ? g->d_Ah.p : g->d_Th.p, kBK, arows, kBK, kBM);
-        L.map[k][1] = make_map(it.folded ? g->d_Al.p : g->d_Tl.p, kBK, arows, kBK, kBM);
         L.map[k][2] = make_map(g->d_Xh.p, ld, Rpad, ld, bn);
         L.map[k][3] = make_map(g->d_Xl.p, ld, Rpad, ld, bn);
         TcGroup &gp = L.grp[k];
+        // A in tile order, one contiguous pre-swizzled 16 KB block per stage tile
+        gp.ah = reinterpret_cast<const uint8_t *>(it.folded ? g->d_Ah.p : g->d_Th.p);
+        gp.al = reinterpret_cast<const uint8_t *>(it.folded ? g->d_Al.p : g->d_Tl.p);
         gp.M = M;
         gp.R = R;
         gp.bn = bn;
