@@ -95,6 +95,7 @@ class ServeRequest:
         self.error = None
         self.mode = None
         self.batch_size = 0
+        self.escalated = 0          # frequencies solved again in plain FP64 (mixed form, unconverged)
         self.worker = None
         self.done = threading.Event()
 
