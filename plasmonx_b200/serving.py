@@ -38,6 +38,13 @@ import numpy as np
 from .solver import Batch, Context, Solver
 
 KRYLOV_INNER = 64
+MEMORY_RETRIES = 3
+
+
+def _out_of_memory(e):
+    """A device allocation failure (the library's NOMEM / BUDGET statuses, or the
+    loop's own refusal)."""
+    return isinstance(e, MemoryError) or getattr(e, 'code', None) in (3, 4)
 
 
 def _is_bem(problem):
@@ -48,6 +55,16 @@ def geometry_key(problem):
     """Identity of a geometry: requests with the same key share a resident geometry."""
     key = getattr(problem, 'geometry_key', None)
     return key if key is not None else id(problem)
+
+
+def build_peak(problem, mode, precision):
+    """Device bytes held only while a geometry is built: matrix-free with the
+    tensor-core operand, the window of generated T rows its fold reads (up to
+    ~6 GB, freed when the operand is done)."""
+    n = int(problem.n_var)
+    if precision.startswith('mixed') and mode == 'iterative on the fly' and not _is_bem(problem):
+        return min(int(6.0e9), 8 * n * n)
+    return 0
 
 
 def footprint(problem, mode, precision, n_cols):
@@ -68,13 +85,17 @@ def footprint(problem, mode, precision, n_cols):
         geo += 20 * 600 * int(problem.n_atoms)
     mixed = precision.startswith('mixed')
     if mixed:
-        geo += 4 * rows * ld
+        # the BF16 high/low operand and the k-split partials (at most 148 pieces of
+        # 256 x 256 FP32)
+        geo += 4 * rows * ld + 148 * 256 * 256 * 4
     if mixed:
         krylov = (KRYLOV_INNER + 1) * n_cols * 2 * n * 4
     else:
         m = min(int(getattr(problem, 'gmres_dim', 1000) or 1000), n)
         krylov = (m + 1) * n_cols * 2 * n * 8
-    work = 12 * n_cols * 2 * n * 8 + (4 * 2 * n_cols * n * 8 if mixed else 0)
+    # work arrays of the outer and inner solves, and the BF16 split of the
+    # contraction's input (2 real columns per complex one, 4 bytes per entry)
+    work = 12 * n_cols * 2 * n * 8 + (4 * 2 * n_cols * n * 8 + 4 * 2 * n_cols * ld if mixed else 0)
     return geo, krylov + work
 
 
@@ -96,6 +117,8 @@ class ServeRequest:
         self.mode = None
         self.batch_size = 0
         self.escalated = 0          # frequencies solved again in plain FP64 (mixed form, unconverged)
+        self.mem_retries = 0        # times put back after running out of device memory
+        self.waiting_memory = False
         self.worker = None
         self.done = threading.Event()
 
@@ -158,7 +181,7 @@ class Server:
 
     def _free_bytes(self):
         free = self._device_free()
-        return 64 << 30 if free is None else int(0.8 * free)
+        return 64 << 30 if free is None else int(0.75 * free)
 
     def _device_free(self):
         try:
@@ -235,6 +258,7 @@ class Server:
         modes = ['iterative'] if _is_bem(p) else ['iterative', 'iterative on the fly']
         for mode in modes:
             geo, batch = footprint(p, mode, req.precision, self._block_cols(p, mode, req.precision, self._cols(req)))
+            batch += build_peak(p, mode, req.precision)      # transient, checked at admission
             short = self.committed + geo + batch - self.budget
             if short > 0 and short > self.freeing:
                 self._evict(short - self.freeing)
@@ -353,9 +377,13 @@ class Server:
         settings; their batch bytes are reserved."""
         q = self.queues[w]
         out = []
+        busy = self._in_flight(w)
         for r in list(q):
             if r.precision == 'fp64':
                 continue
+            if r.waiting_memory and busy:
+                continue                  # out of memory before: waits for this worker to drain
+            r.waiting_memory = False
             ob = self._open[w].get(r.key)
             if ob is not None and ob['precision'] != r.precision:
                 continue                  # waits until that batch drains
@@ -394,7 +422,10 @@ class Server:
             r.worker = w
             ob['reqs'][r.id] = r
         except Exception as e:
-            self._finish(r, error=e)
+            if _out_of_memory(e) and r.mem_retries < MEMORY_RETRIES:
+                self._requeue(w, r)
+            else:
+                self._finish(r, error=e)
 
     def _step(self, w):
         """One outer step of every open batch of this worker with columns in flight:
@@ -410,6 +441,27 @@ class Server:
             else:
                 type(batches[0]).step_group(batches)
         except Exception as e:
+            if _out_of_memory(e):
+                # the failed step leaves its batches unusable: close them and run their
+                # requests again from the start once memory is free
+                for key, ob in list(self._open[w].items()):
+                    if not any(ob is x for x in live):
+                        continue
+                    reqs = list(ob['reqs'].values())
+                    ob['reqs'].clear()
+                    try:
+                        ob['batch'].close()
+                    except Exception:
+                        pass
+                    with self.lock:
+                        del self._open[w][key]
+                        ob['res'].busy = False
+                    for r in reqs:
+                        if r.mem_retries < MEMORY_RETRIES:
+                            self._requeue(w, r)
+                        else:
+                            self._finish(r, error=e)
+                return
             for ob in live:
                 for r in list(ob['reqs'].values()):
                     self._finish(r, error=e)
@@ -449,6 +501,20 @@ class Server:
                     ob['res'].last_used = time.perf_counter()
                     self._dispatch()
                     self.lock.notify_all()
+
+    def _requeue(self, w, r):
+        """An out-of-memory failure (lock not held): the request's batch bytes are
+        released and it goes back to the head of its worker's queue, held there until
+        that worker has nothing in flight (the memory its running batches hold is
+        then free), at most MEMORY_RETRIES times."""
+        with self.lock:
+            self.committed -= getattr(r, 'batch_bytes', 0)
+            r.batch_bytes = 0
+            r.result = None
+            r.mem_retries += 1
+            r.waiting_memory = True
+            self.queues[w].appendleft(r)
+            self.lock.notify_all()
 
     def _escalate(self, w, r, bad):
         """Frequencies of a mixed-precision request that did not converge (the

@@ -9,7 +9,7 @@ import time
 import numpy as np
 
 from plasmonx_b200 import configs
-from plasmonx_b200.serving import Server, ServeRequest, footprint, request_pool, run_mix
+from plasmonx_b200.serving import build_peak, Server, ServeRequest, footprint, request_pool, run_mix
 
 
 class FakeContext:
@@ -151,10 +151,14 @@ def test_two_geometries_on_one_worker_share_grouped_steps():
 
 
 def test_admission_picks_matrix_free_when_t_does_not_fit_and_rejects_too_large():
-    p = configs.particle('Ag', 'sphere', 12.0, n_freq=4, method='iterative', tolerance=1e-9)
+    # large enough that the matrix-free build's window of generated T rows (~6 GB,
+    # held while the geometry is built) is smaller than T itself
+    p = configs.particle('Ag', 'sphere', 33.0, n_freq=4, method='iterative', tolerance=1e-9)
     geo_mem, bat = footprint(p, 'iterative', 'mixed_bf16x3', 4)
     geo_otf, _ = footprint(p, 'iterative on the fly', 'mixed_bf16x3', 4)
-    budget = geo_otf + bat + (geo_mem - geo_otf) // 2
+    peak = build_peak(p, 'iterative on the fly', 'mixed_bf16x3')
+    assert peak < geo_mem - geo_otf
+    budget = geo_otf + bat + peak + (geo_mem - geo_otf - peak) // 2
     with _server(budget) as srv:
         r = srv.submit(ServeRequest(0, p, precision='mixed_bf16x3', pol_mask=1, tol=1.0))
         assert r.done.wait(5)
@@ -258,3 +262,40 @@ def test_unconverged_mixed_frequencies_are_solved_again_in_fp64():
     assert len(solves) == 1 and solves[0][3] == 4
     assert [e for e in FakeSolver.log if e[0] == 'build'] == [('build', id(p), True)]
     np.testing.assert_array_equal(r.result['results'][:, 0], p.freqs)
+
+
+class OnceOutOfMemoryBatch(FakeBatch):
+    """The first outer step of the run fails the way a device allocation does."""
+    failed = False
+
+    @staticmethod
+    def step_group(batches):
+        if not OnceOutOfMemoryBatch.failed:
+            OnceOutOfMemoryBatch.failed = True
+            raise MemoryError('device allocation failed')
+        FakeBatch.step_group(batches)
+
+    def step(self):
+        OnceOutOfMemoryBatch.step_group([self])
+
+
+def test_requests_of_a_step_that_ran_out_of_memory_run_again():
+    p = _na(nf=5)
+    p.geometry_key = 'na-oom'
+    FakeSolver.log = []
+    OnceOutOfMemoryBatch.failed = False
+    srv = Server(hbm_budget=1 << 40, workers=1, solver_factory=FakeSolver, context_factory=FakeContext,
+                 batch_factory=OnceOutOfMemoryBatch)
+    with srv:
+        rs = [srv.submit(_req(k, p, [1.0 + k, 2.0 + k, 3.0 + k])) for k in range(3)]
+        for r in rs:
+            assert r.done.wait(5)
+    assert OnceOutOfMemoryBatch.failed
+    for r in rs:
+        assert r.error is None, r.error
+        np.testing.assert_array_equal(r.result['results'][:, 0], r.problem.freqs)
+    assert max(r.mem_retries for r in rs) == 1
+    # every batch reservation was given back, only the resident geometry's remains
+    assert srv.committed == footprint(p, 'iterative', 'mixed_bf16x3', 1)[0]
+    builds = [e for e in FakeSolver.log if e[0] == 'build']
+    assert len(builds) == 1                                   # the geometry stayed resident
