@@ -341,6 +341,10 @@ class Server:
                         break        # stopping, nothing queued or in flight
                     joining = self._take_joining(w)
                     plain = [] if joining or self._in_flight(w) else self._take_plain(w)
+                    if not joining and not plain and not self._in_flight(w):
+                        # queued work that waits for memory another worker holds
+                        self.lock.wait(0.05)
+                        continue
                 if plain:
                     self._plain_batch(w, plain, ctx)
                     continue
@@ -378,19 +382,26 @@ class Server:
         q = self.queues[w]
         out = []
         busy = self._in_flight(w)
+        device_busy = any(self._in_flight(v) for v in range(self.n_workers))
         for r in list(q):
             if r.precision == 'fp64':
                 continue
             if r.waiting_memory and busy:
                 continue                  # out of memory before: waits for this worker to drain
-            r.waiting_memory = False
             ob = self._open[w].get(r.key)
             if ob is not None and ob['precision'] != r.precision:
                 continue                  # waits until that batch drains
             res = self.resident[w].get(r.key)
             mode = res.mode if res is not None else (r.mode or 'iterative')
-            _, r.batch_bytes = footprint(r.problem, mode, r.precision, self._cols(r))
-            self.committed += r.batch_bytes
+            _, bb = footprint(r.problem, mode, r.precision, self._cols(r))
+            short = self.committed + bb - self.budget
+            if short > 0 and short > self.freeing:
+                self._evict(short - self.freeing)     # idle resident geometries first
+            if self.committed + bb > self.budget and (out or device_busy):
+                continue                  # waits until running batches give their memory back
+            r.waiting_memory = False
+            r.batch_bytes = bb
+            self.committed += bb
             q.remove(r)
             out.append(r)
         return out
