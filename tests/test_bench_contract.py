@@ -61,3 +61,26 @@ def test_field_grid_reference_arm_prints_the_contract_line():
     assert d['impl'] == 'reference' and d['metric'] == bench.POINTS_METRIC and d['unit'] == 'points/s'
     assert d['config']['n_points'] == 12 ** 3 and d['value'] > 0
     assert d['e2e']['h2d_bytes_per_step'] == 0 and d['cpu_baseline']['kind'] == 'port'
+
+
+def test_inversion_reference_arm_times_the_lu():
+    """Config 1 in inversion mode: the reference arm times a complex LU and its
+    three solves per frequency (zgetrf / zgetrs), not GMRES products."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--config',
+                          'na_sphere', '--mode', 'inversion', '--steps', '1', '--warmup', '0'], capture_output=True,
+                         text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip().startswith('{')]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d['impl'] == 'reference' and d['config']['mode'] == 'inversion' and d['value'] > 0
+    assert 'LU' in d['cpu_baseline']['sample'] and d['cpu_baseline']['steps_per_solve'] is None
+    assert d['e2e']['h2d_bytes_per_step'] == 0
+
+
+def test_serving_reference_arm_reports_unavailable():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--config',
+                          'serving'], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads([l for l in out.stdout.splitlines() if l.strip().startswith('{')][-1])
+    assert d['impl'] == 'reference' and 'unavailable' in d
