@@ -98,6 +98,23 @@ STEPS_PER_SOLVE = {'ag_sphere': 335.6, 'na_sphere': 60.0, 'bowtie': 600.0, 'bem_
 TRAFFIC_RATIO = (1.972 + 0.065) / 1.877
 
 
+def contraction_bound(roof, hbm_gbs):
+    """The tensor-core launch's own bound, the slower of streaming its operand once
+    at the measured copy bandwidth and issuing its products at the tensor peak; when
+    the operand stream binds (the one-product form, few columns) the roofline is
+    stated in GB/s against the copy bandwidth, the algorithmic TFLOP/s kept beside."""
+    avg_ms = roof['avg_launch_ms']
+    t_hbm = roof['bytes_per_launch'] / (hbm_gbs * 1e9) * 1e3
+    t_mma = roof['issued_tensor_tflops'] * avg_ms / roof['peak']
+    roof.update({'hbm_bound_ms': t_hbm, 'tensor_issue_bound_ms': t_mma, 'bound_frac': max(t_hbm, t_mma) / avg_ms,
+                 'binding': 'hbm' if t_hbm > t_mma else 'tensor issue'})
+    if t_hbm > t_mma:
+        roof.update({'bound': 'hbm', 'achieved_algorithmic_tflops': roof['achieved'],
+                     'tensor_peak_tflops': roof['peak'], 'achieved': roof['achieved_hbm_gbs'], 'peak': hbm_gbs,
+                     'unit': 'GB/s', 'frac': roof['achieved_hbm_gbs'] / hbm_gbs})
+    return roof
+
+
 def peaks():
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     if os.path.exists(p):
@@ -1005,13 +1022,7 @@ def main():
         if 'issued_tensor_tflops' in roof:
             # the BF16 products the tensor pipe executes (3 per algorithmic product for bf16x3)
             roof['issued_frac'] = roof['issued_tensor_tflops'] / roof['peak']
-            # the launch's own bound: the slower of streaming its operand once at the
-            # measured copy bandwidth and issuing its products at the tensor peak
-            t_hbm = roof['bytes_per_launch'] / (pk['hbm_gbs'] * 1e9) * 1e3
-            t_mma = roof['issued_tensor_tflops'] * avg_ms / roof['peak']
-            roof.update({'hbm_bound_ms': t_hbm, 'tensor_issue_bound_ms': t_mma,
-                         'bound_frac': max(t_hbm, t_mma) / avg_ms,
-                         'binding': 'hbm' if t_hbm > t_mma else 'tensor issue'})
+            contraction_bound(roof, pk['hbm_gbs'])
 
     # serving leg: a seeded Poisson mix of spectrum requests through the request loop
     serving = None

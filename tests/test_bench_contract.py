@@ -84,3 +84,21 @@ def test_serving_reference_arm_reports_unavailable():
     assert out.returncode == 0, out.stderr[-2000:]
     d = json.loads([l for l in out.stdout.splitlines() if l.strip().startswith('{')][-1])
     assert d['impl'] == 'reference' and 'unavailable' in d
+
+
+def test_contraction_roofline_names_the_binding_resource():
+    sys.path.insert(0, ROOT)
+    import bench
+    # one product, few columns: 3.5 GB streamed in 0.95 ms, 0.19 PFLOP issued
+    roof = {'bound': 'tensor', 'achieved': 200.0, 'peak': 1400.0, 'unit': 'TFLOP/s', 'avg_launch_ms': 0.95,
+            'bytes_per_launch': 3.5e9, 'issued_tensor_tflops': 200.0, 'achieved_hbm_gbs': 3.5e9 / 0.95e-3 / 1e9}
+    r = bench.contraction_bound(dict(roof), 6650.0)
+    assert r['binding'] == 'hbm' and r['bound'] == 'hbm' and r['unit'] == 'GB/s' and r['peak'] == 6650.0
+    assert abs(r['frac'] - r['achieved'] / 6650.0) < 1e-12 and r['achieved_algorithmic_tflops'] == 200.0
+    assert abs(r['bound_frac'] - (3.5e9 / 6650e9 * 1e3) / 0.95) < 1e-12
+    # three products, many columns: the tensor issue binds and the line stays in TFLOP/s
+    roof.update(issued_tensor_tflops=1000.0, avg_launch_ms=1.9, bytes_per_launch=7.0e9,
+                achieved_hbm_gbs=7.0e9 / 1.9e-3 / 1e9, achieved=333.0)
+    r = bench.contraction_bound(dict(roof), 6650.0)
+    assert r['binding'] == 'tensor issue' and r['bound'] == 'tensor' and r['unit'] == 'TFLOP/s'
+    assert r['achieved'] == 333.0 and r['peak'] == 1400.0
